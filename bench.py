@@ -1,0 +1,325 @@
+#!/usr/bin/env python3
+"""Benchmark of the raw -> RGB hot path (demosaic + 5-level PCA pyramid
+denoise + reconstruct) on 12 MP RGGB frames.
+
+A step is one frame of the 4032x3024 12-bit workload through
+RawConverter::demosaic with noise reduction, on the FP16-storage path.
+`value` is frames/s with the raw frames already resident in HBM; `e2e` is
+the same call with host buffers (pinned raw in, FP16 RGBA out) copied inside
+the timed region. With --gpus N (torchrun), every rank converts its own
+frames (no data-path collective); the time is the max over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "12MP raw->RGB frames/s (demosaic + 5-level PCA pyramid denoise), FP16-storage batched path"
+UNIT = "frames/s"
+WORKLOAD = "cfg2_4032x3024"
+N_ROTATE = 6  # distinct resident frames (6 x 24 MB raw + planes >> 126 MB L2)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, n in enumerate(names):
+                    if r[5 + k].lower().startswith("active"):
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(wl, params_fn, seconds: float):
+    """The oracle's FP32 run (the CPU restatement of the reference path) on
+    all host cores, over a bounded sample: a 1008x756 frame of the same
+    scene recipe and 5-level schedule (1/16 of the 12 MP area), repeated for
+    about `seconds`; frames/s scaled to 12 MP by the pixel-count ratio."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import _oracle as O
+    from glasscamerapublic_b200 import scene
+    sw, sh = wl.width // 4, wl.height // 4
+    swl = scene.Workload("cpu_sample", sw, sh, levels=wl.levels, black=wl.black, white=wl.white, gain=wl.gain,
+                         read=wl.read, iso=wl.iso, seed=wl.seed)
+    raw, _ = scene.make_raw(swl)
+    p = params_fn(swl)
+    threads = os.cpu_count() or 1
+    O.lib().orc_set_threads(threads)
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        O.raw_pipeline(raw, p, denoise=True, f64=False)
+        n += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    fps_sample = n / dt
+    scale = (sw * sh) / (wl.width * wl.height)
+    return {"value": fps_sample * scale, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} x {sw}x{sh} frame(s), 5 levels, FP32 oracle, {dt:.1f}s; frames/s scaled by area x{scale:.4f}"}
+
+
+def run_reference(args, rank):
+    """The reference arm: the reference's algorithm on host cores (the
+    oracle port; the Metal reference cannot run here)."""
+    if rank != 0:
+        return
+    from glasscamerapublic_b200 import scene
+    wl = scene.WORKLOADS[WORKLOAD]
+    times = []
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(wl, scene.make_params, seconds=max(2.0, args.cpu_seconds / max(1, args.steps)))
+        if i >= args.warmup:
+            vals.append(r["value"])
+        last = r
+    v = float(np.median(vals)) if vals else last["value"]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "frame": "4032x3024 RGGB 12-bit", "levels": 5},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": last["cores"], "kind": "port",
+                             "sample": last["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+    import torch.distributed as dist
+
+    import glasscamerapublic_b200 as g
+    from glasscamerapublic_b200 import scene
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    wl = scene.WORKLOADS[WORKLOAD]
+    params = scene.make_params(wl)
+    conv = g.RawConverter(local)
+    stream = torch.cuda.Stream()
+    H, W = wl.height, wl.width
+
+    # resident inputs: distinct frames per rank (weak scaling)
+    raws_host = []
+    for f in range(N_ROTATE):
+        raw, _ = scene.make_raw(wl, frame=rank * N_ROTATE + f)
+        raws_host.append(raw)
+    raws = [torch.from_numpy(r.view(np.int16)).to(f"cuda:{local}") for r in raws_host]
+    out = torch.empty((H, W, 4), dtype=torch.float16, device=f"cuda:{local}")
+
+    def step(i, fp16=True, host_pca=False):
+        conv.demosaic(raws[i % N_ROTATE], params, noiseReduction=True, fp16=fp16, out=out, out_fp16=True,
+                      stream=stream, host_pca=host_pca, sync=False)
+
+    lib = g.lib()
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            step(i)
+        stream.synchronize()
+        lib.gls_converter_reset_stats(conv.handle)
+        lib.gls_converter_set_profiling(conv.handle, 0)
+        barrier()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local)
+        sampler.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(args.steps):
+            step(i)
+        e1.record(stream)
+        stream.synchronize()
+        clocks = sampler.stop()
+        ms = e0.elapsed_time(e1)
+        stats = (g.KernelStat * 32)()
+        n = C.c_int32()
+        lib.gls_converter_stats(conv.handle, stats, 32, C.byref(n))
+        launches = int(sum(stats[i].launches for i in range(n.value)))
+        barrier()
+
+        # per-kernel device time inside an identical timed loop (events around
+        # each launch, on the launch stream)
+        lib.gls_converter_reset_stats(conv.handle)
+        lib.gls_converter_set_profiling(conv.handle, 1)
+        for i in range(args.steps):
+            step(i)
+        lib.gls_converter_stats(conv.handle, stats, 32, C.byref(n))
+        lib.gls_converter_set_profiling(conv.handle, 0)
+        per_kernel = {stats[i].name.decode(): {"launches": int(stats[i].launches), "ms": stats[i].ms}
+                      for i in range(n.value) if stats[i].launches}
+
+        # FP32 plain single-frame path (reference structure: FP32 planes, per-level host PCA)
+        for i in range(2):
+            step(i, fp16=False, host_pca=True)
+        stream.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n32 = max(3, args.steps // 4)
+        f0.record(stream)
+        for i in range(n32):
+            step(i, fp16=False, host_pca=True)
+        f1.record(stream)
+        stream.synchronize()
+        ms32 = f0.elapsed_time(f1) / n32
+
+        # end to end through the public API with host buffers
+        pinned_raw = [torch.from_numpy(r.view(np.int16)).pin_memory() for r in raws_host]
+        pinned_out = torch.empty((H, W, 4), dtype=torch.float16).pin_memory()
+        hv = g.ImageView(C.c_void_p(pinned_out.data_ptr()), W, H, 4, g.F16, W * 8)
+        flags = g.DENOISE | g.FP16_STORAGE | g.HOST_IO | g.SYNC
+
+        def e2e_step(i):
+            g.check(lib.gls_demosaic(conv.handle, C.c_void_p(pinned_raw[i % N_ROTATE].data_ptr()), W, H, W * 2,
+                                     C.byref(params), flags, C.byref(hv), C.c_void_p(stream.cuda_stream)))
+
+        for i in range(2):
+            e2e_step(i)
+        n_e2e = max(3, args.steps // 2)
+        barrier()
+        t0 = time.perf_counter()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for i in range(n_e2e):
+            e2e_step(i)
+        g1.record(stream)
+        stream.synchronize()
+        e2e_wall = (time.perf_counter() - t0) / n_e2e
+        e2e_ms = max(g0.elapsed_time(g1) / n_e2e, 1e3 * e2e_wall)
+
+    # max over ranks
+    vals = torch.tensor([ms, ms32, e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+    ms, ms32, e2e_ms = [float(v) for v in vals.tolist()]
+    ms_step = ms / args.steps
+    value = world * args.steps / (ms / 1e3)
+
+    # roofline of the dominant kernel (block matching), from the live event times
+    bm = per_kernel.get("block_match", {"launches": 1, "ms": float("nan")})
+    px = sum((W >> i) * (H >> i) for i in range(wl.levels))
+    taps = 21 * 21
+    flop_per_tap = 50.0  # 8-D distance + norm 24, chroma 6, 2 weights 8, accumulate 10 (FMA = 2)
+    frames_prof = args.steps
+    bm_tflops = px * taps * flop_per_tap * frames_prof / (bm["ms"] / 1e3) / 1e12
+    sm_clock = clocks.get("sm_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * (sm_clock * 1e6) / 1e12  # SIMT FP32 FMA peak at the sampled clock
+    mufu_rate = 148 * 16 * (sm_clock * 1e6) / 1e12  # ex2 per SM per clock = 16
+    bm_mufu = px * taps * 2 * frames_prof / (bm["ms"] / 1e3) / 1e12
+    total_prof_ms = sum(v["ms"] for v in per_kernel.values())
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f16-storage/f32-math", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "frame": f"{W}x{H} RGGB 12-bit", "levels": wl.levels, "iso": wl.iso,
+                   "frames_rotated": N_ROTATE, "l2": "inputs + planes per frame > 126 MB L2 (6 rotating frames)",
+                   "parallelism": f"frames sharded over {world} rank(s)"},
+        "e2e": {"value": world / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": W * H * 2,
+                "d2h_bytes_per_step": W * H * 8},
+        "fp32_plain": {"value": world / (ms32 / 1e3), "unit": UNIT, "ms_per_frame": ms32,
+                       "note": "FP32 planes, per-level host PCA sync (the reference's structure)"},
+        "speedup_vs_fp32_plain": ms32 / ms_step,
+        "roofline": {"bound": "fp32+mufu", "kernel": "block_match",
+                     "achieved": bm_tflops, "peak": fp32_peak, "unit": "TFLOP/s", "frac": bm_tflops / fp32_peak,
+                     "mufu_frac": bm_mufu / mufu_rate, "traffic": None,
+                     "share": bm["ms"] / total_prof_ms if total_prof_ms else None,
+                     "ms_per_launch": bm["ms"] / max(1, bm["launches"]),
+                     "peak_note": "nominal SIMT FP32 (148 SMs x 128 lanes x 2 x sampled SM clock); "
+                                  "MEASURED_PEAKS has HBM and bf16-tensor peaks only"},
+        "per_kernel_ms_per_frame": {k: v["ms"] / frames_prof for k, v in per_kernel.items()},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(wl, scene.make_params, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    conv.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,167 @@
+"""GlassCamera raw-image path on B200 (sm_100a).
+
+Python mirror of the C ABI in include/glscam.h, loaded through ctypes from
+the in-tree ``libglscam.so``. The native library is the product; this
+module only binds it. There is no CPU fallback: if the library or a CUDA
+device is missing, calls fail with :class:`GlsError`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "libglscam.so"
+
+GLS_OK = 0
+GLS_ERR_INVALID_ARG = 1
+GLS_ERR_OOM = 2
+GLS_ERR_CUDA = 3
+GLS_ERR_TIMEOUT = 4
+GLS_ERR_DEGENERATE = 5
+GLS_ERR_UNSUPPORTED = 6
+GLS_ERR_RANGE = 7
+
+GRBG, GBRG, RGGB, BGGR = 0, 1, 2, 3
+MAX_LEVELS = 5
+F32, F16, U16 = 0, 1, 2
+
+DENOISE = 1 << 0
+POSTPROCESS = 1 << 1
+FP16_STORAGE = 1 << 2
+HOST_IO = 1 << 3
+SYNC = 1 << 4
+HOST_PCA = 1 << 5
+
+PLANE_SCALED_RAW = 0
+PLANE_GRADIENT = 1
+PLANE_DEMOSAIC = 2
+PLANE_DESPECKLED = 3
+PLANE_OUTPUT = 4
+PLANE_DENOISED_L0 = 8
+
+CAMERA_IPHONE14_WIDE = 0
+
+
+class DenoiseParams(C.Structure):
+    _fields_ = [(n, C.c_float) for n in
+                ("luma", "chroma", "chroma_boost", "gradient_boost", "gradient_threshold", "sharpening")]
+
+
+class YCbCrNLF(C.Structure):
+    _fields_ = [("a", C.c_float * 3), ("b", C.c_float * 3)]
+
+
+class RawNLF(C.Structure):
+    _fields_ = [("a", C.c_float * 4), ("b", C.c_float * 4)]
+
+
+class DemosaicParams(C.Structure):
+    _fields_ = [
+        ("bayer_pattern", C.c_int32),
+        ("black_level", C.c_float),
+        ("white_level", C.c_float),
+        ("exposure_multiplier", C.c_float),
+        ("lens_shading_correction", C.c_float),
+        ("scale_mul", C.c_float * 4),
+        ("rgb_cam", C.c_float * 9),
+        ("xyz_rgb", C.c_float * 9),
+        ("high_noise_image", C.c_int32),
+        ("raw_denoise_strength", C.c_float),
+        ("raw_nlf", RawNLF),
+        ("pyramid_nlf", YCbCrNLF * MAX_LEVELS),
+        ("denoise", DenoiseParams * MAX_LEVELS),
+        ("levels", C.c_int32),
+        ("iso", C.c_int32),
+    ]
+
+
+class ImageView(C.Structure):
+    _fields_ = [
+        ("data", C.c_void_p),
+        ("width", C.c_int32),
+        ("height", C.c_int32),
+        ("channels", C.c_int32),
+        ("dtype", C.c_int32),
+        ("stride_bytes", C.c_size_t),
+    ]
+
+
+class FrameDesc(C.Structure):
+    _fields_ = [
+        ("raw", C.c_void_p),
+        ("width", C.c_int32),
+        ("height", C.c_int32),
+        ("raw_stride_bytes", C.c_size_t),
+        ("params", C.POINTER(DemosaicParams)),
+        ("out", ImageView),
+    ]
+
+
+class KernelStat(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("launches", C.c_uint64), ("ms", C.c_double)]
+
+
+class GlsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"gls status {code}: {msg}")
+        self.code = code
+
+
+# every symbol include/glscam.h declares: name -> (restype, argtypes)
+_SIGNATURES = {
+    "gls_last_error_message": (C.c_char_p, []),
+    "gls_version": (C.c_char_p, []),
+    "gls_converter_create": (C.c_int, [C.c_int32, C.c_void_p, C.c_size_t, C.c_int32, C.POINTER(C.c_void_p)]),
+    "gls_converter_destroy": (C.c_int, [C.c_void_p]),
+    "gls_demosaic": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_size_t,
+                               C.POINTER(DemosaicParams), C.c_uint32, C.POINTER(ImageView), C.c_void_p]),
+    "gls_demosaic_batch": (C.c_int, [C.c_void_p, C.POINTER(FrameDesc), C.c_int32, C.c_uint32, C.c_void_p]),
+    "gls_pyramid_denoise": (C.c_int, [C.c_void_p, C.POINTER(ImageView), C.POINTER(ImageView),
+                                      C.POINTER(DemosaicParams), C.c_uint32, C.POINTER(ImageView), C.c_void_p]),
+    "gls_converter_plane": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(ImageView)]),
+    "gls_converter_pca_basis": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_float)]),
+    "gls_copy_view": (C.c_int, [C.POINTER(ImageView), C.POINTER(ImageView), C.c_int32, C.c_void_p]),
+    "gls_converter_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
+    "gls_converter_stats": (C.c_int, [C.c_void_p, C.POINTER(KernelStat), C.c_int32, C.POINTER(C.c_int32)]),
+    "gls_converter_reset_stats": (C.c_int, [C.c_void_p]),
+    "gls_calibration_fill": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(DemosaicParams)]),
+    "gls_gaussian_bilinear_taps": (C.c_int, [C.c_float, C.POINTER(C.c_float), C.c_int32, C.POINTER(C.c_int32)]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded native library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise GlsError(GLS_ERR_UNSUPPORTED,
+                           f"{LIB_PATH} is missing: build it with `python -m glasscamerapublic_b200.build`")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(code: int) -> None:
+    if code != GLS_OK:
+        msg = lib().gls_last_error_message().decode(errors="replace")
+        raise GlsError(code, msg)
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGNATURES)
+
+
+from .api import CameraCalibration, iPhone14WideCalibration, RawConverter, PyramidProcessor  # noqa: E402
+
+__all__ = [
+    "lib", "check", "GlsError", "DemosaicParams", "ImageView", "FrameDesc", "DenoiseParams",
+    "RawConverter", "PyramidProcessor", "CameraCalibration", "iPhone14WideCalibration",
+]

@@ -1,0 +1,763 @@
+// gls_capi.cu — the converter object and the extern "C" entry points of
+// include/glscam.h. The host sequence follows RawConverter::demosaic
+// (raw_converter.cpp:148-248) and PyramidProcessor<levels>::denoise
+// (pyramid_processor.cpp:96-172); the kernels are in gls_front.cu and
+// gls_pyramid.cu.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "gls_common.cuh"
+#include "gls_host.h"
+#include "gls_kernels.h"
+
+namespace gls {
+
+static thread_local std::string g_last_error;
+
+gls_status set_error(gls_status code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+void clear_error() { g_last_error.clear(); }
+
+#define GLS_CUDA(...)                                                                                   \
+    do {                                                                                                \
+        cudaError_t e_ = (__VA_ARGS__);                                                                     \
+        if (e_ != cudaSuccess)                                                                          \
+            return set_error(e_ == cudaErrorMemoryAllocation ? GLS_ERR_OOM : GLS_ERR_CUDA, "%s: %s (%s:%d)", \
+                             #__VA_ARGS__, cudaGetErrorString(e_), __FILE__, __LINE__);                        \
+    } while (0)
+
+#define GLS_TRY(...)                     \
+    do {                                 \
+        gls_status s_ = (__VA_ARGS__);   \
+        if (s_ != GLS_OK) return s_;     \
+    } while (0)
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    gls_status ensure(size_t b) {
+        if (b <= bytes) return GLS_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return set_error(GLS_ERR_OOM, "cudaMalloc(%zu) failed: %s", b, cudaGetErrorString(e));
+        }
+        bytes = b;
+        return GLS_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+};
+
+template <class S, int C>
+static Plane<S, C> plane(DevBuf& b, int w, int h) {
+    return Plane<S, C>{reinterpret_cast<S*>(b.p), w, h, size_t(w) * C};
+}
+
+// Device state of one storage type: every plane of RawConverter and
+// PyramidProcessor (raw_converter.hpp:84-104, pyramid_processor.hpp:42-48).
+template <class S>
+struct Pipeline {
+    int W = 0, H = 0, L = 0;
+    DevBuf raw, scaled, grad, quad, A, B, pca, acc, basis, status;
+    DevBuf img[GLS_MAX_LEVELS], gradp[GLS_MAX_LEVELS], sub[GLS_MAX_LEVELS], den[GLS_MAX_LEVELS];
+    DevBuf out_f32, out_f16, stage_in, stage_grad;
+    std::vector<double> host_acc;
+    std::vector<float> host_basis;
+
+    gls_status ensure(int w, int h, int levels) {
+        const size_t n = size_t(w) * h;
+        GLS_TRY(raw.ensure(n * sizeof(uint16_t)));
+        GLS_TRY(scaled.ensure(n * sizeof(S)));
+        GLS_TRY(grad.ensure(n * 2 * sizeof(S)));
+        GLS_TRY(quad.ensure((n / 4 + 1) * 4 * sizeof(S)));
+        GLS_TRY(A.ensure(n * 4 * sizeof(S)));
+        GLS_TRY(B.ensure(n * 4 * sizeof(S)));
+        GLS_TRY(pca.ensure(n * 8 * sizeof(S)));
+        GLS_TRY(acc.ensure(sizeof(double) * kPcaAcc * GLS_MAX_LEVELS));
+        GLS_TRY(basis.ensure(sizeof(float) * 200 * GLS_MAX_LEVELS));
+        GLS_TRY(status.ensure(sizeof(int) * GLS_MAX_LEVELS));
+        for (int i = 0; i < levels; i++) {
+            const size_t ni = size_t(w >> i) * (h >> i);
+            if (i > 0) {
+                GLS_TRY(img[i].ensure(ni * 4 * sizeof(S)));
+                GLS_TRY(gradp[i].ensure(ni * 2 * sizeof(S)));
+            }
+            GLS_TRY(sub[i].ensure(ni * 4 * sizeof(S)));
+            GLS_TRY(den[i].ensure(ni * 4 * sizeof(S)));
+        }
+        W = w;
+        H = h;
+        L = levels;
+        return GLS_OK;
+    }
+    void release() {
+        for (DevBuf* b : {&raw, &scaled, &grad, &quad, &A, &B, &pca, &acc, &basis, &status, &out_f32, &out_f16,
+                          &stage_in, &stage_grad})
+            b->release();
+        for (int i = 0; i < GLS_MAX_LEVELS; i++) {
+            img[i].release();
+            gradp[i].release();
+            sub[i].release();
+            den[i].release();
+        }
+    }
+};
+
+}  // namespace gls
+
+using namespace gls;
+
+namespace gls {
+// kernel classes for launch accounting
+enum KernelClass {
+    KC_SCALE, KC_SOBEL_BLUR, KC_RAW_DENOISE, KC_DEMOSAIC, KC_DESPECKLE, KC_DOWNSAMPLE, KC_SUBTRACT,
+    KC_PCA_COV, KC_PCA_EIGEN, KC_PCA_PROJECT, KC_BLOCK_MATCH, KC_OUTPUT, KC_VIEW_IN, KC_COUNT
+};
+static const char* const kKcNames[KC_COUNT] = {
+    "scale_raw", "sobel_blur", "raw_quad_denoise", "demosaic", "despeckle", "downsample", "subtract_noise",
+    "pca_cov", "pca_eigen", "pca_project", "block_match", "output_transform", "view_in"};
+
+struct Prof {
+    bool on = false;
+    uint64_t launches[KC_COUNT] = {};
+    double ms[KC_COUNT] = {};
+    struct Pending {
+        int kc;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> pool;
+    cudaEvent_t get() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void drain() {  // device must be synchronised
+        for (auto& p : pending) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, p.a, p.b) == cudaSuccess) ms[p.kc] += t;
+            pool.push_back(p.a);
+            pool.push_back(p.b);
+        }
+        pending.clear();
+    }
+    ~Prof() {
+        for (auto& p : pending) {
+            cudaEventDestroy(p.a);
+            cudaEventDestroy(p.b);
+        }
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
+// Counts the launches of one kernel class and, when profiling, brackets
+// them with events on the launch stream.
+struct KScope {
+    Prof& pr;
+    int kc;
+    cudaStream_t s;
+    cudaEvent_t a = nullptr;
+    KScope(Prof& p, int k, cudaStream_t st, int n = 1) : pr(p), kc(k), s(st) {
+        pr.launches[kc] += n;
+        if (pr.on) {
+            a = pr.get();
+            cudaEventRecord(a, s);
+        }
+    }
+    ~KScope() {
+        if (pr.on) {
+            cudaEvent_t b = pr.get();
+            cudaEventRecord(b, s);
+            pr.pending.push_back({kc, a, b});
+        }
+    }
+};
+}  // namespace gls
+
+struct gls_converter {
+    int device = 0;
+    Prof prof;
+    Pipeline<float> p32;
+    Pipeline<__half> p16;
+    int last_storage = -1;  // GLS_F32 / GLS_F16 of the last call
+    int last_levels = 0;
+    int last_w = 0, last_h = 0;
+    bool last_denoise = false;
+};
+
+namespace gls {
+
+// ---- view conversion kernels (caller views <-> internal planes)
+template <class I, class S, int C>
+__global__ void k_view_in(const I* __restrict__ src, size_t pitch, Plane<S, C> dst) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= dst.w || y >= dst.h) return;
+    const I* s = src + size_t(y) * pitch + size_t(x) * C;
+    S* d = dst.px(x, y);
+#pragma unroll
+    for (int c = 0; c < C; c++) d[c] = from_f<S>(to_f(s[c]));
+}
+
+template <class S, int C>
+static gls_status view_to_plane(const gls_image_view* v, bool host_io, DevBuf& stage, Plane<S, C> dst, cudaStream_t s) {
+    if (v->channels != C) return set_error(GLS_ERR_INVALID_ARG, "view has %d channels, expected %d", v->channels, C);
+    if (v->dtype != GLS_F32 && v->dtype != GLS_F16) return set_error(GLS_ERR_INVALID_ARG, "view dtype must be F32 or F16");
+    const size_t es = v->dtype == GLS_F32 ? 4 : 2;
+    const size_t row = size_t(v->width) * C * es;
+    if (v->stride_bytes < row || v->stride_bytes % es) return set_error(GLS_ERR_INVALID_ARG, "bad view stride");
+    const void* src = v->data;
+    size_t pitch = v->stride_bytes / es;
+    if (host_io) {
+        GLS_TRY(stage.ensure(row * v->height));
+        GLS_CUDA(cudaMemcpy2DAsync(stage.p, row, v->data, v->stride_bytes, row, v->height, cudaMemcpyHostToDevice, s));
+        src = stage.p;
+        pitch = size_t(v->width) * C;
+    }
+    dim3 b(32, 8), g((dst.w + 31) / 32, (dst.h + 7) / 8);
+    if (v->dtype == GLS_F32) k_view_in<float, S, C><<<g, b, 0, s>>>(static_cast<const float*>(src), pitch, dst);
+    else k_view_in<__half, S, C><<<g, b, 0, s>>>(static_cast<const __half*>(src), pitch, dst);
+    GLS_CUDA(cudaGetLastError());
+    return GLS_OK;
+}
+
+static gls_status check_params(const gls_demosaic_params* p, int w, int h) {
+    if (!p) return set_error(GLS_ERR_INVALID_ARG, "params is NULL");
+    if (p->bayer_pattern < 0 || p->bayer_pattern > 3) return set_error(GLS_ERR_INVALID_ARG, "bad bayer_pattern %d", p->bayer_pattern);
+    if (p->levels < 1 || p->levels > GLS_MAX_LEVELS) return set_error(GLS_ERR_INVALID_ARG, "levels must be 1..5 (got %d)", p->levels);
+    if (w < 4 || h < 4 || (w & 1) || (h & 1))
+        return set_error(GLS_ERR_INVALID_ARG, "image must be at least 4x4 with even width and height (got %dx%d)", w, h);
+    if ((w >> (p->levels - 1)) < 1 || (h >> (p->levels - 1)) < 1)
+        return set_error(GLS_ERR_INVALID_ARG, "image %dx%d too small for %d pyramid levels", w, h, p->levels);
+    if (!(p->white_level > p->black_level)) return set_error(GLS_ERR_INVALID_ARG, "white_level must exceed black_level");
+    return GLS_OK;
+}
+
+// Output of the final stage: either the caller's buffer (device, or host
+// through the converter's internal plane) or the converter's own plane.
+template <class O>
+struct OutTarget {
+    Plane<O, 4> plane;
+    bool copy_to_host = false;
+    void* host = nullptr;
+    size_t host_stride = 0;
+};
+
+template <class S>
+static gls_status pyramid_run(gls_converter* cv, Pipeline<S>& P, Plane<S, 4> img0, Plane<S, 2> grad0,
+                              const gls_demosaic_params* p, uint32_t flags, cudaStream_t s) {
+    const int L = p->levels;
+    const int W = img0.w, H = img0.h;
+    Plane<S, 4> img[GLS_MAX_LEVELS];
+    Plane<S, 2> grd[GLS_MAX_LEVELS];
+    img[0] = img0;
+    grd[0] = grad0;
+    for (int i = 1; i < L; i++) {  // Gaussian pyramid, pyramid_processor.cpp:103-120
+        img[i] = plane<S, 4>(P.img[i], W >> i, H >> i);
+        grd[i] = plane<S, 2>(P.gradp[i], W >> i, H >> i);
+        KScope k(cv->prof, KC_DOWNSAMPLE, s, 2);
+        launch_downsample<S, 4>(img[i - 1], img[i], s);
+        launch_downsample<S, 2>(grd[i - 1], grd[i], s);
+    }
+    double* acc = static_cast<double*>(P.acc.p);
+    float* basis = static_cast<float*>(P.basis.p);
+    int* status = static_cast<int*>(P.status.p);
+    for (int i = L - 1; i >= 0; i--) {  // coarse to fine, pyramid_processor.cpp:123-168
+        const gls_denoise_params& dp = p->denoise[i];
+        const int wi = W >> i, hi = H >> i;
+        Plane<S, 4> layer = img[i];
+        if (i < L - 1) {
+            SubtractArgs sa;
+            sa.luma_weight = 1.f;  // lumaDenoiseWeight, pyramid_processor.cpp:93
+            sa.sharpening = dp.sharpening;
+            sa.nlf_a = p->pyramid_nlf[i].a[0] * dp.luma;
+            sa.nlf_b = p->pyramid_nlf[i].b[0] * dp.luma;
+            layer = plane<S, 4>(P.sub[i], wi, hi);
+            KScope k(cv->prof, KC_SUBTRACT, s);
+            launch_subtract_noise<S>(img[i], img[i + 1], plane<S, 4>(P.den[i + 1], W >> (i + 1), H >> (i + 1)), grd[i],
+                                     layer, sa, s);
+        }
+        const int n_patches = (wi / 8) * (hi / 8);
+        {
+            KScope k(cv->prof, KC_PCA_COV, s, n_patches > 0 ? 1 : 0);
+            launch_pca_cov<S>(layer, acc + i * kPcaAcc, s);
+        }
+        if (flags & GLS_HOST_PCA) {
+            P.host_acc.resize(kPcaAcc);
+            P.host_basis.resize(200);
+            GLS_CUDA(cudaMemcpyAsync(P.host_acc.data(), acc + i * kPcaAcc, sizeof(double) * kPcaAcc,
+                                     cudaMemcpyDeviceToHost, s));
+            GLS_CUDA(cudaStreamSynchronize(s));  // the reference's per-level wait, pyramid_processor.cpp:148
+            host_pca_basis(P.host_acc.data(), n_patches, P.host_basis.data());
+            GLS_CUDA(cudaMemcpyAsync(basis + i * 200, P.host_basis.data(), sizeof(float) * 200,
+                                     cudaMemcpyHostToDevice, s));
+            GLS_CUDA(cudaStreamSynchronize(s));
+        } else {
+            KScope k(cv->prof, KC_PCA_EIGEN, s);
+            launch_pca_eigen(acc + i * kPcaAcc, n_patches, basis + i * 200, status + i, s);
+        }
+        Plane<S, 8> pcap = plane<S, 8>(P.pca, wi, hi);
+        {
+            KScope k(cv->prof, KC_PCA_PROJECT, s);
+            launch_pca_project<S>(layer, basis + i * 200, pcap, s);
+        }
+        BlockMatchArgs ba;
+        for (int c = 0; c < 3; c++) {
+            ba.var_a[c] = p->pyramid_nlf[i].a[c];
+            ba.var_b[c] = p->pyramid_nlf[i].b[c];
+        }
+        ba.tm[0] = dp.luma;
+        ba.tm[1] = dp.chroma;
+        ba.tm[2] = dp.chroma;
+        ba.chroma_boost = dp.chroma_boost;
+        ba.gradient_boost = dp.gradient_boost;
+        ba.gradient_threshold = dp.gradient_threshold;
+        ba.lsc = p->lens_shading_correction;
+        KScope k(cv->prof, KC_BLOCK_MATCH, s);
+        launch_block_match<S>(layer, grd[i], pcap, plane<S, 4>(P.den[i], wi, hi), ba, s);
+    }
+    GLS_CUDA(cudaGetLastError());
+    cv->last_levels = L;
+    return GLS_OK;
+}
+
+template <class S, class O>
+static gls_status finish_output(gls_converter* cv, Plane<S, 4> src, bool transform, const float* m, OutTarget<O>& t,
+                                cudaStream_t s) {
+    KScope k(cv->prof, KC_OUTPUT, s);
+    if (transform) {
+        Mat3Args ma;
+        std::memcpy(ma.m, m, sizeof(ma.m));
+        launch_transform<S, O>(src, t.plane, ma, s);
+    } else {
+        launch_convert4<S, O>(src, t.plane, s);
+    }
+    GLS_CUDA(cudaGetLastError());
+    if (t.copy_to_host) {
+        const size_t row = size_t(t.plane.w) * 4 * sizeof(O);
+        GLS_CUDA(cudaMemcpy2DAsync(t.host, t.host_stride, t.plane.p, t.plane.pitch * sizeof(O), row, t.plane.h,
+                                   cudaMemcpyDeviceToHost, s));
+    }
+    return GLS_OK;
+}
+
+template <class S, class O>
+static gls_status make_target(Pipeline<S>& P, gls_image_view* out, int w, int h, bool host_io, OutTarget<O>& t) {
+    DevBuf& own = sizeof(O) == 4 ? P.out_f32 : P.out_f16;
+    if (!out->data || host_io) {
+        GLS_TRY(own.ensure(size_t(w) * h * 4 * sizeof(O)));
+        t.plane = plane<O, 4>(own, w, h);
+        if (out->data) {
+            t.copy_to_host = true;
+            t.host = out->data;
+            t.host_stride = out->stride_bytes ? out->stride_bytes : size_t(w) * 4 * sizeof(O);
+            if (t.host_stride < size_t(w) * 4 * sizeof(O)) return set_error(GLS_ERR_INVALID_ARG, "output stride too small");
+        } else {
+            out->data = own.p;
+            out->width = w;
+            out->height = h;
+            out->channels = 4;
+            out->stride_bytes = size_t(w) * 4 * sizeof(O);
+        }
+    } else {
+        const size_t stride = out->stride_bytes ? out->stride_bytes : size_t(w) * 4 * sizeof(O);
+        if (stride % (4 * sizeof(O)) || stride < size_t(w) * 4 * sizeof(O) || (uintptr_t(out->data) % (4 * sizeof(O))))
+            return set_error(GLS_ERR_INVALID_ARG, "device output must be %zu-byte aligned with a matching stride",
+                             4 * sizeof(O));
+        t.plane = Plane<O, 4>{static_cast<O*>(out->data), w, h, stride / sizeof(O)};
+    }
+    return GLS_OK;
+}
+
+template <class S>
+static gls_status demosaic_run(gls_converter* cv, const uint16_t* raw, int w, int h, size_t stride_bytes,
+                               const gls_demosaic_params* p, uint32_t flags, gls_image_view* out, cudaStream_t s) {
+    Pipeline<S>& P = *reinterpret_cast<Pipeline<S>*>(is_half<S>::value ? (void*)&cv->p16 : (void*)&cv->p32);
+    const bool host_io = flags & GLS_HOST_IO;
+    const bool denoise = flags & GLS_DENOISE;
+    GLS_TRY(P.ensure(w, h, p->levels));
+
+    // raw input
+    const uint16_t* rawp = raw;
+    size_t raw_pitch = stride_bytes / 2;
+    if (host_io) {
+        GLS_CUDA(cudaMemcpy2DAsync(P.raw.p, size_t(w) * 2, raw, stride_bytes, size_t(w) * 2, h,
+                                   cudaMemcpyHostToDevice, s));
+        rawp = static_cast<const uint16_t*>(P.raw.p);
+        raw_pitch = size_t(w);
+    } else if ((uintptr_t(raw) & 3) || (stride_bytes & 3)) {
+        return set_error(GLS_ERR_INVALID_ARG, "device raw input must be 4-byte aligned with a 4-byte multiple stride");
+    }
+
+    Plane<S, 1> scaled = plane<S, 1>(P.scaled, w, h);
+    Plane<S, 2> grad = plane<S, 2>(P.grad, w, h);
+
+    // scaleRawData, raw_converter.cpp:179-183
+    ScaleArgs sa;
+    sa.pattern = p->bayer_pattern;
+    sa.black = int(lroundf(p->black_level));
+    for (int c = 0; c < 4; c++) sa.k[c] = float(double(p->scale_mul[c]) * 0.9 / 65535.0);
+    sa.lsc = p->lens_shading_correction;
+    sa.cx = float(w / 2);
+    sa.cy = float(h / 2);
+    {
+        volatile float cx2 = sa.cx * sa.cx, cy2 = sa.cy * sa.cy;
+        volatile float ss = cx2 + cy2;
+        sa.clen = sqrtf(ss);
+    }
+    {
+        KScope k(cv->prof, KC_SCALE, s);
+        launch_scale_raw<S>(rawp, raw_pitch, scaled, sa, s);
+    }
+
+    // rawImageSobel + sampledConvolutionSobel, raw_converter.cpp:185-193
+    BlurArgs ba;
+    float taps[3 * kMaxTaps];
+    const int n1 = gaussian_taps(1.5f, taps, kMaxTaps);
+    const int n2 = gaussian_taps(4.5f, taps + 3 * n1, kMaxTaps - n1);
+    if (n1 <= 0 || n2 <= 0) return set_error(GLS_ERR_INVALID_ARG, "blur tap table overflow");
+    ba.n1 = n1;
+    ba.n2 = n2;
+    for (int t = 0; t < n1 + n2; t++) {
+        ba.w[t] = taps[3 * t];
+        const float fdx = floorf(taps[3 * t + 1]), fdy = floorf(taps[3 * t + 2]);
+        ba.ix[t] = int(fdx);
+        ba.iy[t] = int(fdy);
+        ba.fx[t] = taps[3 * t + 1] - fdx;
+        ba.fy[t] = taps[3 * t + 2] - fdy;
+    }
+    // getRawVariance, demosaic.hpp:186-193
+    const float rv0 = p->raw_nlf.a[0], rv1 = p->raw_nlf.b[0];
+    const float gv0 = (p->raw_nlf.a[1] + p->raw_nlf.a[3]) / 2, gv1 = (p->raw_nlf.b[1] + p->raw_nlf.b[3]) / 2;
+    const float bv0 = p->raw_nlf.a[2], bv1 = p->raw_nlf.b[2];
+    ba.var0 = gv0;
+    ba.var1 = gv1;
+    ba.inv_sqrt45 = 1.0f / sqrtf(4.5f);
+    {
+        KScope k(cv->prof, KC_SOBEL_BLUR, s);
+        launch_sobel_blur<S>(scaled, grad, ba, s);
+    }
+
+    // high-noise raw branch, raw_converter.cpp:195-202
+    if (denoise && p->high_noise_image) {
+        RawDenoiseArgs ra;
+        ra.pattern = p->bayer_pattern;
+        for (int c = 0; c < 4; c++) ra.var[c] = p->raw_nlf.b[c];
+        ra.strength = p->raw_denoise_strength;
+        ra.fast = is_half<S>::value ? 1 : 0;
+        KScope k(cv->prof, KC_RAW_DENOISE, s, 2);
+        launch_raw_denoise<S>(scaled, grad, plane<S, 4>(P.quad, w / 2, h / 2), ra, s);
+    }
+
+    // demosaic + blendHighlights (+ cam -> YCbCr), raw_converter.cpp:204-214
+    float c2y[9], y2c[9];
+    cam_ycbcr(p->rgb_cam, p->xyz_rgb, c2y, y2c);
+    DemosaicArgs da;
+    da.pattern = p->bayer_pattern;
+    da.rv0 = rv0; da.rv1 = rv1; da.gv0 = gv0; da.gv1 = gv1; da.bv0 = bv0; da.bv1 = bv1;
+    da.transform = denoise ? 1 : 0;
+    std::memcpy(da.m, c2y, sizeof(c2y));
+    Plane<S, 4> A = plane<S, 4>(P.A, w, h);
+    {
+        KScope k(cv->prof, KC_DEMOSAIC, s);
+        launch_demosaic<S>(scaled, grad, A, da, s);
+    }
+    GLS_CUDA(cudaGetLastError());
+
+    Plane<S, 4> final_src = A;
+    if (denoise) {
+        // RawConverter::denoise, raw_converter.cpp:70-116
+        Plane<S, 4> B = plane<S, 4>(P.B, w, h);
+        {
+            KScope k(cv->prof, KC_DESPECKLE, s);
+            launch_despeckle<S>(A, B, p->pyramid_nlf[0].a[0], p->pyramid_nlf[0].b[0], s);
+        }
+        GLS_TRY(pyramid_run<S>(cv, P, B, grad, p, flags, s));
+        final_src = plane<S, 4>(P.den[0], w, h);
+    }
+    // transformImage(YCbCr -> cam), raw_converter.cpp:219
+    if (out->dtype == GLS_F16) {
+        OutTarget<__half> t;
+        GLS_TRY(make_target<S, __half>(P, out, w, h, host_io, t));
+        GLS_TRY(finish_output<S, __half>(cv, final_src, denoise, y2c, t, s));
+    } else {
+        out->dtype = GLS_F32;
+        OutTarget<float> t;
+        GLS_TRY(make_target<S, float>(P, out, w, h, host_io, t));
+        GLS_TRY(finish_output<S, float>(cv, final_src, denoise, y2c, t, s));
+    }
+    cv->last_storage = is_half<S>::value ? GLS_F16 : GLS_F32;
+    cv->last_w = w;
+    cv->last_h = h;
+    cv->last_denoise = denoise;
+    if (host_io || (flags & GLS_SYNC)) GLS_CUDA(cudaStreamSynchronize(s));
+    return GLS_OK;
+}
+
+template <class S>
+static gls_status pyramid_only(gls_converter* cv, const gls_image_view* ycc, const gls_image_view* gradient,
+                               const gls_demosaic_params* p, uint32_t flags, gls_image_view* out, cudaStream_t s) {
+    Pipeline<S>& P = *reinterpret_cast<Pipeline<S>*>(is_half<S>::value ? (void*)&cv->p16 : (void*)&cv->p32);
+    const int w = ycc->width, h = ycc->height;
+    const bool host_io = flags & GLS_HOST_IO;
+    GLS_TRY(P.ensure(w, h, p->levels));
+    Plane<S, 4> B = plane<S, 4>(P.B, w, h);
+    Plane<S, 2> grad = plane<S, 2>(P.grad, w, h);
+    {
+        KScope k(cv->prof, KC_VIEW_IN, s, 2);
+        GLS_TRY(view_to_plane<S, 4>(ycc, host_io, P.stage_in, B, s));
+        GLS_TRY(view_to_plane<S, 2>(gradient, host_io, P.stage_grad, grad, s));
+    }
+    GLS_TRY(pyramid_run<S>(cv, P, B, grad, p, flags, s));
+    Plane<S, 4> den0 = plane<S, 4>(P.den[0], w, h);
+    if (out->dtype == GLS_F16) {
+        OutTarget<__half> t;
+        GLS_TRY(make_target<S, __half>(P, out, w, h, host_io, t));
+        GLS_TRY(finish_output<S, __half>(cv, den0, false, nullptr, t, s));
+    } else {
+        out->dtype = GLS_F32;
+        OutTarget<float> t;
+        GLS_TRY(make_target<S, float>(P, out, w, h, host_io, t));
+        GLS_TRY(finish_output<S, float>(cv, den0, false, nullptr, t, s));
+    }
+    cv->last_storage = is_half<S>::value ? GLS_F16 : GLS_F32;
+    cv->last_w = w;
+    cv->last_h = h;
+    cv->last_denoise = true;
+    if (host_io || (flags & GLS_SYNC)) GLS_CUDA(cudaStreamSynchronize(s));
+    return GLS_OK;
+}
+
+}  // namespace gls
+
+// ============================================================== C ABI
+extern "C" {
+
+const char* gls_last_error_message(void) { return g_last_error.c_str(); }
+
+const char* gls_version(void) {
+    return "glscam 0.1 (sm_100a; demosaic, pyramid PCA block-matching denoise)";
+}
+
+gls_status gls_converter_create(int32_t device, const uint8_t* icc, size_t icc_len, int32_t calibrate_from_image,
+                                gls_converter** out) {
+    clear_error();
+    if (!out) return set_error(GLS_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    if (icc && icc_len)
+        return set_error(GLS_ERR_UNSUPPORTED, "ICC profiles are not part of this path; pass xyz_rgb in the parameters");
+    if (calibrate_from_image)
+        return set_error(GLS_ERR_UNSUPPORTED, "calibrateFromImage (noise measurement) is not part of this path");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || device < 0 || device >= n)
+        return set_error(GLS_ERR_CUDA, "no CUDA device %d (%s)", device, e != cudaSuccess ? cudaGetErrorString(e) : "out of range");
+    gls_converter* c = new (std::nothrow) gls_converter();
+    if (!c) return set_error(GLS_ERR_OOM, "host allocation failed");
+    c->device = device;
+    *out = c;
+    return GLS_OK;
+}
+
+gls_status gls_converter_destroy(gls_converter* conv) {
+    clear_error();
+    if (!conv) return GLS_OK;
+    cudaSetDevice(conv->device);
+    conv->p32.release();
+    conv->p16.release();
+    delete conv;
+    return GLS_OK;
+}
+
+gls_status gls_demosaic(gls_converter* conv, const uint16_t* raw, int32_t width, int32_t height,
+                        size_t raw_stride_bytes, const gls_demosaic_params* params, uint32_t flags,
+                        gls_image_view* out, void* stream) {
+    clear_error();
+    if (!conv || !raw || !out) return set_error(GLS_ERR_INVALID_ARG, "converter, raw and out must not be NULL");
+    if (flags & GLS_POSTPROCESS)
+        return set_error(GLS_ERR_UNSUPPORTED, "sRGB post-processing is not part of this path (linear camera RGB only)");
+    GLS_TRY(check_params(params, width, height));
+    if (raw_stride_bytes == 0) raw_stride_bytes = size_t(width) * 2;
+    if (raw_stride_bytes < size_t(width) * 2) return set_error(GLS_ERR_INVALID_ARG, "raw stride too small");
+    if (out->dtype != GLS_F32 && out->dtype != GLS_F16) return set_error(GLS_ERR_INVALID_ARG, "output dtype must be F32 or F16");
+    GLS_CUDA(cudaSetDevice(conv->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (flags & GLS_FP16_STORAGE)
+        return demosaic_run<__half>(conv, raw, width, height, raw_stride_bytes, params, flags, out, s);
+    return demosaic_run<float>(conv, raw, width, height, raw_stride_bytes, params, flags, out, s);
+}
+
+gls_status gls_demosaic_batch(gls_converter* conv, gls_frame_desc* frames, int32_t n_frames, uint32_t flags,
+                              void* stream) {
+    clear_error();
+    if (!conv || (!frames && n_frames > 0) || n_frames < 0) return set_error(GLS_ERR_INVALID_ARG, "bad batch");
+    for (int i = 0; i < n_frames; i++) {
+        gls_status st = gls_demosaic(conv, frames[i].raw, frames[i].width, frames[i].height,
+                                     frames[i].raw_stride_bytes, frames[i].params, flags & ~GLS_SYNC, &frames[i].out,
+                                     stream);
+        if (st != GLS_OK) return st;
+    }
+    if (flags & GLS_SYNC) GLS_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    return GLS_OK;
+}
+
+gls_status gls_pyramid_denoise(gls_converter* conv, const gls_image_view* ycc, const gls_image_view* gradient,
+                               const gls_demosaic_params* params, uint32_t flags, gls_image_view* out, void* stream) {
+    clear_error();
+    if (!conv || !ycc || !gradient || !out || !ycc->data || !gradient->data)
+        return set_error(GLS_ERR_INVALID_ARG, "NULL argument");
+    if (!params) return set_error(GLS_ERR_INVALID_ARG, "params is NULL");
+    if (params->levels < 1 || params->levels > GLS_MAX_LEVELS) return set_error(GLS_ERR_INVALID_ARG, "levels must be 1..5");
+    if (gradient->width != ycc->width || gradient->height != ycc->height)
+        return set_error(GLS_ERR_INVALID_ARG, "gradient and image sizes differ");
+    if (ycc->width < 1 || ycc->height < 1 || (ycc->width >> (params->levels - 1)) < 1 ||
+        (ycc->height >> (params->levels - 1)) < 1)
+        return set_error(GLS_ERR_INVALID_ARG, "image too small for the pyramid");
+    if (out->dtype != GLS_F32 && out->dtype != GLS_F16) return set_error(GLS_ERR_INVALID_ARG, "output dtype must be F32 or F16");
+    GLS_CUDA(cudaSetDevice(conv->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (flags & GLS_FP16_STORAGE) return pyramid_only<__half>(conv, ycc, gradient, params, flags, out, s);
+    return pyramid_only<float>(conv, ycc, gradient, params, flags, out, s);
+}
+
+gls_status gls_converter_plane(gls_converter* conv, int32_t which, gls_image_view* view) {
+    clear_error();
+    if (!conv || !view) return set_error(GLS_ERR_INVALID_ARG, "NULL argument");
+    if (conv->last_storage < 0) return set_error(GLS_ERR_INVALID_ARG, "no frame has been processed");
+    const bool h = conv->last_storage == GLS_F16;
+    const int w = conv->last_w, hh = conv->last_h;
+    const size_t es = h ? 2 : 4;
+    auto pick = [&](DevBuf& b16, DevBuf& b32) { return h ? b16.p : b32.p; };
+    view->dtype = h ? GLS_F16 : GLS_F32;
+    switch (which) {
+        case GLS_PLANE_SCALED_RAW:
+            *view = {pick(conv->p16.scaled, conv->p32.scaled), w, hh, 1, view->dtype, size_t(w) * es};
+            return GLS_OK;
+        case GLS_PLANE_GRADIENT:
+            *view = {pick(conv->p16.grad, conv->p32.grad), w, hh, 2, view->dtype, size_t(w) * 2 * es};
+            return GLS_OK;
+        case GLS_PLANE_DEMOSAIC:
+        case GLS_PLANE_OUTPUT:
+            if (which == GLS_PLANE_DEMOSAIC || !conv->last_denoise) {
+                *view = {pick(conv->p16.A, conv->p32.A), w, hh, 4, view->dtype, size_t(w) * 4 * es};
+                return GLS_OK;
+            }
+            return set_error(GLS_ERR_INVALID_ARG, "the denoised output lives in the caller's view");
+        case GLS_PLANE_DESPECKLED:
+            *view = {pick(conv->p16.B, conv->p32.B), w, hh, 4, view->dtype, size_t(w) * 4 * es};
+            return GLS_OK;
+        default:
+            if (which >= GLS_PLANE_DENOISED_L0 && which < GLS_PLANE_DENOISED_L0 + conv->last_levels) {
+                const int l = which - GLS_PLANE_DENOISED_L0;
+                *view = {pick(conv->p16.den[l], conv->p32.den[l]), w >> l, hh >> l, 4, view->dtype,
+                         size_t(w >> l) * 4 * es};
+                return GLS_OK;
+            }
+            return set_error(GLS_ERR_INVALID_ARG, "unknown plane %d", which);
+    }
+}
+
+gls_status gls_converter_pca_basis(gls_converter* conv, int32_t level, float* basis25x8) {
+    clear_error();
+    if (!conv || !basis25x8) return set_error(GLS_ERR_INVALID_ARG, "NULL argument");
+    if (conv->last_storage < 0 || level < 0 || level >= conv->last_levels)
+        return set_error(GLS_ERR_INVALID_ARG, "no PCA basis for level %d", level);
+    GLS_CUDA(cudaSetDevice(conv->device));
+    const float* b = static_cast<const float*>(conv->last_storage == GLS_F16 ? conv->p16.basis.p : conv->p32.basis.p);
+    GLS_CUDA(cudaDeviceSynchronize());
+    GLS_CUDA(cudaMemcpy(basis25x8, b + level * 200, sizeof(float) * 200, cudaMemcpyDeviceToHost));
+    return GLS_OK;
+}
+
+gls_status gls_copy_view(const gls_image_view* src, gls_image_view* dst, int32_t direction, void* stream) {
+    clear_error();
+    if (!src || !dst || !src->data || !dst->data) return set_error(GLS_ERR_INVALID_ARG, "NULL view");
+    if (src->width != dst->width || src->height != dst->height || src->channels != dst->channels ||
+        src->dtype != dst->dtype)
+        return set_error(GLS_ERR_INVALID_ARG, "views differ in shape or dtype");
+    const size_t es = src->dtype == GLS_F32 ? 4 : 2;
+    const size_t row = size_t(src->width) * src->channels * es;
+    if (src->stride_bytes < row || dst->stride_bytes < row) return set_error(GLS_ERR_INVALID_ARG, "stride too small");
+    cudaMemcpyKind kind = direction == GLS_COPY_D2H   ? cudaMemcpyDeviceToHost
+                          : direction == GLS_COPY_D2D ? cudaMemcpyDeviceToDevice
+                                                      : cudaMemcpyHostToDevice;
+    if (direction < 0 || direction > 2) return set_error(GLS_ERR_INVALID_ARG, "bad direction");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    GLS_CUDA(cudaMemcpy2DAsync(dst->data, dst->stride_bytes, src->data, src->stride_bytes, row, src->height, kind, s));
+    if (direction == GLS_COPY_D2H) GLS_CUDA(cudaStreamSynchronize(s));
+    return GLS_OK;
+}
+
+gls_status gls_converter_set_profiling(gls_converter* conv, int32_t enable) {
+    clear_error();
+    if (!conv) return set_error(GLS_ERR_INVALID_ARG, "NULL converter");
+    GLS_CUDA(cudaSetDevice(conv->device));
+    if (conv->prof.on && !enable) {
+        GLS_CUDA(cudaDeviceSynchronize());
+        conv->prof.drain();
+    }
+    conv->prof.on = enable != 0;
+    return GLS_OK;
+}
+
+gls_status gls_converter_stats(gls_converter* conv, gls_kernel_stat* stats, int32_t max_stats, int32_t* n_stats) {
+    clear_error();
+    if (!conv || !n_stats) return set_error(GLS_ERR_INVALID_ARG, "NULL argument");
+    GLS_CUDA(cudaSetDevice(conv->device));
+    GLS_CUDA(cudaDeviceSynchronize());
+    conv->prof.drain();
+    *n_stats = KC_COUNT;
+    for (int i = 0; i < KC_COUNT && i < max_stats && stats; i++)
+        stats[i] = {kKcNames[i], conv->prof.launches[i], conv->prof.ms[i]};
+    return GLS_OK;
+}
+
+gls_status gls_converter_reset_stats(gls_converter* conv) {
+    clear_error();
+    if (!conv) return set_error(GLS_ERR_INVALID_ARG, "NULL converter");
+    GLS_CUDA(cudaSetDevice(conv->device));
+    GLS_CUDA(cudaDeviceSynchronize());
+    conv->prof.drain();
+    for (int i = 0; i < KC_COUNT; i++) {
+        conv->prof.launches[i] = 0;
+        conv->prof.ms[i] = 0;
+    }
+    return GLS_OK;
+}
+
+gls_status gls_calibration_fill(int32_t camera, int32_t iso, gls_demosaic_params* params) {
+    clear_error();
+    return calibration_fill(camera, iso, params);
+}
+
+gls_status gls_gaussian_bilinear_taps(float radius, float* taps, int32_t max_taps, int32_t* n_taps) {
+    clear_error();
+    if (!taps || !n_taps || !(radius > 0.f) || radius > 30.f) return set_error(GLS_ERR_INVALID_ARG, "bad arguments");
+    const int n = gaussian_taps(radius, taps, max_taps);
+    *n_taps = n < 0 ? -n : n;
+    if (n < 0) return set_error(GLS_ERR_INVALID_ARG, "max_taps too small (%d needed)", -n);
+    return GLS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,542 @@
+// gls_front.cu — front-end kernels of the raw path: Bayer unpack + scale,
+// Sobel + noise-adaptive gradient blur, the high-noise quad-domain raw
+// denoise, the fused three-pass demosaic with highlight blend and colour
+// transform, and the luma/chroma despeckle.
+//
+// Each kernel is a shared-memory halo tile: a block loads its tile plus the
+// stencil's halo once (clamped to the image edge), computes every
+// intermediate plane of the stencil chain for the tile in shared memory and
+// writes only the final plane. Intermediate planes of the reference
+// (Sobel image, green image, red/blue temporary) never reach HBM.
+#include "gls_common.cuh"
+#include "gls_kernels.h"
+
+namespace gls {
+
+// --------------------------------------------------------------------------
+// scaleRawData, demosaic.metal:96-118. One thread per 2 horizontal pixels.
+// value = max(ls * k_c * (raw - black) + 0.1, 0), k_c = scale_mul[c]*0.9/65535
+// (formed on the host in double). The black-level subtraction is integer;
+// the FP32 operations are explicitly rounded (no contraction) so the FP32
+// plane is bit-identical to the CPU oracle's FP32 run.
+template <class S>
+__global__ void __launch_bounds__(256) k_scale_raw(const uint16_t* __restrict__ raw, size_t raw_pitch,
+                                                   Plane<S, 1> out, ScaleArgs a) {
+    const int x2 = (blockIdx.x * blockDim.x + threadIdx.x) * 2;
+    const int y = blockIdx.y;
+    if (x2 >= out.w || y >= out.h) return;
+    const ushort2 rv = *reinterpret_cast<const ushort2*>(raw + size_t(y) * raw_pitch + x2);
+    float ls = 1.f;
+    if (a.lsc > 0.f) {
+        const float dx = __fsub_rn(float(x2), a.cx), dy = __fsub_rn(float(y & ~1), a.cy);
+        const float r = __fdiv_rn(__fsqrt_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy))), a.clen);
+        ls = __fadd_rn(1.f, __fmul_rn(__fmul_rn(a.lsc, r), r));
+    }
+    float v[2];
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        const int c = bayer_channel(a.pattern, x2 + i, y);
+        const int d = int(i == 0 ? rv.x : rv.y) - a.black;
+        const float k = a.lsc > 0.f ? __fmul_rn(ls, a.k[c]) : a.k[c];
+        v[i] = fmaxf(__fadd_rn(a.lsc > 0.f ? __fmul_rn(k, float(d)) : __fmul_rn(float(d), k), 0.1f), 0.f);
+    }
+    S* o = out.px(x2, y);
+    if constexpr (is_half<S>::value) {
+        *reinterpret_cast<__half2*>(o) = __floats2half2_rn(v[0], v[1]);
+    } else {
+        *reinterpret_cast<float2*>(o) = make_float2(v[0], v[1]);
+    }
+}
+
+// --------------------------------------------------------------------------
+// rawImageSobel + sampledConvolutionSobel fused, demosaic.metal:120-213.
+// Output tile 32 x 16 per 256-thread block. Shared memory: the scaled raw
+// tile with a 5-pixel halo (+1 right/bottom for the bilinear pair) and the
+// Sobel (gx, gy) tile with a 4/5-pixel halo. The blur taps are bilinear
+// samples at integer + fractional offsets (host-computed Gaussian folding).
+constexpr int SB_TW = 32, SB_TH = 16;
+constexpr int SB_RW = SB_TW + 11, SB_RH = SB_TH + 11;  // raw tile, origin -5
+constexpr int SB_SW = SB_TW + 9, SB_SH = SB_TH + 9;    // sobel tile, origin -4
+
+template <class S>
+__global__ void __launch_bounds__(256) k_sobel_blur(Plane<S, 1> raw, Plane<S, 2> out, BlurArgs a) {
+    __shared__ float sraw[SB_RH][SB_RW];
+    __shared__ float2 ssob[SB_SH][SB_SW];
+    const int x0 = blockIdx.x * SB_TW, y0 = blockIdx.y * SB_TH;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int nth = blockDim.x * blockDim.y;
+    for (int i = tid; i < SB_RW * SB_RH; i += nth) {
+        const int ty = i / SB_RW, tx = i % SB_RW;
+        sraw[ty][tx] = to_f(*raw.pxc(x0 - 5 + tx, y0 - 5 + ty));
+    }
+    __syncthreads();
+    const float inv = a.inv_sqrt45;
+    for (int i = tid; i < SB_SW * SB_SH; i += nth) {
+        const int ty = i / SB_SW, tx = i % SB_SW;
+        // Sobel at the clamped position of this tile entry
+        const int qx = clampi(x0 - 4 + tx, 0, raw.w - 1) - (x0 - 5);
+        const int qy = clampi(y0 - 4 + ty, 0, raw.h - 1) - (y0 - 5);
+        const float tl = sraw[qy - 1][qx - 1], tc = sraw[qy - 1][qx], tr = sraw[qy - 1][qx + 1];
+        const float ml = sraw[qy][qx - 1], mr = sraw[qy][qx + 1];
+        const float bl = sraw[qy + 1][qx - 1], bc = sraw[qy + 1][qx], br = sraw[qy + 1][qx + 1];
+        const float gx = ((tl - tr) + 2.f * (ml - mr) + (bl - br)) * inv;
+        const float gy = ((tl - bl) + 2.f * (tc - bc) + (tr - br)) * inv;
+        ssob[ty][tx] = make_float2(gx, gy);
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < SB_TH; r += blockDim.y) {
+        const int x = x0 + threadIdx.x, y = y0 + r;
+        if (x >= out.w || y >= out.h) continue;
+        const int lx = threadIdx.x + 4, ly = r + 4;  // sobel tile index of (x, y)
+        auto conv = [&](int first, int n, float res[4]) {
+            float s0 = 0, s1 = 0, s2 = 0, s3 = 0, norm = 0;
+            for (int t = first; t < first + n; t++) {
+                const float w = a.w[t];
+                const int ix = lx + a.ix[t], iy = ly + a.iy[t];
+                const float ax = a.fx[t], ay = a.fy[t];
+                const float2 p00 = ssob[iy][ix], p01 = ssob[iy][ix + 1];
+                const float2 p10 = ssob[iy + 1][ix], p11 = ssob[iy + 1][ix + 1];
+                auto bil = [&](float v00, float v01, float v10, float v11) {
+                    const float top = v00 + (v01 - v00) * ax;
+                    const float bot = v10 + (v11 - v10) * ax;
+                    return top + (bot - top) * ay;
+                };
+                s0 += w * bil(p00.x, p01.x, p10.x, p11.x);
+                s1 += w * bil(p00.y, p01.y, p10.y, p11.y);
+                s2 += w * bil(fabsf(p00.x), fabsf(p01.x), fabsf(p10.x), fabsf(p11.x));
+                s3 += w * bil(fabsf(p00.y), fabsf(p01.y), fabsf(p10.y), fabsf(p11.y));
+                norm += w;
+            }
+            res[0] = s0 / norm;
+            res[1] = s1 / norm;
+            res[2] = s2 / norm;
+            res[3] = s3 / norm;
+        };
+        float res[4];
+        conv(0, a.n1, res);
+        const float sigma = sqrtf(a.var0 + a.var1 * sraw[r + 5][threadIdx.x + 5]);
+        if (sqrtf(res[0] * res[0] + res[1] * res[1]) < 4.f * sigma) conv(a.n1, a.n2, res);
+        st2<S>(out.px(x, y), f2{copysignf(res[2], res[0]), copysignf(res[3], res[1])});
+    }
+}
+
+// --------------------------------------------------------------------------
+// High-noise raw branch, raw_converter.cpp:195-202: bayerToRawRGBA ->
+// despeckleRawRGBAImage -> crossDenoiseRawRGBAImage -> rawRGBAToBayer.
+// The quad gather/scatter is folded into the two stencil kernels.
+
+// despeckle_3x3x4 on the quad image read straight from the Bayer plane,
+// demosaic.metal:1025-1092. Output: quad RGBA plane.
+template <class S>
+__global__ void __launch_bounds__(256) k_raw_despeckle(Plane<S, 1> bayer, Plane<S, 2> grad, Plane<S, 4> quad,
+                                                       RawDenoiseArgs a) {
+    const int qx = blockIdx.x * blockDim.x + threadIdx.x, qy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (qx >= quad.w || qy >= quad.h) return;
+    const f2 g = ld2<S>(grad.px(2 * qx, 2 * qy));
+    const float gradient = sqrtf(g.x * g.x + g.y * g.y);
+    float res[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const int ox = kBayer[a.pattern][c][0], oy = kBayer[a.pattern][c][1];
+        float fmx = 0, smx = 0, fmn = 65504.f, smn = 65504.f;
+#pragma unroll
+        for (int i = -1; i <= 1; i++)
+#pragma unroll
+            for (int j = -1; j <= 1; j++) {
+                const int sx = clampi(qx + i, 0, quad.w - 1), sy = clampi(qy + j, 0, quad.h - 1);
+                const float v = to_f(*bayer.px(2 * sx + ox, 2 * sy + oy));
+                smx = v >= fmx ? fmx : fmaxf(v, smx);
+                fmx = fmaxf(v, fmx);
+                smn = v <= fmn ? fmn : fminf(v, smn);
+                fmn = fminf(v, fmn);
+            }
+        const float s = to_f(*bayer.px(2 * qx + ox, 2 * qy + oy));
+        const float sigma = sqrtf(a.var[c] * s);
+        const float tex = 1.f - 0.5f * smoothstepf(1.f, 2.f, gradient / sigma);
+        const float mn = mixf(fmn, smn, tex * (1.f - smoothstepf(2.f * sigma, 8.f * sigma, smn - fmn)));
+        const float mx = mixf(fmx, smx, tex * (1.f - smoothstepf(sigma, 4.f * sigma, fmx - smx)));
+        res[c] = clampf(s, mn, mx);
+    }
+    st4<S>(quad.px(qx, qy), f4{res[0], res[1], res[2], res[3]});
+}
+
+// crossDenoiseRawRGBAImage, demosaic.metal:999-1023, writing the result
+// back into the Bayer plane (rawRGBAToBayer, :980-997).
+template <class S>
+__global__ void __launch_bounds__(256) k_raw_cross_denoise(Plane<S, 4> quad, Plane<S, 1> bayer, RawDenoiseArgs a) {
+    const int qx = blockIdx.x * blockDim.x + threadIdx.x, qy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (qx >= quad.w || qy >= quad.h) return;
+    const f4 p = ld4<S>(quad.px(qx, qy));
+    const float pc[4] = {p.x, p.y, p.z, p.w};
+    float inv[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) inv[c] = 1.f / (a.strength * sqrtf(a.var[c] * (pc[c] + 0.0001f)));
+    float sum[4] = {0, 0, 0, 0}, sw = 0;
+    for (int j = -2; j <= 2; j++)
+        for (int i = -2; i <= 2; i++) {
+            const f4 s = ld4<S>(quad.pxc(qx + i, qy + j));
+            const float sc[4] = {s.x, s.y, s.z, s.w};
+            float d2 = 0;
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const float d = (pc[c] - sc[c]) * inv[c];
+                d2 += d * d;
+            }
+            const float w = a.fast ? __expf(-2.f * d2) : expf(-2.f * d2);
+#pragma unroll
+            for (int c = 0; c < 4; c++) sum[c] += w * sc[c];
+            sw += w;
+        }
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const int ox = kBayer[a.pattern][c][0], oy = kBayer[a.pattern][c][1];
+        *bayer.px(2 * qx + ox, 2 * qy + oy) = from_f<S>(sum[c] / sw);
+    }
+}
+
+// --------------------------------------------------------------------------
+// Fused demosaic: interpolateGreen (demosaic.metal:215-316) ->
+// interpolateRedBlue (:318-416) -> interpolateRedBlueAtGreen (:418-521) ->
+// blendHighlightsImage (:523-564) -> optional transformImage (:649-662).
+// Output tile 32 x 16; halos: red/blue temporary +-3, green +-5, raw +-7.
+constexpr int DM_TW = 32, DM_TH = 16;
+constexpr int DM_RW = DM_TW + 14, DM_RH = DM_TH + 14;  // raw, origin -7
+constexpr int DM_GW = DM_TW + 10, DM_GH = DM_TH + 10;  // green + gradient, origin -5
+constexpr int DM_CW = DM_TW + 6, DM_CH = DM_TH + 6;    // red/blue temporary, origin -3
+
+struct DemosaicSmem {
+    float raw[DM_RH][DM_RW];
+    float green[DM_GH][DM_GW];
+    float2 grad[DM_GH][DM_GW];
+    float tmp[3][DM_CH][DM_CW];
+};
+
+
+template <class S>
+__global__ void __launch_bounds__(256) k_demosaic(Plane<S, 1> raw, Plane<S, 2> grad, Plane<S, 4> out, DemosaicArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    DemosaicSmem& sm = *reinterpret_cast<DemosaicSmem*>(smem_raw);
+    const int x0 = blockIdx.x * DM_TW, y0 = blockIdx.y * DM_TH;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nth = blockDim.x * blockDim.y;
+    const int W = raw.w, H = raw.h;
+    const int rx = kBayer[a.pattern][0][0], ry = kBayer[a.pattern][0][1];
+    const int bx = kBayer[a.pattern][2][0], by = kBayer[a.pattern][2][1];
+    const float kPi = 3.14159265358979323846f;
+
+    for (int i = tid; i < DM_RW * DM_RH; i += nth) {
+        const int ty = i / DM_RW, tx = i % DM_RW;
+        sm.raw[ty][tx] = to_f(*raw.pxc(x0 - 7 + tx, y0 - 7 + ty));
+    }
+    for (int i = tid; i < DM_GW * DM_GH; i += nth) {
+        const int ty = i / DM_GW, tx = i % DM_GW;
+        const f2 g = ld2<S>(grad.pxc(x0 - 5 + tx, y0 - 5 + ty));
+        sm.grad[ty][tx] = make_float2(fabsf(g.x), fabsf(g.y));
+    }
+    __syncthreads();
+
+    // ---- green at the clamped position of every green-tile entry
+    const float lowNoise = 1.f - smoothstepf(3.5e-4f, 2e-3f, a.gv1);
+    for (int i = tid; i < DM_GW * DM_GH; i += nth) {
+        const int ty = i / DM_GW, tx = i % DM_GW;
+        const int px = clampi(x0 - 5 + tx, 0, W - 1), py = clampi(y0 - 5 + ty, 0, H - 1);
+        const int lx = px - (x0 - 7), ly = py - (y0 - 7);  // raw-tile index of the clamped position
+        auto R = [&](int di, int dj) { return sm.raw[ly + dj][lx + di]; };
+        const bool red = (rx & 1) == (px & 1) && (ry & 1) == (py & 1);
+        const bool blue = (bx & 1) == (px & 1) && (by & 1) == (py & 1);
+        float g;
+        if (!(red || blue)) {
+            g = R(0, 0);
+        } else {
+            const float gl = R(-1, 0), gr = R(1, 0), gu = R(0, -1), gd = R(0, 1);
+            const float cxy = R(0, 0);
+            const float cl = R(-2, 0), cr = R(2, 0), cu = R(0, -2), cd = R(0, 2);
+            const float c2ave = (R(-1, -1) + R(1, -1) + R(-1, 1) + R(1, 1)) / 4.f;
+            const float gave = (gl + gr + gu + gd) / 4.f;
+            const float2 gg = sm.grad[ty][tx];
+            const float glfx = (gl + gr) / 2.f, glfy = (gu + gd) / 2.f;
+            const float ghfx = ((cl + cr) - 2.f * cxy) / 4.f, ghfy = ((cu + cd) - 2.f * cxy) / 4.f;
+            const float sd = sqrtf(a.gv0 + a.gv1 * gave);
+            const float glen = sqrtf(gg.x * gg.x + gg.y * gg.y);
+            const float gthr = smoothstepf(sd, 4.f * sd, glen);
+            const float lowthr = 1.f - smoothstepf(2.f * sd, 8.f * sd, glen);
+            const float sharp = (0.5f + 0.5f * lowNoise) * gthr * (1.f + lowNoise * lowthr);
+            const float hl = 1.f - smoothstepf(0.25f, 1.f, fmaxf(cxy, fmaxf(fmaxf(cl, cr), fmaxf(cu, cd))));
+            float dir = 2.f * atan2f(gg.y, gg.x) / kPi;
+            if (a.gv1 < 1e-3f) {
+                dir = dir < 0.5f ? mixf(dir, 0.f, 1.f - smoothstepf(0.3f, 0.45f, dir))
+                                 : mixf(dir, 1.f, smoothstepf(1.f - 0.45f, 1.f - 0.3f, dir));
+            }
+            const float cmin = fminf(cxy, fminf(gave, c2ave)), cmax = fmaxf(cxy, fmaxf(gave, c2ave));
+            const float white = cmin / cmax;
+            const float k = hl * white * sharp;
+            const float gex = glfx - k * ghfx, gey = glfy - k * ghfy;
+            g = mixf(gey, gex, dir);
+            const float maxo = mixf(1.f, 1.5f, white), mino = mixf(1.f, 0.5f, white);
+            const float gmax = fmaxf(fmaxf(gl, gr), fmaxf(gu, gd));
+            const float gmin = fminf(fminf(gl, gr), fminf(gu, gd));
+            g = clampf(g, mino * gmin, maxo * gmax);
+        }
+        sm.green[ty][tx] = g;
+    }
+    __syncthreads();
+
+    // ---- red/blue temporary at the clamped position of every tmp-tile entry
+    for (int i = tid; i < DM_CW * DM_CH; i += nth) {
+        const int ty = i / DM_CW, tx = i % DM_CW;
+        const int px = clampi(x0 - 3 + tx, 0, W - 1), py = clampi(y0 - 3 + ty, 0, H - 1);
+        const int gx = px - (x0 - 5), gy = py - (y0 - 5);  // green-tile index
+        const int lx = px - (x0 - 7), ly = py - (y0 - 7);  // raw-tile index
+        const bool red = (rx & 1) == (px & 1) && (ry & 1) == (py & 1);
+        const bool blue = (bx & 1) == (px & 1) && (by & 1) == (py & 1);
+        float o0, o1, o2;
+        if (!(red || blue)) {
+            o0 = 0.f;
+            o1 = sm.green[gy][gx];
+            o2 = 0.f;
+        } else {
+            auto R = [&](int di, int dj) { return sm.raw[ly + dj][lx + di]; };
+            auto G = [&](int di, int dj) { return sm.green[gy + dj][gx + di]; };
+            const float g0 = G(0, 0), c1 = R(0, 0);
+            const float c2tl = R(-1, -1), c2tr = R(1, -1), c2bl = R(-1, 1), c2br = R(1, 1);
+            const float c2ave = (c2tl + c2tr + c2bl + c2br) / 4.f;
+            const float gctl = G(-1, -1) - c2tl, gctr = G(1, -1) - c2tr, gcbl = G(-1, 1) - c2bl, gcbr = G(1, 1) - c2br;
+            const float gtl2 = G(-2, -2), gtr2 = G(2, -2), gbl2 = G(-2, 2), gbr2 = G(2, 2);
+            const float gctl2 = gtl2 - R(-2, -2), gctr2 = gtr2 - R(2, -2), gcbl2 = gbl2 - R(-2, 2),
+                        gcbr2 = gbr2 - R(2, 2);
+            const float v0 = red ? a.rv0 : a.bv0, v1 = red ? a.rv1 : a.bv1;
+            const float sd = sqrtf(v0 + v1 * c2ave);
+            const float2 gg = sm.grad[gy][gx];
+            const float dir = 1.f - 2.f * atan2f(gg.y, gg.x) / kPi;
+            const float gthr = smoothstepf(sd, 4.f * sd, sqrtf(gg.x * gg.x + gg.y * gg.y));
+            const float alpha = mixf(0.5f, dir, gthr);
+            const float hl = 1.f - smoothstepf(0.25f, 1.f, fmaxf(g0, fmaxf(fmaxf(gtr2, gbl2), fmaxf(gtl2, gbr2))));
+            const float gc = g0 - c1;
+            const float aa = (gctr + gcbl) / 2.f + hl * (gctr2 + gcbl2 - 2.f * gc) / 8.f;
+            const float bb = (gctl + gcbr) / 2.f + hl * (gctl2 + gcbr2 - 2.f * gc) / 8.f;
+            float c2 = g0 - mixf(aa, bb, alpha);
+            const float c2max = fmaxf(fmaxf(c2tl, c2tr), fmaxf(c2bl, c2br));
+            const float c2min = fminf(fminf(c2tl, c2tr), fminf(c2bl, c2br));
+            c2 = clampf(c2, c2min, c2max);
+            if (red) {
+                o0 = c1; o1 = g0; o2 = c2;
+            } else {
+                o0 = c2; o1 = g0; o2 = c1;
+            }
+        }
+        sm.tmp[0][ty][tx] = o0;
+        sm.tmp[1][ty][tx] = o1;
+        sm.tmp[2][ty][tx] = o2;
+    }
+    __syncthreads();
+
+    // ---- red/blue at green sites, highlights, colour transform
+    for (int r = threadIdx.y; r < DM_TH; r += blockDim.y) {
+        const int x = x0 + threadIdx.x, y = y0 + r;
+        if (x >= W || y >= H) continue;
+        const int cx = threadIdx.x + 3, cy = r + 3;  // tmp-tile index of (x, y)
+        const bool red = (rx & 1) == (x & 1) && (ry & 1) == (y & 1);
+        const bool blue = (bx & 1) == (x & 1) && (by & 1) == (y & 1);
+        float rgb[3];
+        if (red || blue) {
+            rgb[0] = sm.tmp[0][cy][cx];
+            rgb[1] = sm.tmp[1][cy][cx];
+            rgb[2] = sm.tmp[2][cy][cx];
+        } else {
+            auto P = [&](int di, int dj, int c) { return sm.tmp[c][cy + dj][cx + di]; };
+            const float g0 = P(0, 0, 1);
+            const float lr = P(-1, 0, 0), lg = P(-1, 0, 1), lb = P(-1, 0, 2);
+            const float rr = P(1, 0, 0), rg = P(1, 0, 1), rb = P(1, 0, 2);
+            const float ur = P(0, -1, 0), ug = P(0, -1, 1), ub = P(0, -1, 2);
+            const float dr = P(0, 1, 0), dg = P(0, 1, 1), db = P(0, 1, 2);
+            const float red_ave = (lr + rr + ur + dr) / 4.f, blue_ave = (lb + rb + ub + db) / 4.f;
+            const float grl = lg - lr, grr = rg - rr, gru = ug - ur, grd = dg - dr;
+            const float gbl = lg - lb, gbr = rg - rb, gbu = ug - ub, gbd = dg - db;
+            const float grl3 = P(-3, 0, 1) - P(-3, 0, 0), grr3 = P(3, 0, 1) - P(3, 0, 0);
+            const float gru3 = P(0, -3, 1) - P(0, -3, 0), grd3 = P(0, 3, 1) - P(0, 3, 0);
+            const float gbl3 = P(-3, 0, 1) - P(-3, 0, 2), gbr3 = P(3, 0, 1) - P(3, 0, 2);
+            const float gbu3 = P(0, -3, 1) - P(0, -3, 2), gbd3 = P(0, 3, 1) - P(0, 3, 2);
+            const float2 gg = sm.grad[r + 5][threadIdx.x + 5];
+            const float dir = 2.f * atan2f(gg.y, gg.x) / kPi;
+            const float glen = sqrtf(gg.x * gg.x + gg.y * gg.y);
+            const float rsd = sqrtf(a.rv0 + a.rv1 * red_ave), bsd = sqrtf(a.bv0 + a.bv1 * blue_ave);
+            const float ralpha = mixf(0.5f, dir, smoothstepf(rsd, 4.f * rsd, glen));
+            const float balpha = mixf(0.5f, dir, smoothstepf(bsd, 4.f * bsd, glen));
+            const float hl = 1.f - smoothstepf(0.25f, 1.f, fmaxf(g0, fmaxf(fmaxf(rg, lg), fmaxf(dg, ug))));
+            const float red_v = g0 - mixf((gru + grd) / 2.f - hl * ((grd3 - gru) - (grd - gru3)) / 8.f,
+                                          (grl + grr) / 2.f - hl * ((grr3 - grl) - (grr - grl3)) / 8.f, ralpha);
+            const float blue_v = g0 - mixf((gbu + gbd) / 2.f - hl * ((gbd3 - gbu) - (gbd - gbu3)) / 8.f,
+                                           (gbl + gbr) / 2.f - hl * ((gbr3 - gbl) - (gbr - gbl3)) / 8.f, balpha);
+            rgb[0] = clampf(red_v, fminf(fminf(lr, rr), fminf(ur, dr)), fmaxf(fmaxf(lr, rr), fmaxf(ur, dr)));
+            rgb[1] = g0;
+            rgb[2] = clampf(blue_v, fminf(fminf(lb, rb), fminf(ub, db)), fmaxf(fmaxf(lb, rb), fmaxf(ub, db)));
+        }
+        // blendHighlightsImage, clip = 1
+        const float clip = 1.f;
+        if (rgb[0] > clip || rgb[1] > clip || rgb[2] > clip) {
+            const float s3 = 1.7320508f;
+            const float c0[3] = {rgb[0], rgb[1], rgb[2]};
+            const float c1[3] = {fminf(rgb[0], clip), fminf(rgb[1], clip), fminf(rgb[2], clip)};
+            const float l0x = c0[0] + c0[1] + c0[2], l0y = s3 * c0[0] - s3 * c0[1], l0z = -c0[0] - c0[1] + 2.f * c0[2];
+            const float l1y = s3 * c1[0] - s3 * c1[1], l1z = -c1[0] - c1[1] + 2.f * c1[2];
+            const float sum0 = l0y * l0y + l0z * l0z, sum1 = l1y * l1y + l1z * l1z;
+            const float chr = sum0 > 0.f ? sqrtf(sum1 / sum0) : 1.f;
+            const float ly = l0y * chr, lz = l0z * chr;
+            rgb[0] = (l0x + (s3 / 2.f) * ly - 0.5f * lz) / 3.f;
+            rgb[1] = (l0x - (s3 / 2.f) * ly - 0.5f * lz) / 3.f;
+            rgb[2] = (l0x + lz) / 3.f;
+        }
+        f4 o;
+        if (a.transform) {
+            o.x = a.m[0] * rgb[0] + a.m[1] * rgb[1] + a.m[2] * rgb[2];
+            o.y = a.m[3] * rgb[0] + a.m[4] * rgb[1] + a.m[5] * rgb[2];
+            o.z = a.m[6] * rgb[0] + a.m[7] * rgb[1] + a.m[8] * rgb[2];
+        } else {
+            o.x = rgb[0]; o.y = rgb[1]; o.z = rgb[2];
+        }
+        o.w = 0.f;
+        st4<S>(out.px(x, y), o);
+    }
+}
+
+// --------------------------------------------------------------------------
+// despeckleLumaMedianChromaImage, demosaic.metal:1161-1283.
+__device__ __forceinline__ void sort2(float& a, float& b) {
+    const float t = fminf(a, b);
+    b = fmaxf(a, b);
+    a = t;
+}
+// exact median of 9 (a min/max selection network)
+__device__ __forceinline__ float median9(float v[9]) {
+    sort2(v[1], v[2]); sort2(v[4], v[5]); sort2(v[7], v[8]);
+    sort2(v[0], v[1]); sort2(v[3], v[4]); sort2(v[6], v[7]);
+    sort2(v[1], v[2]); sort2(v[4], v[5]); sort2(v[7], v[8]);
+    sort2(v[0], v[3]); sort2(v[5], v[8]); sort2(v[4], v[7]);
+    sort2(v[3], v[6]); sort2(v[1], v[4]); sort2(v[2], v[5]);
+    sort2(v[4], v[7]); sort2(v[4], v[2]); sort2(v[6], v[4]);
+    sort2(v[4], v[2]);
+    return v[4];
+}
+
+template <class S>
+__global__ void __launch_bounds__(256) k_despeckle(Plane<S, 4> in, Plane<S, 4> out, float va, float vb) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= in.w || y >= in.h) return;
+    float cb[9], cr[9];
+    float fmx = 0.f, smx = 0.f, fmn = INFINITY, smn = INFINITY, sample = 0.f;
+    int k = 0;
+#pragma unroll
+    for (int j = -1; j <= 1; j++)
+#pragma unroll
+        for (int i = -1; i <= 1; i++, k++) {
+            const f4 p = ld4<S>(in.pxc(x + i, y + j));
+            const float v = p.x;
+            smx = (v <= fmx && v > smx) ? v : smx;
+            smx = v > fmx ? fmx : smx;
+            fmx = v > fmx ? v : fmx;
+            smn = (v >= fmn && v < smn) ? v : smn;
+            smn = v < fmn ? fmn : smn;
+            fmn = v < fmn ? v : fmn;
+            if (i == 0 && j == 0) sample = v;
+            cb[k] = p.y;
+            cr[k] = p.z;
+        }
+    const float sigma = sqrtf(va + vb * sample);
+    const float mn = mixf(smn, fmn, smoothstepf(sigma, 4.f * sigma, smn - fmn));
+    const float mx = mixf(smx, fmx, smoothstepf(sigma, 4.f * sigma, fmx - smx));
+    st4<S>(out.px(x, y), f4{clampf(sample, mn, mx), median9(cb), median9(cr), 0.f});
+}
+
+// transformImage, demosaic.metal:649-662, from plane S4 to an output of
+// element type O (float or half), w = 0.
+template <class S, class O>
+__global__ void __launch_bounds__(256) k_transform(Plane<S, 4> in, Plane<O, 4> out, Mat3Args m) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= in.w || y >= in.h) return;
+    const f4 p = ld4<S>(in.px(x, y));
+    f4 o;
+    o.x = m.m[0] * p.x + m.m[1] * p.y + m.m[2] * p.z;
+    o.y = m.m[3] * p.x + m.m[4] * p.y + m.m[5] * p.z;
+    o.z = m.m[6] * p.x + m.m[7] * p.y + m.m[8] * p.z;
+    o.w = 0.f;
+    st4<O>(out.px(x, y), o);
+}
+
+// plain copy with element conversion (for output views)
+template <class S, class O>
+__global__ void __launch_bounds__(256) k_convert4(Plane<S, 4> in, Plane<O, 4> out) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= in.w || y >= in.h) return;
+    st4<O>(out.px(x, y), ld4<S>(in.px(x, y)));
+}
+
+// ------------------------------------------------------------------ launchers
+static inline dim3 grid2(int w, int h, dim3 b) { return dim3((w + b.x - 1) / b.x, (h + b.y - 1) / b.y); }
+
+template <class S>
+void launch_scale_raw(const uint16_t* raw, size_t raw_pitch, Plane<S, 1> out, const ScaleArgs& a, cudaStream_t s) {
+    dim3 b(128, 1);
+    dim3 g((out.w / 2 + b.x - 1) / b.x, out.h);
+    k_scale_raw<S><<<g, b, 0, s>>>(raw, raw_pitch, out, a);
+}
+
+template <class S>
+void launch_sobel_blur(Plane<S, 1> raw, Plane<S, 2> out, const BlurArgs& a, cudaStream_t s) {
+    dim3 b(32, 8);
+    dim3 g((raw.w + SB_TW - 1) / SB_TW, (raw.h + SB_TH - 1) / SB_TH);
+    k_sobel_blur<S><<<g, b, 0, s>>>(raw, out, a);
+}
+
+template <class S>
+void launch_raw_denoise(Plane<S, 1> bayer, Plane<S, 2> grad, Plane<S, 4> quad, const RawDenoiseArgs& a,
+                        cudaStream_t s) {
+    dim3 b(32, 8);
+    k_raw_despeckle<S><<<grid2(quad.w, quad.h, b), b, 0, s>>>(bayer, grad, quad, a);
+    k_raw_cross_denoise<S><<<grid2(quad.w, quad.h, b), b, 0, s>>>(quad, bayer, a);
+}
+
+template <class S>
+void launch_demosaic(Plane<S, 1> raw, Plane<S, 2> grad, Plane<S, 4> out, const DemosaicArgs& a, cudaStream_t s) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_demosaic<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(DemosaicSmem)));
+        attr_set = true;
+    }
+    dim3 b(32, 8);
+    dim3 g((raw.w + DM_TW - 1) / DM_TW, (raw.h + DM_TH - 1) / DM_TH);
+    k_demosaic<S><<<g, b, sizeof(DemosaicSmem), s>>>(raw, grad, out, a);
+}
+
+template <class S>
+void launch_despeckle(Plane<S, 4> in, Plane<S, 4> out, float va, float vb, cudaStream_t s) {
+    dim3 b(32, 8);
+    k_despeckle<S><<<grid2(in.w, in.h, b), b, 0, s>>>(in, out, va, vb);
+}
+
+template <class S, class O>
+void launch_transform(Plane<S, 4> in, Plane<O, 4> out, const Mat3Args& m, cudaStream_t s) {
+    dim3 b(32, 8);
+    k_transform<S, O><<<grid2(in.w, in.h, b), b, 0, s>>>(in, out, m);
+}
+
+template <class S, class O>
+void launch_convert4(Plane<S, 4> in, Plane<O, 4> out, cudaStream_t s) {
+    dim3 b(32, 8);
+    k_convert4<S, O><<<grid2(in.w, in.h, b), b, 0, s>>>(in, out);
+}
+
+#define GLS_INST(S)                                                                                            \
+    template void launch_scale_raw<S>(const uint16_t*, size_t, Plane<S, 1>, const ScaleArgs&, cudaStream_t);  \
+    template void launch_sobel_blur<S>(Plane<S, 1>, Plane<S, 2>, const BlurArgs&, cudaStream_t);              \
+    template void launch_raw_denoise<S>(Plane<S, 1>, Plane<S, 2>, Plane<S, 4>, const RawDenoiseArgs&,         \
+                                        cudaStream_t);                                                         \
+    template void launch_demosaic<S>(Plane<S, 1>, Plane<S, 2>, Plane<S, 4>, const DemosaicArgs&, cudaStream_t); \
+    template void launch_despeckle<S>(Plane<S, 4>, Plane<S, 4>, float, float, cudaStream_t);                  \
+    template void launch_transform<S, float>(Plane<S, 4>, Plane<float, 4>, const Mat3Args&, cudaStream_t);    \
+    template void launch_transform<S, __half>(Plane<S, 4>, Plane<__half, 4>, const Mat3Args&, cudaStream_t);  \
+    template void launch_convert4<S, float>(Plane<S, 4>, Plane<float, 4>, cudaStream_t);                      \
+    template void launch_convert4<S, __half>(Plane<S, 4>, Plane<__half, 4>, cudaStream_t);
+GLS_INST(float)
+GLS_INST(__half)
+#undef GLS_INST
+
+}  // namespace gls

@@ -1,0 +1,100 @@
+// gls_kernels.h — kernel argument blocks and host launchers of the raw path.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "gls_common.cuh"
+
+namespace gls {
+
+constexpr int kMaxTaps = 32;
+
+struct ScaleArgs {
+    int pattern;
+    int black;       // integer black level (DN)
+    float k[4];      // scale_mul[c] * 0.9 / 65535, per Bayer channel
+    float lsc;       // lens shading strength (0 = off)
+    float cx, cy, clen;
+};
+
+struct BlurArgs {
+    int n1, n2;                  // narrow / wide tap counts (wide taps follow the narrow ones)
+    float w[kMaxTaps];           // tap weights
+    int ix[kMaxTaps], iy[kMaxTaps];    // floor of the tap offsets
+    float fx[kMaxTaps], fy[kMaxTaps];  // fractional parts
+    float var0, var1;            // green raw variance (a, b)
+    float inv_sqrt45;
+};
+
+struct RawDenoiseArgs {
+    int pattern;
+    float var[4];     // raw NLF b coefficients per channel (R, G, B, G2)
+    float strength;   // cross-denoise strength
+    int fast;         // fast exp (FP16-storage path)
+};
+
+struct DemosaicArgs {
+    int pattern;
+    float rv0, rv1, gv0, gv1, bv0, bv1;  // raw variance (a, b) of R, G, B
+    int transform;                       // apply m (cam -> YCbCr) to the output
+    float m[9];
+};
+
+struct Mat3Args {
+    float m[9];
+};
+
+template <class S>
+void launch_scale_raw(const uint16_t* raw, size_t raw_pitch, Plane<S, 1> out, const ScaleArgs& a, cudaStream_t s);
+template <class S>
+void launch_sobel_blur(Plane<S, 1> raw, Plane<S, 2> out, const BlurArgs& a, cudaStream_t s);
+template <class S>
+void launch_raw_denoise(Plane<S, 1> bayer, Plane<S, 2> grad, Plane<S, 4> quad, const RawDenoiseArgs& a,
+                        cudaStream_t s);
+template <class S>
+void launch_demosaic(Plane<S, 1> raw, Plane<S, 2> grad, Plane<S, 4> out, const DemosaicArgs& a, cudaStream_t s);
+template <class S>
+void launch_despeckle(Plane<S, 4> in, Plane<S, 4> out, float va, float vb, cudaStream_t s);
+template <class S, class O>
+void launch_transform(Plane<S, 4> in, Plane<O, 4> out, const Mat3Args& m, cudaStream_t s);
+template <class S, class O>
+void launch_convert4(Plane<S, 4> in, Plane<O, 4> out, cudaStream_t s);
+
+// ---- pyramid ----
+struct BlockMatchArgs {
+    float var_a[3], var_b[3];     // YCbCr NLF of the level
+    float tm[3];                  // threshold multipliers (luma, chroma, chroma)
+    float chroma_boost, gradient_boost, gradient_threshold;
+    float lsc;                    // lens shading correction (0 = off)
+};
+
+struct SubtractArgs {
+    float luma_weight, sharpening, nlf_a, nlf_b;
+};
+
+// PCA accumulators of one level: sum of (p - shift) over patches (25) and
+// the upper triangle of sum (p - shift)(p - shift)^T (325), FP64.
+constexpr int kPcaAcc = 25 + 325;
+constexpr int kPcaDim = 25, kPcaComp = 8;
+
+template <class S, int C>
+void launch_downsample(Plane<S, C> in, Plane<S, C> out, cudaStream_t s);
+template <class S>
+void launch_subtract_noise(Plane<S, 4> in, Plane<S, 4> coarse, Plane<S, 4> coarse_den, Plane<S, 2> grad,
+                           Plane<S, 4> out, const SubtractArgs& a, cudaStream_t s);
+template <class S>
+void launch_pca_cov(Plane<S, 4> img, double* acc, cudaStream_t s);
+void launch_pca_eigen(const double* acc, int n_patches, float* basis /*25x8*/, int* status, cudaStream_t s);
+template <class S>
+void launch_pca_project(Plane<S, 4> img, const float* basis, Plane<S, 8> out, cudaStream_t s);
+template <class S>
+void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, Plane<S, 4> out,
+                        const BlockMatchArgs& a, cudaStream_t s);
+
+// host-side eigen-solve of the same accumulators (the reference's per-level
+// host PCA, pyramid_processor.cpp:148-149)
+void host_pca_basis(const double* acc, int n_patches, float* basis);
+
+}  // namespace gls

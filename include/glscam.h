@@ -1,0 +1,223 @@
+/*
+ * glscam.h — C ABI of the B200 raw-image path (demosaic, pyramid PCA
+ * block-matching denoise and reconstruct, SURF registration, burst fusion).
+ *
+ * Every entry point is a plain C function over plain pointers and sizes; no
+ * C++ or torch type crosses this boundary and no exception escapes it.
+ * Errors come back as gls_status codes, with a thread-local message from
+ * gls_last_error_message().
+ *
+ * The functions replace the reference's C++ entry points (paths are relative
+ * to the GlassCameraPublic tree):
+ *   RawConverter ctor / demosaic    MetalPipeline/raw_converter.hpp:128-183,
+ *                                   MetalPipeline/raw_converter.cpp:148-248
+ *   PyramidProcessor<levels>        MetalPipeline/pyramid_processor.hpp:23-62,
+ *                                   MetalPipeline/pyramid_processor.cpp:96-172
+ *   CameraCalibration<levels>       MetalPipeline/CameraCalibration.hpp:24-39
+ *   parameter structs               MetalPipeline/demosaic.hpp:28-124
+ *   SURF / FindHomography           ImageRegistration/SURF.hpp:45-80,
+ *                                   ImageRegistration/Homography.hpp:26-37
+ *   registerAndFuse                 MetalPipeline/demosaic_kernels.hpp:690-710
+ *
+ * Threading: a converter is not thread-safe (the reference's RawConverter is
+ * not reentrant either: one Metal queue per converter). Distinct converters
+ * are independent. All device work is ordered on the stream passed in.
+ */
+#ifndef GLSCAM_H
+#define GLSCAM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (replace the reference's exceptions and asserts:
+ *      gls_mtl.hpp:74, iPhone14WideCalibration.cpp:61,
+ *      LeastSquaresHomography.cpp:382-384, demosaic_kernels.hpp:160-163) ---- */
+typedef enum gls_status {
+    GLS_OK = 0,
+    GLS_ERR_INVALID_ARG = 1,
+    GLS_ERR_OOM = 2,
+    GLS_ERR_CUDA = 3,
+    GLS_ERR_TIMEOUT = 4,
+    GLS_ERR_DEGENERATE = 5,
+    GLS_ERR_UNSUPPORTED = 6,
+    GLS_ERR_RANGE = 7
+} gls_status;
+
+/* BayerPattern, demosaic.hpp:24 */
+enum { GLS_GRBG = 0, GLS_GBRG = 1, GLS_RGGB = 2, GLS_BGGR = 3 };
+
+#define GLS_MAX_LEVELS 5
+
+/* DenoiseParameters, demosaic.hpp:33-40 */
+typedef struct gls_denoise_params {
+    float luma;
+    float chroma;
+    float chroma_boost;
+    float gradient_boost;
+    float gradient_threshold;
+    float sharpening;
+} gls_denoise_params;
+
+/* YCbCrNLF = pair<Vector<3>, Vector<3>>, demosaic.hpp:53 (variance = a + b*Y) */
+typedef struct gls_ycbcr_nlf {
+    float a[3];
+    float b[3];
+} gls_ycbcr_nlf;
+
+/* RawNLF = pair<Vector<4>, Vector<4>>, demosaic.hpp:51 (channels R, G, B, G2) */
+typedef struct gls_raw_nlf {
+    float a[4];
+    float b[4];
+} gls_raw_nlf;
+
+/* DemosaicParameters, demosaic.hpp:102-124, flattened to plain data. The
+ * local-tone-mapping and sRGB conversion members are not part of this path. */
+typedef struct gls_demosaic_params {
+    int32_t bayer_pattern;           /* GLS_GRBG .. GLS_BGGR */
+    float black_level;               /* DN */
+    float white_level;               /* DN */
+    float exposure_multiplier;
+    float lens_shading_correction;   /* 0 disables */
+    float scale_mul[4];              /* per Bayer channel R, G, B, G2 */
+    float rgb_cam[9];                /* row-major 3x3 */
+    float xyz_rgb[9];                /* row-major 3x3, xyz_sRGB by default */
+    int32_t high_noise_image;        /* RAWDenoiseParameters::highNoiseImage */
+    float raw_denoise_strength;      /* RAWDenoiseParameters::strength */
+    gls_raw_nlf raw_nlf;
+    gls_ycbcr_nlf pyramid_nlf[GLS_MAX_LEVELS];
+    gls_denoise_params denoise[GLS_MAX_LEVELS];
+    int32_t levels;                  /* pyramid levels, 1..5 (the reference fixes 5) */
+    int32_t iso;
+} gls_demosaic_params;
+
+/* element types of an image view */
+enum { GLS_F32 = 0, GLS_F16 = 1, GLS_U16 = 2 };
+
+/* An image in memory: interleaved channels, row stride in bytes. */
+typedef struct gls_image_view {
+    void* data;
+    int32_t width;
+    int32_t height;
+    int32_t channels;
+    int32_t dtype;                   /* GLS_F32 / GLS_F16 / GLS_U16 */
+    size_t stride_bytes;
+} gls_image_view;
+
+/* flags for gls_demosaic / gls_demosaic_batch / gls_pyramid_denoise */
+enum {
+    GLS_DENOISE = 1u << 0,       /* run the pyramid denoise (RawConverter::demosaic noiseReduction) */
+    GLS_POSTPROCESS = 1u << 1,   /* sRGB post-processing: not on this path, rejected */
+    GLS_FP16_STORAGE = 1u << 2,  /* FP16 planes + fused kernels + device PCA (the batched path) */
+    GLS_HOST_IO = 1u << 3,       /* raw input and caller output buffers are host memory */
+    GLS_SYNC = 1u << 4,          /* block until the stream has finished (the reference is synchronous) */
+    GLS_HOST_PCA = 1u << 5       /* per-level PCA eigen-solve on the host, as the reference does */
+};
+
+/* Planes a converter exposes after gls_demosaic, for stage checks. */
+enum {
+    GLS_PLANE_SCALED_RAW = 0,    /* 1 ch, after scaleRawData (and the high-noise raw branch) */
+    GLS_PLANE_GRADIENT = 1,      /* 2 ch, sampledConvolutionSobel output */
+    GLS_PLANE_DEMOSAIC = 2,      /* 4 ch camera RGB after blendHighlights */
+    GLS_PLANE_DESPECKLED = 3,    /* 4 ch YCbCr input of the pyramid (after despeckle) */
+    GLS_PLANE_OUTPUT = 4,        /* 4 ch final camera RGB */
+    GLS_PLANE_DENOISED_L0 = 8    /* + level: 4 ch denoised YCbCr of a pyramid level */
+};
+
+typedef struct gls_converter gls_converter;
+
+/* Message of the last error on this thread ("" if none). */
+const char* gls_last_error_message(void);
+
+/* Library build string (kernels, architecture). */
+const char* gls_version(void);
+
+/* RawConverter(device, icc, calibrateFromImage), raw_converter.hpp:128-156.
+ * icc may be NULL (xyz_sRGB). calibrate_from_image must be 0: the noise
+ * measurement path is not part of this library. */
+gls_status gls_converter_create(int32_t device, const uint8_t* icc, size_t icc_len,
+                                int32_t calibrate_from_image, gls_converter** out);
+gls_status gls_converter_destroy(gls_converter* conv);
+
+/* RawConverter::demosaic(raw, params, noiseReduction, postProcess),
+ * raw_converter.cpp:148-248. raw is width x height uint16 (stride in bytes).
+ * If out->data is NULL, *out is filled with a view of the converter-owned
+ * device output (4 ch RGBA, w = 0), valid until the next call on this
+ * converter, as in the reference (RawProcessor.mm:75-78). Otherwise the
+ * result is written to out->data in out->dtype (GLS_F32 or GLS_F16),
+ * 4 channels. stream is a cudaStream_t (NULL = legacy default stream). */
+gls_status gls_demosaic(gls_converter* conv, const uint16_t* raw, int32_t width, int32_t height,
+                        size_t raw_stride_bytes, const gls_demosaic_params* params, uint32_t flags,
+                        gls_image_view* out, void* stream);
+
+/* One frame of a batch. */
+typedef struct gls_frame_desc {
+    const uint16_t* raw;
+    int32_t width;
+    int32_t height;
+    size_t raw_stride_bytes;
+    const gls_demosaic_params* params;
+    gls_image_view out;
+} gls_frame_desc;
+
+/* Batched RawConverter::demosaic over frames of uneven sizes (no reference
+ * counterpart: the reference converts one frame per call). */
+gls_status gls_demosaic_batch(gls_converter* conv, gls_frame_desc* frames, int32_t n_frames,
+                              uint32_t flags, void* stream);
+
+/* PyramidProcessor<levels>::denoise, pyramid_processor.cpp:96-172, on a
+ * YCbCr image (4 ch) and its gradient (2 ch), both device memory (or host
+ * with GLS_HOST_IO). Result: 4 ch denoised YCbCr (w = kernel norm). */
+gls_status gls_pyramid_denoise(gls_converter* conv, const gls_image_view* ycc,
+                               const gls_image_view* gradient, const gls_demosaic_params* params,
+                               uint32_t flags, gls_image_view* out, void* stream);
+
+/* View of an internal plane of the last call (device memory). */
+gls_status gls_converter_plane(gls_converter* conv, int32_t which, gls_image_view* view);
+
+/* Strided copy between two views of equal width, height, channels and
+ * dtype (no reference counterpart: the reference maps shared-storage
+ * textures, gls_mtl_image.hpp:117-208). direction: GLS_COPY_D2H,
+ * GLS_COPY_D2D or GLS_COPY_H2D. Synchronous for D2H. */
+enum { GLS_COPY_D2H = 0, GLS_COPY_D2D = 1, GLS_COPY_H2D = 2 };
+gls_status gls_copy_view(const gls_image_view* src, gls_image_view* dst, int32_t direction, void* stream);
+
+/* PCA basis of a pyramid level from the last denoise: 25 x 8 floats,
+ * row-major (pcaSpace[row][component], pyramid_processor.hpp:46). */
+gls_status gls_converter_pca_basis(gls_converter* conv, int32_t level, float* basis25x8);
+
+/* ---- launch accounting (no reference counterpart; the reference prints
+ *      wall-clock timers, pipelineTest.cpp:161-169) ----
+ * Every kernel launch of a converter is counted per kernel class. With
+ * profiling enabled, each launch is also bracketed by CUDA events on its
+ * stream; gls_converter_stats synchronises the device and reports the
+ * summed device time per class. */
+typedef struct gls_kernel_stat {
+    const char* name;
+    uint64_t launches;
+    double ms;              /* summed event time (0 unless profiling) */
+} gls_kernel_stat;
+gls_status gls_converter_set_profiling(gls_converter* conv, int32_t enable);
+gls_status gls_converter_stats(gls_converter* conv, gls_kernel_stat* stats, int32_t max_stats, int32_t* n_stats);
+gls_status gls_converter_reset_stats(gls_converter* conv);
+
+/* ---- CameraCalibration<levels> (CameraCalibration.hpp:24-39) ----
+ * Fills the noise model and the denoise schedule of a built-in camera for
+ * an ISO, as nlfFromIso() + getDenoiseParameters() do. Returns GLS_ERR_RANGE
+ * for an ISO the calibration does not cover. */
+enum { GLS_CAMERA_IPHONE14_WIDE = 0 };
+gls_status gls_calibration_fill(int32_t camera, int32_t iso, gls_demosaic_params* params);
+
+/* Gaussian kernel folded into bilinear taps (weight, dx, dy) per tap,
+ * gaussianKernelBilinearWeights, demosaic_utils.cpp:987-1006. Writes at
+ * most max_taps taps; *n_taps receives the count. */
+gls_status gls_gaussian_bilinear_taps(float radius, float* taps, int32_t max_taps, int32_t* n_taps);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GLSCAM_H */

@@ -1,0 +1,199 @@
+// oracle_capi.cpp — TEST INFRASTRUCTURE ONLY. extern "C" entry points of the
+// CPU oracle (gls_oracle.hpp) for the pytest suite and the CPU-baseline leg
+// of bench.py, called through ctypes. Parameters arrive in the library's own
+// gls_demosaic_params layout (include/glscam.h) so that both sides read one
+// struct. Parity of the oracle: see the header of gls_oracle.hpp.
+#include <chrono>
+#include <cstdio>
+
+#include "../include/glscam.h"
+#include "gls_oracle.hpp"
+
+using namespace orc;
+
+static Params to_params(const gls_demosaic_params* g) {
+    Params p;
+    p.bayer = g->bayer_pattern;
+    p.black = g->black_level;
+    p.white = g->white_level;
+    p.lsc = g->lens_shading_correction;
+    for (int c = 0; c < 4; c++) p.scale_mul[c] = g->scale_mul[c];
+    for (int i = 0; i < 9; i++) {
+        p.rgb_cam[i] = g->rgb_cam[i];
+        p.xyz_rgb[i] = g->xyz_rgb[i];
+    }
+    p.high_noise = g->high_noise_image != 0;
+    p.raw_strength = g->raw_denoise_strength;
+    for (int c = 0; c < 4; c++) {
+        p.raw_nlf.a[c] = g->raw_nlf.a[c];
+        p.raw_nlf.b[c] = g->raw_nlf.b[c];
+    }
+    for (int l = 0; l < 5; l++) {
+        for (int c = 0; c < 3; c++) {
+            p.pyr_nlf[l].a[c] = g->pyramid_nlf[l].a[c];
+            p.pyr_nlf[l].b[c] = g->pyramid_nlf[l].b[c];
+        }
+        p.dn[l].luma = g->denoise[l].luma;
+        p.dn[l].chroma = g->denoise[l].chroma;
+        p.dn[l].chromaBoost = g->denoise[l].chroma_boost;
+        p.dn[l].gradientBoost = g->denoise[l].gradient_boost;
+        p.dn[l].gradientThreshold = g->denoise[l].gradient_threshold;
+        p.dn[l].sharpening = g->denoise[l].sharpening;
+    }
+    p.levels = g->levels;
+    return p;
+}
+
+template <class T, int C>
+static void copy_out(const Img<T, C>& img, float* dst) {
+    if (!dst) return;
+    for (size_t i = 0; i < img.d.size(); i++) dst[i] = float(img.d[i]);
+}
+
+template <class T, int C>
+static Img<T, C> copy_in(const float* src, int w, int h) {
+    Img<T, C> img(w, h);
+    for (size_t i = 0; i < img.d.size(); i++) img.d[i] = T(src[i]);
+    return img;
+}
+
+template <class T>
+static void run_pipeline(const uint16_t* raw, int w, int h, size_t stride, const gls_demosaic_params* gp,
+                         int denoise, float* out, float* scaled, float* grad, float* demosaiced,
+                         float* despeckled, double* bases) {
+    const Params p = to_params(gp);
+    Stages st;
+    st.keep = scaled || grad || demosaiced || despeckled;
+    PyramidOut info;
+    auto res = raw_pipeline<T>(raw, stride, w, h, p, denoise != 0, &st, &info);
+    copy_out(res, out);
+    if (st.keep) {
+        copy_out(st.scaled, scaled);
+        copy_out(st.gradient, grad);
+        copy_out(st.demosaiced, demosaiced);
+        if (denoise) copy_out(st.despeckled, despeckled);
+    }
+    if (bases && denoise) {
+        for (size_t l = 0; l < info.bases.size(); l++)
+            for (int r = 0; r < 25; r++)
+                for (int c = 0; c < 8; c++) bases[(l * 25 + r) * 8 + c] = info.bases[l][r][c];
+    }
+}
+
+extern "C" {
+
+void orc_set_threads(int n) { num_threads() = n > 0 ? n : 1; }
+int orc_get_threads(void) { return num_threads(); }
+
+// RawConverter::demosaic on the CPU. f64 selects the double "truth" run.
+// Optional outputs may be NULL: scaled (w*h), grad (w*h*2), demosaiced and
+// despeckled (w*h*4), bases (levels*25*8 doubles).
+int orc_raw_pipeline(const uint16_t* raw, int w, int h, size_t stride_elems, const gls_demosaic_params* p,
+                     int denoise, int f64, float* out_rgba, float* scaled, float* grad, float* demosaiced,
+                     float* despeckled, double* bases) {
+    if (!raw || !p || w < 2 || h < 2 || p->levels < 1 || p->levels > 5) return 1;
+    if (f64)
+        run_pipeline<double>(raw, w, h, stride_elems, p, denoise, out_rgba, scaled, grad, demosaiced, despeckled, bases);
+    else
+        run_pipeline<float>(raw, w, h, stride_elems, p, denoise, out_rgba, scaled, grad, demosaiced, despeckled, bases);
+    return 0;
+}
+
+// PyramidProcessor::denoise on the CPU, from a YCbCr RGBA image and a 2-ch
+// gradient. den_levels (optional) receives the denoised level images packed
+// one after the other (4 ch each, level sizes w>>i x h>>i).
+int orc_pyramid_denoise(const float* ycc, const float* grad, int w, int h, const gls_demosaic_params* gp, int f64,
+                        float* out, float* den_levels, double* bases) {
+    const Params p = to_params(gp);
+    auto run = [&](auto tag) {
+        using T = decltype(tag);
+        auto img = copy_in<T, 4>(ycc, w, h);
+        auto g = copy_in<T, 2>(grad, w, h);
+        std::vector<Plane4<T>> levels;
+        PyramidOut info;
+        auto res = pyramid_denoise<T>(img, g, p, &levels, &info);
+        copy_out(res, out);
+        if (den_levels) {
+            size_t off = 0;
+            for (auto& l : levels) {
+                copy_out(l, den_levels + off);
+                off += l.d.size();
+            }
+        }
+        if (bases)
+            for (size_t l = 0; l < info.bases.size(); l++)
+                for (int r = 0; r < 25; r++)
+                    for (int c = 0; c < 8; c++) bases[(l * 25 + r) * 8 + c] = info.bases[l][r][c];
+    };
+    if (f64) run(double());
+    else run(float());
+    return 0;
+}
+
+int orc_gaussian_taps(float radius, float* taps, int max_taps, int* n) {
+    Taps t = gaussian_bilinear_taps(radius);
+    *n = int(t.t.size());
+    if (int(t.t.size()) > max_taps) return 1;
+    for (size_t i = 0; i < t.t.size(); i++)
+        for (int k = 0; k < 3; k++) taps[i * 3 + k] = t.t[i][k];
+    return 0;
+}
+
+void orc_cam_ycbcr(const float* rgb_cam, const float* xyz_rgb, float* fwd, float* inv) {
+    Mat3 m = cam_ycbcr(rgb_cam, xyz_rgb);
+    Mat3 mi = inverse3(m);
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            fwd[i * 3 + j] = m.m[i][j];
+            inv[i * 3 + j] = mi.m[i][j];
+        }
+}
+
+// Bayer quad pack then unpack (bayerToRawRGBA o rawRGBAToBayer), identity.
+int orc_bayer_roundtrip(const float* raw, int w, int h, int pattern, float* rgba, float* back) {
+    auto img = copy_in<float, 1>(raw, w, h);
+    auto q = bayer_to_rgba(img, pattern);
+    copy_out(q, rgba);
+    Plane<float> b(w, h);
+    rgba_to_bayer(q, pattern, b);
+    copy_out(b, back);
+    return 0;
+}
+
+// Pyramid downsample of a C-channel float image (C = 2 or 4).
+int orc_downsample(const float* in, int w, int h, int ch, int ow, int oh, int f64, float* out) {
+    auto run = [&](auto tag) {
+        using T = decltype(tag);
+        if (ch == 4) copy_out(downsample<T, 4>(copy_in<T, 4>(in, w, h), ow, oh, 4), out);
+        else copy_out(downsample<T, 2>(copy_in<T, 2>(in, w, h), ow, oh, 2), out);
+    };
+    if (ch != 2 && ch != 4) return 1;
+    if (f64) run(double());
+    else run(float());
+    return 0;
+}
+
+// PCA basis (25 x 8, row-major) of the luma of a 4-channel float image.
+int orc_pca_basis(const float* img4, int w, int h, double* basis) {
+    auto img = copy_in<double, 4>(img4, w, h);
+    auto b = pca_basis(img);
+    for (int r = 0; r < 25; r++)
+        for (int c = 0; c < 8; c++) basis[r * 8 + c] = b[r][c];
+    return 0;
+}
+
+// Symmetric eigen-decomposition (values descending, vectors as columns).
+int orc_jacobi(int n, const double* a, double* evals, double* evecs) {
+    std::vector<double> m(a, a + size_t(n) * n), v;
+    jacobi_eigen(n, m, v);
+    std::vector<int> idx(n);
+    for (int i = 0; i < n; i++) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return m[x * n + x] > m[y * n + y]; });
+    for (int c = 0; c < n; c++) {
+        evals[c] = m[idx[c] * n + idx[c]];
+        for (int r = 0; r < n; r++) evecs[r * n + c] = v[r * n + idx[c]];
+    }
+    return 0;
+}
+
+}  // extern "C"
