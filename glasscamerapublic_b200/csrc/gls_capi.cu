@@ -90,7 +90,7 @@ struct Pipeline {
         GLS_TRY(A.ensure(n * 4 * sizeof(S)));
         GLS_TRY(B.ensure(n * 4 * sizeof(S)));
         GLS_TRY(pca.ensure(n * 8 * sizeof(S)));
-        GLS_TRY(acc.ensure(sizeof(double) * kPcaAcc * GLS_MAX_LEVELS));
+        GLS_TRY(acc.ensure(sizeof(double) * kPcaAcc * kPcaMaxBlocks * GLS_MAX_LEVELS));
         GLS_TRY(basis.ensure(sizeof(float) * 200 * GLS_MAX_LEVELS));
         GLS_TRY(status.ensure(sizeof(int) * GLS_MAX_LEVELS));
         for (int i = 0; i < levels; i++) {
@@ -299,23 +299,26 @@ static gls_status pyramid_run(gls_converter* cv, Pipeline<S>& P, Plane<S, 4> img
                                      layer, sa, s);
         }
         const int n_patches = (wi / 8) * (hi / 8);
+        const int n_blocks = pca_cov_blocks(wi, hi);
+        double* part = acc + size_t(i) * kPcaAcc * kPcaMaxBlocks;
         {
-            KScope k(cv->prof, KC_PCA_COV, s, n_patches > 0 ? 1 : 0);
-            launch_pca_cov<S>(layer, acc + i * kPcaAcc, s);
+            KScope k(cv->prof, KC_PCA_COV, s, n_blocks > 0 ? 1 : 0);
+            launch_pca_cov<S>(layer, part, s);
         }
         if (flags & GLS_HOST_PCA) {
-            P.host_acc.resize(kPcaAcc);
+            P.host_acc.resize(size_t(kPcaAcc) * std::max(1, n_blocks));
             P.host_basis.resize(200);
-            GLS_CUDA(cudaMemcpyAsync(P.host_acc.data(), acc + i * kPcaAcc, sizeof(double) * kPcaAcc,
-                                     cudaMemcpyDeviceToHost, s));
+            if (n_blocks > 0)
+                GLS_CUDA(cudaMemcpyAsync(P.host_acc.data(), part, sizeof(double) * kPcaAcc * n_blocks,
+                                         cudaMemcpyDeviceToHost, s));
             GLS_CUDA(cudaStreamSynchronize(s));  // the reference's per-level wait, pyramid_processor.cpp:148
-            host_pca_basis(P.host_acc.data(), n_patches, P.host_basis.data());
+            host_pca_basis(P.host_acc.data(), n_blocks, n_patches, P.host_basis.data());
             GLS_CUDA(cudaMemcpyAsync(basis + i * 200, P.host_basis.data(), sizeof(float) * 200,
                                      cudaMemcpyHostToDevice, s));
             GLS_CUDA(cudaStreamSynchronize(s));
         } else {
             KScope k(cv->prof, KC_PCA_EIGEN, s);
-            launch_pca_eigen(acc + i * kPcaAcc, n_patches, basis + i * 200, status + i, s);
+            launch_pca_eigen(part, n_blocks, n_patches, basis + i * 200, status + i, s);
         }
         Plane<S, 8> pcap = plane<S, 8>(P.pca, wi, hi);
         {

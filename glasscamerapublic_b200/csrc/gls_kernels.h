@@ -74,10 +74,12 @@ struct SubtractArgs {
     float luma_weight, sharpening, nlf_a, nlf_b;
 };
 
-// PCA accumulators of one level: sum of (p - shift) over patches (25) and
-// the upper triangle of sum (p - shift)(p - shift)^T (325), FP64.
+// PCA accumulators of one level: the upper triangle of sum p p^T over the
+// patches (325, row-major) followed by sum p (25), FP64.
 constexpr int kPcaAcc = 25 + 325;
 constexpr int kPcaDim = 25, kPcaComp = 8;
+constexpr int kPcaMaxBlocks = 296;  // covariance blocks (2 per SM); partials: kPcaMaxBlocks x kPcaAcc FP64
+int pca_cov_blocks(int w, int h);
 
 template <class S, int C>
 void launch_downsample(Plane<S, C> in, Plane<S, C> out, cudaStream_t s);
@@ -85,8 +87,9 @@ template <class S>
 void launch_subtract_noise(Plane<S, 4> in, Plane<S, 4> coarse, Plane<S, 4> coarse_den, Plane<S, 2> grad,
                            Plane<S, 4> out, const SubtractArgs& a, cudaStream_t s);
 template <class S>
-void launch_pca_cov(Plane<S, 4> img, double* acc, cudaStream_t s);
-void launch_pca_eigen(const double* acc, int n_patches, float* basis /*25x8*/, int* status, cudaStream_t s);
+void launch_pca_cov(Plane<S, 4> img, double* part, cudaStream_t s);
+void launch_pca_eigen(const double* part, int n_blocks, int n_patches, float* basis /*25x8*/, int* status,
+                      cudaStream_t s);
 template <class S>
 void launch_pca_project(Plane<S, 4> img, const float* basis, Plane<S, 8> out, cudaStream_t s);
 template <class S>
@@ -95,6 +98,54 @@ void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, Plan
 
 // host-side eigen-solve of the same accumulators (the reference's per-level
 // host PCA, pyramid_processor.cpp:148-149)
-void host_pca_basis(const double* acc, int n_patches, float* basis);
+void host_pca_basis(const double* part, int n_blocks, int n_patches, float* basis);
+
+// Top-8 basis (row-major 25 x 8, FP32) from eigenpairs sorted by decreasing
+// eigenvalue: ev[c] and column c of evec (row stride ld). Columns whose
+// eigenvalue is not above 1e-9 x the largest lie in a null space that a
+// solver fills arbitrarily (fewer than 26 patches, or a flat level); they
+// are completed deterministically by Gram-Schmidt of the unit vectors
+// e0, e1, ... against the previous columns. Each column is signed so that
+// its largest-magnitude entry (first on ties) is positive. work: 200 doubles.
+__host__ __device__ inline void select_pca_basis(const double* ev, const double* evec, int ld, double* work,
+                                                 float* basis) {
+    const double lam0 = ev[0] > 0.0 ? ev[0] : 0.0;
+    const double tol = 1e-9 * lam0;
+    int cand = 0;
+    bool kept = true;
+    for (int c = 0; c < 8; c++) {
+        double* v = work + c * 25;
+        kept = kept && lam0 > 0.0 && ev[c] > tol;
+        if (kept) {
+            for (int r = 0; r < 25; r++) v[r] = evec[r * ld + c];
+        } else {
+            for (int guard = 0; guard < 25; guard++) {
+                for (int r = 0; r < 25; r++) v[r] = (r == cand) ? 1.0 : 0.0;
+                cand++;
+                for (int pass = 0; pass < 2; pass++)
+                    for (int k = 0; k < c; k++) {
+                        const double* b = work + k * 25;
+                        double d = 0;
+                        for (int r = 0; r < 25; r++) d += b[r] * v[r];
+                        for (int r = 0; r < 25; r++) v[r] -= d * b[r];
+                    }
+                double nn = 0;
+                for (int r = 0; r < 25; r++) nn += v[r] * v[r];
+                if (nn > 0.25) {
+                    const double inv = 1.0 / sqrt(nn);
+                    for (int r = 0; r < 25; r++) v[r] *= inv;
+                    break;
+                }
+            }
+        }
+        int amax = 0;
+        for (int r = 1; r < 25; r++)
+            if (fabs(v[r]) > fabs(v[amax])) amax = r;
+        const double sgn = v[amax] < 0 ? -1.0 : 1.0;
+        for (int r = 0; r < 25; r++) v[r] *= sgn;
+    }
+    for (int c = 0; c < 8; c++)
+        for (int r = 0; r < 25; r++) basis[r * 8 + c] = float(work[c * 25 + r]);
+}
 
 }  // namespace gls

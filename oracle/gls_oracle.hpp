@@ -744,7 +744,7 @@ inline void jacobi_eigen(int n, std::vector<double>& a, std::vector<double>& v) 
                 tot += a[i * n + j] * a[i * n + j];
                 if (i != j) off += a[i * n + j] * a[i * n + j];
             }
-        if (off <= 1e-30 * tot || off == 0) break;
+        if (off <= 1e-26 * tot || off == 0) break;  // off-diagonal norm <= 1e-13 x total
         for (int p = 0; p < n - 1; p++)
             for (int q = p + 1; q < n; q++) {
                 const double apq = a[p * n + q];
@@ -772,13 +772,55 @@ inline void jacobi_eigen(int n, std::vector<double>& a, std::vector<double>& v) 
     }
 }
 
+// Top-8 basis from eigenpairs sorted by decreasing eigenvalue (ev[c], column
+// c of evec). Eigenvectors whose eigenvalue is not above 1e-9 x the largest
+// (a rank-deficient sample: fewer than 26 patches, or a flat image) span a
+// null space whose basis any solver picks arbitrarily; those columns are
+// instead completed deterministically by Gram-Schmidt of the unit vectors
+// e0, e1, ... against the columns before them. Every column's sign is fixed
+// so that its largest-magnitude entry (first on ties) is positive.
+inline void select_basis(const double ev[25], const double evec[25][25], std::array<std::array<double, 8>, 25>& basis) {
+    const double lam0 = std::max(ev[0], 0.0);
+    const double tol = 1e-9 * lam0;
+    int cand = 0;
+    bool kept = true;
+    for (int c = 0; c < 8; c++) {
+        double v[25];
+        kept = kept && lam0 > 0 && ev[c] > tol;
+        if (kept) {
+            for (int r = 0; r < 25; r++) v[r] = evec[r][c];
+        } else {
+            for (;;) {
+                for (int r = 0; r < 25; r++) v[r] = (r == cand) ? 1.0 : 0.0;
+                cand++;
+                for (int pass = 0; pass < 2; pass++)
+                    for (int k = 0; k < c; k++) {
+                        double d = 0;
+                        for (int r = 0; r < 25; r++) d += basis[r][k] * v[r];
+                        for (int r = 0; r < 25; r++) v[r] -= d * basis[r][k];
+                    }
+                double nn = 0;
+                for (int r = 0; r < 25; r++) nn += v[r] * v[r];
+                if (nn > 0.25) {
+                    const double inv = 1.0 / std::sqrt(nn);
+                    for (int r = 0; r < 25; r++) v[r] *= inv;
+                    break;
+                }
+            }
+        }
+        int amax = 0;
+        for (int r = 1; r < 25; r++)
+            if (std::abs(v[r]) > std::abs(v[amax])) amax = r;
+        const double sgn = v[amax] < 0 ? -1.0 : 1.0;
+        for (int r = 0; r < 25; r++) basis[r][c] = sgn * v[r];
+    }
+}
+
 // collectPatches + build_pca_space<25, 8>, demosaic.metal:755-772 and
 // PCA.cpp:23-56: 5x5 luma patches on the 8-pixel grid, mean-centred
 // covariance / (n - 1) (accumulated in double), top-8 eigenvectors in
-// decreasing eigenvalue order. Each eigenvector's sign is fixed so that its
-// largest-magnitude component is positive (the sign is free: only distances
-// in the projected space are used). Fewer than 2 patches: the first 8 unit
-// vectors.
+// decreasing eigenvalue order (select_basis). Fewer than 2 patches: the
+// first 8 unit vectors.
 template <class T>
 std::array<std::array<double, 8>, 25> pca_basis(const Plane4<T>& img) {
     const int gw = img.w / 8, gh = img.h / 8;
@@ -816,14 +858,12 @@ std::array<std::array<double, 8>, 25> pca_basis(const Plane4<T>& img) {
     int idx[25];
     for (int i = 0; i < 25; i++) idx[i] = i;
     std::stable_sort(idx, idx + 25, [&](int a, int b) { return cov[a * 25 + a] > cov[b * 25 + b]; });
-    for (int c = 0; c < 8; c++) {
-        const int e = idx[c];
-        int amax = 0;
-        for (int r = 1; r < 25; r++)
-            if (std::abs(vec[r * 25 + e]) > std::abs(vec[amax * 25 + e])) amax = r;
-        const double sgn = vec[amax * 25 + e] < 0 ? -1.0 : 1.0;
-        for (int r = 0; r < 25; r++) basis[r][c] = sgn * vec[r * 25 + e];
+    double ev[25], evec[25][25];
+    for (int c = 0; c < 25; c++) {
+        ev[c] = cov[idx[c] * 25 + idx[c]];
+        for (int r = 0; r < 25; r++) evec[r][c] = vec[r * 25 + idx[c]];
     }
+    select_basis(ev, evec, basis);
     return basis;
 }
 
