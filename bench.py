@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--workload", default=WORKLOAD, help="workload name (cfg2_4032x3024 or cfg1_1024x768)")
+    ap.add_argument("--quick", action="store_true", help="timed FP16 loop only (for profiler captures)")
     return ap.parse_args()
 
 
@@ -177,7 +179,7 @@ def main():
         if world > 1:
             dist.barrier()
 
-    wl = scene.WORKLOADS[WORKLOAD]
+    wl = scene.WORKLOADS[args.workload]
     params = scene.make_params(wl)
     conv = g.RawConverter(local)
     stream = torch.cuda.Stream()
@@ -219,6 +221,13 @@ def main():
         lib.gls_converter_stats(conv.handle, stats, 32, C.byref(n))
         launches = int(sum(stats[i].launches for i in range(n.value)))
         barrier()
+
+        if args.quick:
+            if rank == 0:
+                print(json.dumps({"quick": True, "workload": args.workload, "ms_per_step": ms / args.steps,
+                                  "gpu_launches": launches}), flush=True)
+            conv.close()
+            return
 
         # per-kernel device time inside an identical timed loop (events around
         # each launch, on the launch stream)
@@ -293,7 +302,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f16-storage/f32-math", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "frame": f"{W}x{H} RGGB 12-bit", "levels": wl.levels, "iso": wl.iso,
+        "config": {"workload": args.workload, "frame": f"{W}x{H} RGGB 12-bit", "levels": wl.levels, "iso": wl.iso,
                    "frames_rotated": N_ROTATE, "l2": "inputs + planes per frame > 126 MB L2 (6 rotating frames)",
                    "parallelism": f"frames sharded over {world} rank(s)"},
         "e2e": {"value": world / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": W * H * 2,

@@ -1,0 +1,354 @@
+// gls_blockmatch.cu — blockMatchingDenoiseImage (demosaic.metal:806-884):
+// 21 x 21 non-local means with a PCA-space patch distance for luma, a
+// chroma distance for chroma and a fixed spatial Gaussian:
+//   lw = exp(-2 (|p - q|_8 s)^2),   s = 1 / (luma_mult sigma_Y (1 + gb edge))
+//   cw = exp(-2 (lw^2 + (dCb m1 / cb)^2 + (dCr m2 / cb)^2))
+//   w  = gaussian(0.1 |(i, j)|) * (lw, cw, cw)
+// accumulated in FP32; output (Y, Cb, Cr, sum of luma weights).
+//
+// Both kernels stage the tile's window region (halo 10) in shared memory
+// and give each thread a column of vertically adjacent pixels, which share
+// all but one of their window rows: one staged neighbour feeds several
+// taps. The kernel for the FP32 plain path evaluates the formula directly
+// with correctly rounded exponentials (parity with the oracle's FP32 run);
+// the FP16-storage path's kernel is arranged for the fewest FMA-pipe and
+// shared-memory operations per tap.
+#include <cmath>
+
+#include "gls_common.cuh"
+#include "gls_kernels.h"
+
+namespace gls {
+
+__device__ __forceinline__ __half2 u2h_(uint32_t u) { return *reinterpret_cast<__half2*>(&u); }
+
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Per-pixel constants shared by both kernels.
+struct BmConst {
+    float in_y, in_cb, in_cr;
+    float s;       // luma distance scale
+    float c1, c2;  // chroma scales (dm / chroma_boost)
+};
+
+template <class S>
+__device__ __forceinline__ BmConst bm_const(const BlockMatchArgs& a, Plane<S, 2> grad, int w, int h, int px, int py,
+                                            float y, float cb, float cr) {
+    BmConst k;
+    k.in_y = y;
+    k.in_cb = cb;
+    k.in_cr = cr;
+    float ls = 1.f;
+    if (a.lsc > 0.f) {  // lensShading, demosaic.metal:91-93, at the pixel
+        const float cx = float(w / 2), cy = float(h / 2);
+        const float dx = float(px) - cx, dy = float(py) - cy;
+        const float rr = sqrtf(dx * dx + dy * dy) / sqrtf(cx * cx + cy * cy);
+        ls = 1.f + a.lsc * rr * rr;
+    }
+    const float sig0 = sqrtf(a.var_a[0] + a.var_b[0] * ls * y);
+    const float sig1 = sqrtf(a.var_a[1] + a.var_b[1] * ls * y);
+    const float sig2 = sqrtf(a.var_a[2] + a.var_b[2] * ls * y);
+    const float dm0 = 1.f / (a.tm[0] * sig0), dm1 = 1.f / (a.tm[1] * sig1), dm2 = 1.f / (a.tm[2] * sig2);
+    const f2 g = ld2<S>(grad.px(px, py));
+    const float mag = sqrtf(g.x * g.x + g.y * g.y);
+    const float edge = smoothstepf(2.f, 16.f, a.gradient_threshold * mag / sig0);
+    k.s = dm0 / (1.f + a.gradient_boost * edge);
+    k.c1 = dm1 / a.chroma_boost;
+    k.c2 = dm2 / a.chroma_boost;
+    return k;
+}
+
+__device__ __forceinline__ float spatial_weight(int i, int j) {  // gaussian(0.1 |(i, j)|)
+    const float d = 0.1f * sqrtf(float(i * i + j * j));
+    return expf(-2.f * d * d);
+}
+
+// ============================================================ FP32 plain path
+// Two vertically adjacent pixels per thread, tile 32 x 16, FP32 staging.
+constexpr int BP_TX = 32, BP_TY = 8, BP_W = BP_TX + 20, BP_H = 2 * BP_TY + 20;
+
+struct BmPlainSmem {
+    float4 pca[BP_H * BP_W][2];
+    float4 ycc[BP_H * BP_W];
+    float spatial[21 * 21];
+};
+
+struct BmPlainPix {
+    float4 p0, p1;
+    float kl;              // -2 log2(e) s^2
+    float c1, c2, o1, o2;  // sqrt(2 log2 e) c, times the centre chroma
+};
+
+template <bool UP, bool LO>
+__device__ __forceinline__ void bmp_row(const BmPlainSmem& sm, int base, int r, const BmPlainPix& u,
+                                        const BmPlainPix& l, float (&acc)[10]) {
+    const float kLk = 2.f * 1.4426950408889634f;
+#pragma unroll
+    for (int i = 0; i < 21; i++) {
+        const float4 q0 = sm.pca[base + i][0], q1 = sm.pca[base + i][1];
+        const float4 y = sm.ycc[base + i];
+        auto tap = [&](const BmPlainPix& p, int j, int o) {
+            float d, d2;
+            d = q0.x - p.p0.x; d2 = d * d;
+            d = q0.y - p.p0.y; d2 = fmaf(d, d, d2);
+            d = q0.z - p.p0.z; d2 = fmaf(d, d, d2);
+            d = q0.w - p.p0.w; d2 = fmaf(d, d, d2);
+            d = q1.x - p.p1.x; d2 = fmaf(d, d, d2);
+            d = q1.y - p.p1.y; d2 = fmaf(d, d, d2);
+            d = q1.z - p.p1.z; d2 = fmaf(d, d, d2);
+            d = q1.w - p.p1.w; d2 = fmaf(d, d, d2);
+            const float lw = exp2f(p.kl * d2);
+            const float e1 = fmaf(p.c1, y.y, -p.o1), e2 = fmaf(p.c2, y.z, -p.o2);
+            const float cw = exp2f(-fmaf(kLk * lw, lw, fmaf(e1, e1, e2 * e2)));
+            const float sw = sm.spatial[j * 21 + i];
+            const float wy = sw * lw, wc = sw * cw;
+            acc[o + 0] = fmaf(wy, y.x, acc[o + 0]);
+            acc[o + 1] = fmaf(wc, y.y, acc[o + 1]);
+            acc[o + 2] = fmaf(wc, y.z, acc[o + 2]);
+            acc[o + 3] += wy;
+            acc[o + 4] += wc;
+        };
+        if (UP) tap(u, r, 0);
+        if (LO) tap(l, r - 1, 5);
+    }
+}
+
+template <class S>
+__global__ void __launch_bounds__(256) k_block_match_plain(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca,
+                                                           Plane<S, 4> out, BlockMatchArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BmPlainSmem& sm = *reinterpret_cast<BmPlainSmem*>(smem_raw);
+    const int x0 = blockIdx.x * BP_TX, y0 = blockIdx.y * (2 * BP_TY);
+    const int tid = threadIdx.y * BP_TX + threadIdx.x;
+    for (int k = tid; k < 441; k += 256) sm.spatial[k] = spatial_weight(k % 21 - 10, k / 21 - 10);
+    for (int k = tid; k < BP_W * BP_H; k += 256) {
+        const int ty = k / BP_W, tx = k % BP_W;
+        const int sx = clampi(x0 - 10 + tx, 0, img.w - 1), sy = clampi(y0 - 10 + ty, 0, img.h - 1);
+        const S* q = pca.px(sx, sy);
+        if constexpr (is_half<S>::value) {
+            const uint4 u = *reinterpret_cast<const uint4*>(q);
+            const float2 a0 = __half22float2(u2h_(u.x)), a1 = __half22float2(u2h_(u.y));
+            const float2 a2 = __half22float2(u2h_(u.z)), a3 = __half22float2(u2h_(u.w));
+            sm.pca[k][0] = make_float4(a0.x, a0.y, a1.x, a1.y);
+            sm.pca[k][1] = make_float4(a2.x, a2.y, a3.x, a3.y);
+        } else {
+            const float4* q4 = reinterpret_cast<const float4*>(q);
+            sm.pca[k][0] = q4[0];
+            sm.pca[k][1] = q4[1];
+        }
+        const f4 p = ld4<S>(img.px(sx, sy));
+        sm.ycc[k] = make_float4(p.x, p.y, p.z, 0.f);
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.x, yu = y0 + 2 * threadIdx.y;
+    const float kLog2e = 1.4426950408889634f, sq = sqrtf(2.f * kLog2e);
+    BmPlainPix pix[2];
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+        const int c = (2 * threadIdx.y + p + 10) * BP_W + threadIdx.x + 10;
+        const float4 in = sm.ycc[c];
+        const BmConst k = bm_const<S>(a, grad, img.w, img.h, min(x, img.w - 1), min(yu + p, img.h - 1), in.x, in.y, in.z);
+        BmPlainPix& P = pix[p];
+        P.p0 = sm.pca[c][0];
+        P.p1 = sm.pca[c][1];
+        P.kl = -2.f * kLog2e * k.s * k.s;
+        P.c1 = sq * k.c1;
+        P.c2 = sq * k.c2;
+        P.o1 = P.c1 * in.y;
+        P.o2 = P.c2 * in.z;
+    }
+    float acc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const int col = threadIdx.x, row0 = 2 * threadIdx.y;
+    bmp_row<true, false>(sm, row0 * BP_W + col, 0, pix[0], pix[1], acc);
+    for (int r = 1; r <= 20; r++) bmp_row<true, true>(sm, (row0 + r) * BP_W + col, r, pix[0], pix[1], acc);
+    bmp_row<false, true>(sm, (row0 + 21) * BP_W + col, 21, pix[0], pix[1], acc);
+    if (x < out.w) {
+        if (yu < out.h) st4<S>(out.px(x, yu), f4{acc[0] / acc[3], acc[1] / acc[4], acc[2] / acc[4], acc[3]});
+        if (yu + 1 < out.h) st4<S>(out.px(x, yu + 1), f4{acc[5] / acc[8], acc[6] / acc[9], acc[7] / acc[9], acc[8]});
+    }
+}
+
+// ============================================================ FP16-storage path
+// Four vertically adjacent pixels per thread (they share 18 of 24 window
+// rows; a staged neighbour feeds 3.5 taps on average), tile 32 x 32, 256
+// threads. Shared memory per window position: the PCA coefficients minus
+// the tile-centre pixel's, as 8 halves, and (Y, Cb, Cr, |q'|^2) in FP32.
+//   * |p - q|^2 = |p'|^2 + |q'|^2 - 2 p'.q' (an 8-FMA dot product); the
+//     centring keeps the cancellation error at FP32 rounding of the local
+//     variation of the coefficients;
+//   * lw is carried scaled by sqrt(2 log2 e), so the chroma exponent is
+//     three FMAs with log2(sw) folded in as the addend, and the luma weight
+//     is sw / sqrt(2 log2 e) times it;
+//   * both exponentials are ex2.approx (the reference uses half-precision
+//     exp under fast math here).
+constexpr int BX_NP = 4, BX_TX = 32, BX_TY = 8, BX_W = BX_TX + 20, BX_H = BX_NP * BX_TY + 20;
+
+struct BmFastSmem {
+    uint4 pca[BX_H * BX_W];   // q - c, 8 halves
+    float4 ycc[BX_H * BX_W];  // Y, Cb, Cr, |q - c|^2
+    float2 sp[21 * 21];       // (sw / sqrt(2 log2 e), log2 sw)
+};
+
+struct BmFastPix {
+    float4 p0, p1;   // p - c
+    float kl, klm2;  // kl = -2 log2(e) s^2, klm2 = -2 kl
+    float base;      // kl |p'|^2 + 0.5 log2(2 log2 e)
+    float c1, c2, o1, o2;
+};
+
+// One window row r (0 .. 23) of the thread's column; pixel p uses it when
+// p <= r <= p + 20 (bit p of MASK), with window row offset r - p.
+template <int MASK>
+__device__ __forceinline__ void bmx_row(const BmFastSmem& sm, int base, int r, const BmFastPix (&P)[BX_NP],
+                                        float (&acc)[BX_NP][5]) {
+#pragma unroll 7  // full unrolling spills past the 128-register budget of 2 blocks/SM
+    for (int i = 0; i < 21; i++) {
+        const uint4 u = sm.pca[base + i];
+        const float2 a0 = __half22float2(u2h_(u.x)), a1 = __half22float2(u2h_(u.y));
+        const float2 a2 = __half22float2(u2h_(u.z)), a3 = __half22float2(u2h_(u.w));
+        const float4 y = sm.ycc[base + i];
+#pragma unroll
+        for (int p = 0; p < BX_NP; p++) {
+            if (!(MASK & (1 << p))) continue;
+            const BmFastPix& q = P[p];
+            const float2 sw = sm.sp[(r - p) * 21 + i];
+            float dot = a0.x * q.p0.x;
+            dot = fmaf(a0.y, q.p0.y, dot);
+            dot = fmaf(a1.x, q.p0.z, dot);
+            dot = fmaf(a1.y, q.p0.w, dot);
+            dot = fmaf(a2.x, q.p1.x, dot);
+            dot = fmaf(a2.y, q.p1.y, dot);
+            dot = fmaf(a3.x, q.p1.z, dot);
+            dot = fmaf(a3.y, q.p1.w, dot);
+            const float lws = ex2_approx(fminf(fmaf(q.klm2, dot, fmaf(q.kl, y.w, q.base)), 2.f));
+            const float e1 = fmaf(q.c1, y.y, -q.o1), e2 = fmaf(q.c2, y.z, -q.o2);
+            const float wc = ex2_approx(fmaf(-lws, lws, fmaf(-e1, e1, fmaf(-e2, e2, sw.y))));
+            const float wy = sw.x * lws;
+            acc[p][0] = fmaf(wy, y.x, acc[p][0]);
+            acc[p][1] = fmaf(wc, y.y, acc[p][1]);
+            acc[p][2] = fmaf(wc, y.z, acc[p][2]);
+            acc[p][3] += wy;
+            acc[p][4] += wc;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256, 2) k_block_match_fast(Plane<__half, 4> img, Plane<__half, 2> grad,
+                                                             Plane<__half, 8> pca, Plane<__half, 4> out,
+                                                             BlockMatchArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BmFastSmem& sm = *reinterpret_cast<BmFastSmem*>(smem_raw);
+    __shared__ float cen[8];
+    const int x0 = blockIdx.x * BX_TX, y0 = blockIdx.y * (BX_NP * BX_TY);
+    const int tid = threadIdx.y * BX_TX + threadIdx.x;
+    const float kLog2e = 1.4426950408889634f, lk = 2.f * kLog2e, isq = rsqrtf(lk);
+    for (int k = tid; k < 441; k += 256) {
+        const float w = spatial_weight(k % 21 - 10, k / 21 - 10);
+        sm.sp[k] = make_float2(w * isq, log2f(w));
+    }
+    if (tid < 8) {  // centring vector: the tile-centre pixel's coefficients
+        const int cx = clampi(x0 + BX_TX / 2, 0, img.w - 1), cy = clampi(y0 + BX_NP * BX_TY / 2, 0, img.h - 1);
+        cen[tid] = __half2float(pca.px(cx, cy)[tid]);
+    }
+    __syncthreads();
+    for (int k = tid; k < BX_W * BX_H; k += 256) {
+        const int ty = k / BX_W, tx = k % BX_W;
+        const int sx = clampi(x0 - 10 + tx, 0, img.w - 1), sy = clampi(y0 - 10 + ty, 0, img.h - 1);
+        const uint4 u = *reinterpret_cast<const uint4*>(pca.px(sx, sy));
+        const float2 a0 = __half22float2(u2h_(u.x)), a1 = __half22float2(u2h_(u.y));
+        const float2 a2 = __half22float2(u2h_(u.z)), a3 = __half22float2(u2h_(u.w));
+        const __half2 h0 = __floats2half2_rn(a0.x - cen[0], a0.y - cen[1]);
+        const __half2 h1 = __floats2half2_rn(a1.x - cen[2], a1.y - cen[3]);
+        const __half2 h2 = __floats2half2_rn(a2.x - cen[4], a2.y - cen[5]);
+        const __half2 h3 = __floats2half2_rn(a3.x - cen[6], a3.y - cen[7]);
+        // the norm of the values as stored (rounded), so |p'-q'|^2 is exact in them
+        const float2 b0 = __half22float2(h0), b1 = __half22float2(h1), b2 = __half22float2(h2), b3 = __half22float2(h3);
+        const float n = b0.x * b0.x + b0.y * b0.y + b1.x * b1.x + b1.y * b1.y + b2.x * b2.x + b2.y * b2.y +
+                        b3.x * b3.x + b3.y * b3.y;
+        uint4 hv;
+        hv.x = *reinterpret_cast<const uint32_t*>(&h0);
+        hv.y = *reinterpret_cast<const uint32_t*>(&h1);
+        hv.z = *reinterpret_cast<const uint32_t*>(&h2);
+        hv.w = *reinterpret_cast<const uint32_t*>(&h3);
+        sm.pca[k] = hv;
+        const f4 p = ld4<__half>(img.px(sx, sy));
+        sm.ycc[k] = make_float4(p.x, p.y, p.z, n);
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.x, y = y0 + BX_NP * threadIdx.y;
+    BmFastPix P[BX_NP];
+#pragma unroll
+    for (int p = 0; p < BX_NP; p++) {
+        const int c = (BX_NP * threadIdx.y + p + 10) * BX_W + threadIdx.x + 10;
+        const float4 in = sm.ycc[c];
+        const uint4 u = sm.pca[c];
+        const float2 a0 = __half22float2(u2h_(u.x)), a1 = __half22float2(u2h_(u.y));
+        const float2 a2 = __half22float2(u2h_(u.z)), a3 = __half22float2(u2h_(u.w));
+        const BmConst k =
+            bm_const<__half>(a, grad, img.w, img.h, min(x, img.w - 1), min(y + p, img.h - 1), in.x, in.y, in.z);
+        BmFastPix& q = P[p];
+        q.p0 = make_float4(a0.x, a0.y, a1.x, a1.y);
+        q.p1 = make_float4(a2.x, a2.y, a3.x, a3.y);
+        q.kl = fmaxf(-2.f * kLog2e * k.s * k.s, -1e30f);
+        q.klm2 = -2.f * q.kl;
+        q.base = fmaf(q.kl, in.w, 0.5f * log2f(lk));
+        const float sq = sqrtf(lk);
+        q.c1 = sq * k.c1;
+        q.c2 = sq * k.c2;
+        q.o1 = q.c1 * in.y;
+        q.o2 = q.c2 * in.z;
+    }
+    float acc[BX_NP][5] = {};
+    const int col = threadIdx.x, row0 = BX_NP * threadIdx.y;
+    auto rb = [&](int r) { return (row0 + r) * BX_W + col; };
+    bmx_row<0x1>(sm, rb(0), 0, P, acc);
+    bmx_row<0x3>(sm, rb(1), 1, P, acc);
+    bmx_row<0x7>(sm, rb(2), 2, P, acc);
+    for (int r = 3; r <= 20; r++) bmx_row<0xF>(sm, rb(r), r, P, acc);
+    bmx_row<0xE>(sm, rb(21), 21, P, acc);
+    bmx_row<0xC>(sm, rb(22), 22, P, acc);
+    bmx_row<0x8>(sm, rb(23), 23, P, acc);
+    if (x < out.w) {
+#pragma unroll
+        for (int p = 0; p < BX_NP; p++)
+            if (y + p < out.h)
+                st4<__half>(out.px(x, y + p),
+                            f4{acc[p][0] / acc[p][3], acc[p][1] / acc[p][4], acc[p][2] / acc[p][4], acc[p][3]});
+    }
+}
+
+template <class S>
+void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, Plane<S, 4> out, const BlockMatchArgs& a,
+                        cudaStream_t s) {
+    if constexpr (is_half<S>::value) {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_block_match_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(BmFastSmem)));
+            attr = true;
+        }
+        dim3 b(BX_TX, BX_TY);
+        dim3 g((img.w + BX_TX - 1) / BX_TX, (img.h + BX_NP * BX_TY - 1) / (BX_NP * BX_TY));
+        k_block_match_fast<<<g, b, sizeof(BmFastSmem), s>>>(img, grad, pca, out, a);
+    } else {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_block_match_plain<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(sizeof(BmPlainSmem)));
+            attr = true;
+        }
+        dim3 b(BP_TX, BP_TY);
+        dim3 g((img.w + BP_TX - 1) / BP_TX, (img.h + 2 * BP_TY - 1) / (2 * BP_TY));
+        k_block_match_plain<S><<<g, b, sizeof(BmPlainSmem), s>>>(img, grad, pca, out, a);
+    }
+}
+
+template void launch_block_match<float>(Plane<float, 4>, Plane<float, 2>, Plane<float, 8>, Plane<float, 4>,
+                                        const BlockMatchArgs&, cudaStream_t);
+template void launch_block_match<__half>(Plane<__half, 4>, Plane<__half, 2>, Plane<__half, 8>, Plane<__half, 4>,
+                                         const BlockMatchArgs&, cudaStream_t);
+
+}  // namespace gls

@@ -1,8 +1,8 @@
 // gls_pyramid.cu — kernels of PyramidProcessor<levels>::denoise
 // (pyramid_processor.cpp:96-172): Gaussian-pyramid downsample, the
 // reconstruct (noise subtraction) step, the per-level PCA patch basis
-// (covariance + FP64 Jacobi eigen-solve on the device), the 5x5-patch PCA
-// projection and the 21x21 block-matching non-local-means denoise.
+// (covariance + FP64 Jacobi eigen-solve on the device) and the 5x5-patch
+// PCA projection. The block-matching denoise is in gls_blockmatch.cu.
 #include <cmath>
 #include <cstdio>
 
@@ -353,284 +353,6 @@ __global__ void __launch_bounds__(256) k_pca_project(Plane<S, 4> img, const floa
     }
 }
 
-// --------------------------------------------------------------------------
-// blockMatchingDenoiseImage, demosaic.metal:806-884. Output tile 16 x 16,
-// one pixel per thread; the tile's 36 x 36 window region of YCbCr and PCA
-// coefficients is staged in shared memory (FP32), the spatial Gaussian
-// gaussian(0.1 |(i, j)|) is a 21 x 21 table.
-constexpr int BM_T = 16, BM_R = 10, BM_W = BM_T + 2 * BM_R;
-
-struct BlockMatchSmem {
-    float4 pca[BM_W * BM_W][2];
-    float4 ycc[BM_W * BM_W];
-    float spatial[21 * 21];
-};
-
-template <class S>
-__global__ void __launch_bounds__(256) k_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca,
-                                                     Plane<S, 4> out, BlockMatchArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    BlockMatchSmem& sm = *reinterpret_cast<BlockMatchSmem*>(smem_raw);
-    constexpr bool fast = is_half<S>::value;
-    const int x0 = blockIdx.x * BM_T, y0 = blockIdx.y * BM_T;
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    for (int k = tid; k < 441; k += 256) {
-        const int i = k % 21 - 10, j = k / 21 - 10;
-        const float d = 0.1f * sqrtf(float(i * i + j * j));
-        sm.spatial[k] = expf(-2.f * d * d);
-    }
-    for (int k = tid; k < BM_W * BM_W; k += 256) {
-        const int ty = k / BM_W, tx = k % BM_W;
-        const int sx = clampi(x0 - BM_R + tx, 0, img.w - 1), sy = clampi(y0 - BM_R + ty, 0, img.h - 1);
-        const f4 p = ld4<S>(img.px(sx, sy));
-        sm.ycc[k] = make_float4(p.x, p.y, p.z, 0.f);
-        const S* q = pca.px(sx, sy);
-        if constexpr (fast) {
-            const uint4 u = *reinterpret_cast<const uint4*>(q);
-            const float2 a0 = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
-            const float2 a1 = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
-            const float2 a2 = __half22float2(*reinterpret_cast<const __half2*>(&u.z));
-            const float2 a3 = __half22float2(*reinterpret_cast<const __half2*>(&u.w));
-            sm.pca[k][0] = make_float4(a0.x, a0.y, a1.x, a1.y);
-            sm.pca[k][1] = make_float4(a2.x, a2.y, a3.x, a3.y);
-        } else {
-            const float4* q4 = reinterpret_cast<const float4*>(q);
-            sm.pca[k][0] = q4[0];
-            sm.pca[k][1] = q4[1];
-        }
-    }
-    __syncthreads();
-    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
-    if (x >= img.w || y >= img.h) return;
-    const int c0 = (threadIdx.y + BM_R) * BM_W + threadIdx.x + BM_R;
-    const float4 in = sm.ycc[c0];
-    const float4 ip0 = sm.pca[c0][0], ip1 = sm.pca[c0][1];
-    float ls = 1.f;
-    if (a.lsc > 0.f) {
-        const float cx = float(img.w / 2), cy = float(img.h / 2);
-        const float dx = float(x) - cx, dy = float(y) - cy;
-        const float r = sqrtf(dx * dx + dy * dy) / sqrtf(cx * cx + cy * cy);
-        ls = 1.f + a.lsc * r * r;
-    }
-    const float sig0 = sqrtf(a.var_a[0] + a.var_b[0] * ls * in.x);
-    const float sig1 = sqrtf(a.var_a[1] + a.var_b[1] * ls * in.x);
-    const float sig2 = sqrtf(a.var_a[2] + a.var_b[2] * ls * in.x);
-    const float dm0 = 1.f / (a.tm[0] * sig0), dm1 = 1.f / (a.tm[1] * sig1), dm2 = 1.f / (a.tm[2] * sig2);
-    const f2 g = ld2<S>(grad.px(x, y));
-    const float mag = sqrtf(g.x * g.x + g.y * g.y);
-    const float edge = smoothstepf(2.f, 16.f, a.gradient_threshold * mag / sig0);
-    const float ls_ = dm0 / (1.f + a.gradient_boost * edge);
-    // luma weight exp(-2 (|dp| ls_)^2) = exp(kl |dp|^2); chroma weight
-    // exp(-2 (lw^2 + (dcb*c1)^2 + (dcr*c2)^2))
-    const float kl = -2.f * ls_ * ls_;
-    const float c1 = dm1 / a.chroma_boost, c2 = dm2 / a.chroma_boost;
-    float fy = 0.f, fcb = 0.f, fcr = 0.f, ny = 0.f, nc = 0.f;
-    for (int j = 0; j < 21; j++) {
-        const int rowb = (threadIdx.y + j) * BM_W + threadIdx.x;
-#pragma unroll 3
-        for (int i = 0; i < 21; i++) {
-            const int k = rowb + i;
-            const float4 p0 = sm.pca[k][0], p1 = sm.pca[k][1];
-            const float4 s = sm.ycc[k];
-            float d, d2;
-            d = p0.x - ip0.x; d2 = d * d;
-            d = p0.y - ip0.y; d2 += d * d;
-            d = p0.z - ip0.z; d2 += d * d;
-            d = p0.w - ip0.w; d2 += d * d;
-            d = p1.x - ip1.x; d2 += d * d;
-            d = p1.y - ip1.y; d2 += d * d;
-            d = p1.z - ip1.z; d2 += d * d;
-            d = p1.w - ip1.w; d2 += d * d;
-            const float lw = fast ? __expf(kl * d2) : expf(kl * d2);
-            const float e1 = (s.y - in.y) * c1, e2 = (s.z - in.z) * c2;
-            const float cq = lw * lw + e1 * e1 + e2 * e2;
-            const float cw = fast ? __expf(-2.f * cq) : expf(-2.f * cq);
-            const float sw = sm.spatial[j * 21 + i];
-            const float wy = sw * lw, wc = sw * cw;
-            fy += wy * s.x;
-            fcb += wc * s.y;
-            fcr += wc * s.z;
-            ny += wy;
-            nc += wc;
-        }
-    }
-    st4<S>(out.px(x, y), f4{fy / ny, fcb / nc, fcr / nc, ny});
-}
-
-// --------------------------------------------------------------------------
-// FP16-storage block matching. The reference evaluates this kernel in half
-// precision (demosaic.metal:806-884); here the per-tap arithmetic is packed
-// half2 and the five sums stay FP32, as in the reference:
-//   * each thread owns two vertically adjacent pixels, which share 20 of
-//     their 21 window rows, so every staged neighbour feeds two taps;
-//   * the 8-D PCA distance runs on half2 pairs of components;
-//   * both Gaussians of a neighbour for the two pixels are one packed
-//     h2exp2 each (luma: exp(-2 (|dp| s)^2), chroma: exp(-2 (lw^2 + dc^2))),
-//     with the constants pre-scaled by log2(e);
-//   * the spatial Gaussian of the two pixels is a half2 table lookup
-//     (zero where a row is outside a pixel's window).
-// Tile: 32 x 16 output pixels per 256-thread block; shared memory holds
-// the 52 x 36 window region as 8 PCA halves (16 B) + Y, Cb, Cr halves (8 B).
-constexpr int BH_TX = 32, BH_TY = 8, BH_W = BH_TX + 20, BH_H = 2 * BH_TY + 20;
-
-struct BlockMatchH2Smem {
-    uint4 pca[BH_H * BH_W];
-    uint2 ycc[BH_H * BH_W];
-    __half2 sp[22 * 21];  // (weight for the upper pixel, weight for the lower pixel) per (row r, column i)
-};
-
-__device__ __forceinline__ __half2 u2h(uint32_t u) { return *reinterpret_cast<__half2*>(&u); }
-
-template <bool UP, bool LO>
-__device__ __forceinline__ void bm_row(const BlockMatchH2Smem& sm, int base, int r, const __half2 (&ip0)[4],
-                                       const __half2 (&ip1)[4], float2 kl, __half2 incb, __half2 incr,
-                                       __half2 c1, __half2 c2, __half2 lwk, float (&acc)[10]) {
-    const __half2* sp = sm.sp + r * 21;
-#pragma unroll
-    for (int i = 0; i < 21; i++) {
-        const uint4 P = sm.pca[base + i];
-        const uint2 Y = sm.ycc[base + i];
-        const __half2 p01 = u2h(P.x), p23 = u2h(P.y), p45 = u2h(P.z), p67 = u2h(P.w);
-        __half d2u = __float2half(0.f), d2l = __float2half(0.f);
-        if (UP) {
-            __half2 a = __hsub2(p01, ip0[0]), b = __hsub2(p23, ip0[1]);
-            __half2 s = __hmul2(a, a);
-            s = __hfma2(b, b, s);
-            a = __hsub2(p45, ip0[2]);
-            b = __hsub2(p67, ip0[3]);
-            s = __hfma2(a, a, s);
-            s = __hfma2(b, b, s);
-            d2u = __hadd(__low2half(s), __high2half(s));
-        }
-        if (LO) {
-            __half2 a = __hsub2(p01, ip1[0]), b = __hsub2(p23, ip1[1]);
-            __half2 s = __hmul2(a, a);
-            s = __hfma2(b, b, s);
-            a = __hsub2(p45, ip1[2]);
-            b = __hsub2(p67, ip1[3]);
-            s = __hfma2(a, a, s);
-            s = __hfma2(b, b, s);
-            d2l = __hadd(__low2half(s), __high2half(s));
-        }
-        // luma weights of both pixels: exp2(kl * d2). The exponent is formed in
-        // FP32 (kl can exceed the half range for dark pixels; a product past
-        // -65504 becomes -inf in half and exp2 gives 0, as it should).
-        const __half2 lw = h2exp2(__floats2half2_rn(kl.x * __half2float(d2u), kl.y * __half2float(d2l)));
-        // chroma weights: exp2(-(lw'^2 + e1'^2 + e2'^2)), primes pre-scaled by sqrt(2 log2 e)
-        const __half2 ycb = u2h(Y.x), crx = u2h(Y.y);
-        const __half2 e1 = __hmul2(__hsub2(__high2half2(ycb), incb), c1);
-        const __half2 e2 = __hmul2(__hsub2(__low2half2(crx), incr), c2);
-        const __half2 lq = __hmul2(lw, lwk);
-        __half2 q = __hmul2(e2, e2);
-        q = __hfma2(e1, e1, q);
-        q = __hfma2(lq, lq, q);
-        const __half2 cw = h2exp2(__hneg2(q));
-        const __half2 s2 = sp[i];
-        const float2 wy = __half22float2(__hmul2(s2, lw));
-        const float2 wc = __half22float2(__hmul2(s2, cw));
-        const float2 yc = __half22float2(ycb);
-        const float cr = __low2float(crx);
-        if (UP) {
-            acc[0] = fmaf(wy.x, yc.x, acc[0]);
-            acc[1] = fmaf(wc.x, yc.y, acc[1]);
-            acc[2] = fmaf(wc.x, cr, acc[2]);
-            acc[3] += wy.x;
-            acc[4] += wc.x;
-        }
-        if (LO) {
-            acc[5] = fmaf(wy.y, yc.x, acc[5]);
-            acc[6] = fmaf(wc.y, yc.y, acc[6]);
-            acc[7] = fmaf(wc.y, cr, acc[7]);
-            acc[8] += wy.y;
-            acc[9] += wc.y;
-        }
-    }
-}
-
-__global__ void __launch_bounds__(256) k_block_match_h2(Plane<__half, 4> img, Plane<__half, 2> grad,
-                                                        Plane<__half, 8> pca, Plane<__half, 4> out,
-                                                        BlockMatchArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    BlockMatchH2Smem& sm = *reinterpret_cast<BlockMatchH2Smem*>(smem_raw);
-    const int x0 = blockIdx.x * BH_TX, y0 = blockIdx.y * (2 * BH_TY);
-    const int tid = threadIdx.y * BH_TX + threadIdx.x;
-    for (int k = tid; k < 22 * 21; k += 256) {
-        const int r = k / 21, i = k % 21 - 10;
-        auto sw = [&](int j) {
-            const float d = 0.1f * sqrtf(float(i * i + j * j));
-            return expf(-2.f * d * d);
-        };
-        const float up = r <= 20 ? sw(r - 10) : 0.f;  // row r of the upper pixel's window is offset r - 10
-        const float lo = r >= 1 ? sw(r - 11) : 0.f;   // the lower pixel's offset is r - 11
-        sm.sp[k] = __floats2half2_rn(up, lo);
-    }
-    for (int k = tid; k < BH_W * BH_H; k += 256) {
-        const int ty = k / BH_W, tx = k % BH_W;
-        const int sx = clampi(x0 - 10 + tx, 0, img.w - 1), sy = clampi(y0 - 10 + ty, 0, img.h - 1);
-        sm.pca[k] = *reinterpret_cast<const uint4*>(pca.px(sx, sy));
-        uint2 y = *reinterpret_cast<const uint2*>(img.px(sx, sy));
-        y.y &= 0xffffu;  // keep Cr, zero the w half
-        sm.ycc[k] = y;
-    }
-    __syncthreads();
-    const int x = x0 + threadIdx.x, yu = y0 + 2 * threadIdx.y;
-    const float kLog2e = 1.4426950408889634f;
-    __half2 ip0[4], ip1[4];
-    float kl[2], c1v[2], c2v[2], incb[2], incr[2];
-#pragma unroll
-    for (int p = 0; p < 2; p++) {
-        const int c = (2 * threadIdx.y + p + 10) * BH_W + threadIdx.x + 10;
-        const uint4 P = sm.pca[c];
-        __half2* ip = p ? ip1 : ip0;
-        ip[0] = u2h(P.x); ip[1] = u2h(P.y); ip[2] = u2h(P.z); ip[3] = u2h(P.w);
-        const uint2 Y = sm.ycc[c];
-        const float2 yc = __half22float2(u2h(Y.x));
-        const float cr = __low2float(u2h(Y.y));
-        const int py = min(yu + p, img.h - 1), px = min(x, img.w - 1);
-        float ls = 1.f;
-        if (a.lsc > 0.f) {
-            const float cx = float(img.w / 2), cy = float(img.h / 2);
-            const float dx = float(px) - cx, dy = float(py) - cy;
-            const float rr = sqrtf(dx * dx + dy * dy) / sqrtf(cx * cx + cy * cy);
-            ls = 1.f + a.lsc * rr * rr;
-        }
-        const float sig0 = sqrtf(a.var_a[0] + a.var_b[0] * ls * yc.x);
-        const float sig1 = sqrtf(a.var_a[1] + a.var_b[1] * ls * yc.x);
-        const float sig2 = sqrtf(a.var_a[2] + a.var_b[2] * ls * yc.x);
-        const float dm0 = 1.f / (a.tm[0] * sig0), dm1 = 1.f / (a.tm[1] * sig1), dm2 = 1.f / (a.tm[2] * sig2);
-        const f2 g = ld2<__half>(grad.px(px, py));
-        const float mag = sqrtf(g.x * g.x + g.y * g.y);
-        const float edge = smoothstepf(2.f, 16.f, a.gradient_threshold * mag / sig0);
-        const float lsc_ = dm0 / (1.f + a.gradient_boost * edge);
-        kl[p] = -2.f * kLog2e * lsc_ * lsc_;
-        const float sq = sqrtf(2.f * kLog2e);
-        c1v[p] = sq * dm1 / a.chroma_boost;
-        c2v[p] = sq * dm2 / a.chroma_boost;
-        incb[p] = yc.y;
-        incr[p] = cr;
-    }
-    const float2 klh = make_float2(fmaxf(kl[0], -1e30f), fmaxf(kl[1], -1e30f));
-    // chroma scales saturate at the half maximum (a difference of one half
-    // ulp times 65504 already zeroes the weight)
-    const __half2 c1h = __floats2half2_rn(fminf(c1v[0], 65504.f), fminf(c1v[1], 65504.f));
-    const __half2 c2h = __floats2half2_rn(fminf(c2v[0], 65504.f), fminf(c2v[1], 65504.f));
-    const __half2 incbh = __floats2half2_rn(incb[0], incb[1]), incrh = __floats2half2_rn(incr[0], incr[1]);
-    const __half2 lwk = __float2half2_rn(sqrtf(2.f * kLog2e));
-    float acc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    // window rows of the pair: r = 0 (upper only), 1..20 (both), 21 (lower only)
-    const int col = threadIdx.x;
-    const int row0 = 2 * threadIdx.y;
-    bm_row<true, false>(sm, (row0 + 0) * BH_W + col, 0, ip0, ip1, klh, incbh, incrh, c1h, c2h, lwk, acc);
-    for (int r = 1; r <= 20; r++)
-        bm_row<true, true>(sm, (row0 + r) * BH_W + col, r, ip0, ip1, klh, incbh, incrh, c1h, c2h, lwk, acc);
-    bm_row<false, true>(sm, (row0 + 21) * BH_W + col, 21, ip0, ip1, klh, incbh, incrh, c1h, c2h, lwk, acc);
-    if (x < out.w) {
-        if (yu < out.h) st4<__half>(out.px(x, yu), f4{acc[0] / acc[3], acc[1] / acc[4], acc[2] / acc[4], acc[3]});
-        if (yu + 1 < out.h)
-            st4<__half>(out.px(x, yu + 1), f4{acc[5] / acc[8], acc[6] / acc[9], acc[7] / acc[9], acc[8]});
-    }
-}
-
 // ------------------------------------------------------------------ launchers
 static inline dim3 grid2(int w, int h, dim3 b) { return dim3((w + b.x - 1) / b.x, (h + b.y - 1) / b.y); }
 
@@ -685,31 +407,6 @@ template <class S>
 void launch_pca_project(Plane<S, 4> img, const float* basis, Plane<S, 8> out, cudaStream_t s) {
     dim3 b(32, 8);
     k_pca_project<S><<<grid2(img.w, img.h, b), b, 0, s>>>(img, basis, out);
-}
-
-template <class S>
-void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, Plane<S, 4> out, const BlockMatchArgs& a,
-                        cudaStream_t s) {
-    if constexpr (is_half<S>::value) {
-        static bool attr_h = false;
-        if (!attr_h) {
-            cudaFuncSetAttribute(k_block_match_h2, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(sizeof(BlockMatchH2Smem)));
-            attr_h = true;
-        }
-        dim3 b(BH_TX, BH_TY);
-        dim3 g((img.w + BH_TX - 1) / BH_TX, (img.h + 2 * BH_TY - 1) / (2 * BH_TY));
-        k_block_match_h2<<<g, b, sizeof(BlockMatchH2Smem), s>>>(img, grad, pca, out, a);
-    } else {
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(k_block_match<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(sizeof(BlockMatchSmem)));
-            attr = true;
-        }
-        dim3 b(BM_T, BM_T);
-        k_block_match<S><<<grid2(img.w, img.h, b), b, sizeof(BlockMatchSmem), s>>>(img, grad, pca, out, a);
-    }
 }
 
 // Host FP64 eigen-solve of the same accumulators: the per-level host PCA of
@@ -791,9 +488,7 @@ void host_pca_basis(const double* part, int n_blocks, int n_patches, float* basi
     template void launch_subtract_noise<S>(Plane<S, 4>, Plane<S, 4>, Plane<S, 4>, Plane<S, 2>, Plane<S, 4>,     \
                                            const SubtractArgs&, cudaStream_t);                                   \
     template void launch_pca_cov<S>(Plane<S, 4>, double*, cudaStream_t);                                         \
-    template void launch_pca_project<S>(Plane<S, 4>, const float*, Plane<S, 8>, cudaStream_t);                  \
-    template void launch_block_match<S>(Plane<S, 4>, Plane<S, 2>, Plane<S, 8>, Plane<S, 4>,                     \
-                                        const BlockMatchArgs&, cudaStream_t);
+    template void launch_pca_project<S>(Plane<S, 4>, const float*, Plane<S, 8>, cudaStream_t);
 GLS_INST(float)
 GLS_INST(__half)
 #undef GLS_INST
