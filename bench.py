@@ -2,11 +2,11 @@
 """Benchmark of the raw -> RGB hot path (demosaic + 5-level PCA pyramid
 denoise + reconstruct) on 12 MP RGGB frames.
 
-A step is one frame of the 4032x3024 12-bit workload through
-RawConverter::demosaic with noise reduction, on the FP16-storage path.
-`value` is frames/s with the raw frames already resident in HBM; `e2e` is
-the same call with host buffers (pinned raw in, FP16 RGBA out) copied inside
-the timed region. With --gpus N (torchrun), every rank converts its own
+A step is one batch of six frames of the 4032x3024 12-bit workload through
+the batched RawConverter::demosaic with noise reduction, on the FP16-storage
+path (frames run concurrently on three streams). `value` is frames/s with
+the raw frames already resident in HBM; `e2e` is the same batched call with
+host buffers (pinned raw in, FP16 RGBA out) copied inside the timed region. With --gpus N (torchrun), every rank converts its own
 frames (no data-path collective); the time is the max over ranks.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -182,96 +182,98 @@ def main():
     wl = scene.WORKLOADS[args.workload]
     params = scene.make_params(wl)
     conv = g.RawConverter(local)
+    lib = g.lib()
     stream = torch.cuda.Stream()
     H, W = wl.height, wl.width
+    B = N_ROTATE  # frames per step (one batch)
 
     # resident inputs: distinct frames per rank (weak scaling)
-    raws_host = []
-    for f in range(N_ROTATE):
-        raw, _ = scene.make_raw(wl, frame=rank * N_ROTATE + f)
-        raws_host.append(raw)
+    raws_host = [scene.make_raw(wl, frame=rank * B + f)[0] for f in range(B)]
     raws = [torch.from_numpy(r.view(np.int16)).to(f"cuda:{local}") for r in raws_host]
-    out = torch.empty((H, W, 4), dtype=torch.float16, device=f"cuda:{local}")
+    outs = [torch.empty((H, W, 4), dtype=torch.float16, device=f"cuda:{local}") for _ in range(B)]
+    plist = [params] * B
 
-    def step(i, fp16=True, host_pca=False):
-        conv.demosaic(raws[i % N_ROTATE], params, noiseReduction=True, fp16=fp16, out=out, out_fp16=True,
+    def step_batch():
+        conv.demosaic_batch(raws, plist, outs, fp16=True, out_fp16=True, stream=stream)
+
+    def step_frame(i, fp16=True, host_pca=False):
+        conv.demosaic(raws[i % B], params, noiseReduction=True, fp16=fp16, out=outs[i % B], out_fp16=True,
                       stream=stream, host_pca=host_pca, sync=False)
 
-    lib = g.lib()
+    def stats():
+        st = (g.KernelStat * 32)()
+        n = C.c_int32()
+        g.check(lib.gls_converter_stats(conv.handle, st, 32, C.byref(n)))
+        return {st[i].name.decode(): {"launches": int(st[i].launches), "ms": st[i].ms} for i in range(n.value)}
+
     with torch.cuda.stream(stream):
-        for i in range(args.warmup):
-            step(i)
+        for _ in range(args.warmup):
+            step_batch()
         stream.synchronize()
-        lib.gls_converter_reset_stats(conv.handle)
-        lib.gls_converter_set_profiling(conv.handle, 0)
+        g.check(lib.gls_converter_reset_stats(conv.handle))
         barrier()
         torch.cuda.synchronize()
         sampler = ClockSampler(local)
         sampler.start()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for i in range(args.steps):
-            step(i)
+        for _ in range(args.steps):
+            step_batch()
         e1.record(stream)
         stream.synchronize()
         clocks = sampler.stop()
         ms = e0.elapsed_time(e1)
-        stats = (g.KernelStat * 32)()
-        n = C.c_int32()
-        lib.gls_converter_stats(conv.handle, stats, 32, C.byref(n))
-        launches = int(sum(stats[i].launches for i in range(n.value)))
+        launches = sum(v["launches"] for v in stats().values())
         barrier()
-
         if args.quick:
             if rank == 0:
-                print(json.dumps({"quick": True, "workload": args.workload, "ms_per_step": ms / args.steps,
-                                  "gpu_launches": launches}), flush=True)
+                print(json.dumps({"quick": True, "workload": args.workload, "frames_per_step": B,
+                                  "ms_per_frame": ms / args.steps / B, "gpu_launches": launches}), flush=True)
             conv.close()
+            if world > 1:
+                dist.destroy_process_group()
             return
 
-        # per-kernel device time inside an identical timed loop (events around
-        # each launch, on the launch stream)
-        lib.gls_converter_reset_stats(conv.handle)
-        lib.gls_converter_set_profiling(conv.handle, 1)
-        for i in range(args.steps):
-            step(i)
-        lib.gls_converter_stats(conv.handle, stats, 32, C.byref(n))
-        lib.gls_converter_set_profiling(conv.handle, 0)
-        per_kernel = {stats[i].name.decode(): {"launches": int(stats[i].launches), "ms": stats[i].ms}
-                      for i in range(n.value) if stats[i].launches}
+        # per-kernel device time: the same frames one after the other, each
+        # launch bracketed by events on its stream
+        g.check(lib.gls_converter_reset_stats(conv.handle))
+        g.check(lib.gls_converter_set_profiling(conv.handle, 1))
+        n_prof = max(B, args.steps)
+        for i in range(n_prof):
+            step_frame(i)
+        per_kernel = stats()
+        g.check(lib.gls_converter_set_profiling(conv.handle, 0))
 
-        # FP32 plain single-frame path (reference structure: FP32 planes, per-level host PCA)
+        # FP32 plain single-frame path (FP32 planes, per-level host PCA sync:
+        # the reference's structure)
         for i in range(2):
-            step(i, fp16=False, host_pca=True)
+            step_frame(i, fp16=False, host_pca=True)
         stream.synchronize()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        n32 = max(3, args.steps // 4)
+        n32 = max(3, args.steps // 2)
         f0.record(stream)
         for i in range(n32):
-            step(i, fp16=False, host_pca=True)
+            step_frame(i, fp16=False, host_pca=True)
         f1.record(stream)
         stream.synchronize()
         ms32 = f0.elapsed_time(f1) / n32
 
-        # end to end through the public API with host buffers
+        # end to end through the public batched call with host buffers
+        # (pinned raw in, FP16 RGBA out; copies inside the timed region)
         pinned_raw = [torch.from_numpy(r.view(np.int16)).pin_memory() for r in raws_host]
-        pinned_out = torch.empty((H, W, 4), dtype=torch.float16).pin_memory()
-        hv = g.ImageView(C.c_void_p(pinned_out.data_ptr()), W, H, 4, g.F16, W * 8)
-        flags = g.DENOISE | g.FP16_STORAGE | g.HOST_IO | g.SYNC
+        pinned_out = [torch.empty((H, W, 4), dtype=torch.float16).pin_memory() for _ in range(B)]
 
-        def e2e_step(i):
-            g.check(lib.gls_demosaic(conv.handle, C.c_void_p(pinned_raw[i % N_ROTATE].data_ptr()), W, H, W * 2,
-                                     C.byref(params), flags, C.byref(hv), C.c_void_p(stream.cuda_stream)))
+        def e2e_step():
+            conv.demosaic_batch(pinned_raw, plist, pinned_out, fp16=True, out_fp16=True, stream=stream)
 
-        for i in range(2):
-            e2e_step(i)
+        e2e_step()
         n_e2e = max(3, args.steps // 2)
         barrier()
         t0 = time.perf_counter()
         g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         g0.record(stream)
-        for i in range(n_e2e):
-            e2e_step(i)
+        for _ in range(n_e2e):
+            e2e_step()
         g1.record(stream)
         stream.synchronize()
         e2e_wall = (time.perf_counter() - t0) / n_e2e
@@ -283,19 +285,18 @@ def main():
         dist.all_reduce(vals, op=dist.ReduceOp.MAX)
     ms, ms32, e2e_ms = [float(v) for v in vals.tolist()]
     ms_step = ms / args.steps
-    value = world * args.steps / (ms / 1e3)
+    value = world * B * args.steps / (ms / 1e3)
 
-    # roofline of the dominant kernel (block matching), from the live event times
+    # roofline of the dominant kernel (block matching) from the live event times
     bm = per_kernel.get("block_match", {"launches": 1, "ms": float("nan")})
     px = sum((W >> i) * (H >> i) for i in range(wl.levels))
     taps = 21 * 21
-    flop_per_tap = 50.0  # 8-D distance + norm 24, chroma 6, 2 weights 8, accumulate 10 (FMA = 2)
-    frames_prof = args.steps
-    bm_tflops = px * taps * flop_per_tap * frames_prof / (bm["ms"] / 1e3) / 1e12
+    flop_per_tap = 50.0  # 8-D distance 24, chroma 6, two weights 8, accumulate 10 (FMA = 2)
+    bm_tflops = px * taps * flop_per_tap * n_prof / (bm["ms"] / 1e3) / 1e12
     sm_clock = clocks.get("sm_mhz") or 1965.0
     fp32_peak = 148 * 128 * 2 * (sm_clock * 1e6) / 1e12  # SIMT FP32 FMA peak at the sampled clock
-    mufu_rate = 148 * 16 * (sm_clock * 1e6) / 1e12  # ex2 per SM per clock = 16
-    bm_mufu = px * taps * 2 * frames_prof / (bm["ms"] / 1e3) / 1e12
+    mufu_rate = 148 * 16 * (sm_clock * 1e6) / 1e12       # ex2 per SM per clock = 16
+    bm_mufu = px * taps * 2 * n_prof / (bm["ms"] / 1e3) / 1e12
     total_prof_ms = sum(v["ms"] for v in per_kernel.values())
 
     line = {
@@ -303,13 +304,13 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f16-storage/f32-math", "data": "synthetic",
         "config": {"workload": args.workload, "frame": f"{W}x{H} RGGB 12-bit", "levels": wl.levels, "iso": wl.iso,
-                   "frames_rotated": N_ROTATE, "l2": "inputs + planes per frame > 126 MB L2 (6 rotating frames)",
-                   "parallelism": f"frames sharded over {world} rank(s)"},
-        "e2e": {"value": world / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": W * H * 2,
-                "d2h_bytes_per_step": W * H * 8},
+                   "frames_per_step": B, "l2": "each step reads 6 distinct frames; inputs + planes >> 126 MB L2",
+                   "parallelism": f"frames sharded over {world} rank(s), {B}-frame batch per rank on 3 streams"},
+        "e2e": {"value": world * B / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": B * W * H * 2,
+                "d2h_bytes_per_step": B * W * H * 8},
         "fp32_plain": {"value": world / (ms32 / 1e3), "unit": UNIT, "ms_per_frame": ms32,
-                       "note": "FP32 planes, per-level host PCA sync (the reference's structure)"},
-        "speedup_vs_fp32_plain": ms32 / ms_step,
+                       "note": "FP32 planes, one frame at a time, per-level host PCA sync (the reference's structure)"},
+        "speedup_vs_fp32_plain": ms32 / (ms_step / B),
         "roofline": {"bound": "fp32+mufu", "kernel": "block_match",
                      "achieved": bm_tflops, "peak": fp32_peak, "unit": "TFLOP/s", "frac": bm_tflops / fp32_peak,
                      "mufu_frac": bm_mufu / mufu_rate, "traffic": None,
@@ -317,7 +318,7 @@ def main():
                      "ms_per_launch": bm["ms"] / max(1, bm["launches"]),
                      "peak_note": "nominal SIMT FP32 (148 SMs x 128 lanes x 2 x sampled SM clock); "
                                   "MEASURED_PEAKS has HBM and bf16-tensor peaks only"},
-        "per_kernel_ms_per_frame": {k: v["ms"] / frames_prof for k, v in per_kernel.items()},
+        "per_kernel_ms_per_frame": {k: v["ms"] / n_prof for k, v in per_kernel.items() if v["launches"]},
         "gpu_launches": launches,
         "clocks": clocks,
     }

@@ -127,22 +127,28 @@ class RawConverter:
         return out
 
     def demosaic_batch(self, raws, params_list, outs, fp16: bool = True, noiseReduction: bool = True,
-                       out_fp16: bool = True, stream=None, sync: bool = False):
-        """Batched RawConverter::demosaic over device frames of uneven sizes."""
+                       out_fp16: bool = True, stream=None, sync: bool = False, host_pca: bool = False):
+        """Batched RawConverter::demosaic over frames of uneven sizes.
+
+        ``raws``/``outs``: torch CUDA tensors (device I/O), or host buffers
+        (numpy arrays or pinned torch CPU tensors; copied inside the call).
+        """
         n = len(raws)
         frames = (FrameDesc * n)()
-        keep = []
+        host = False
         for i, (r, p, o) in enumerate(zip(raws, params_list, outs)):
             h, w = r.shape[0], r.shape[1]
+            host = host or not (_is_torch(r) and r.is_cuda)
             frames[i].raw = C.c_void_p(_ptr(r))
             frames[i].width = w
             frames[i].height = h
             frames[i].raw_stride_bytes = _row_stride(r)
             frames[i].params = C.pointer(p)
             frames[i].out = ImageView(C.c_void_p(_ptr(o)), w, h, 4, F16 if out_fp16 else F32, _row_stride(o))
-            keep.append(p)
         flags = (DENOISE if noiseReduction else 0) | (FP16_STORAGE if fp16 else 0) | (SYNC if sync else 0)
+        flags |= (HOST_IO if host else 0) | (HOST_PCA if host_pca else 0)
         check(lib().gls_demosaic_batch(self._h, frames, n, flags, _stream_handle(stream)))
+        return outs
 
     def plane(self, which: int) -> np.ndarray:
         """Host copy of an internal plane of the last call."""

@@ -196,12 +196,20 @@ struct KScope {
 };
 }  // namespace gls
 
+// Frames of a batch run concurrently on kSlots streams, each slot with its
+// own planes; slot 0 also serves the single-frame calls.
+constexpr int kSlots = 3;
+
 struct gls_converter {
     int device = 0;
     Prof prof;
-    Pipeline<float> p32;
-    Pipeline<__half> p16;
-    int last_storage = -1;  // GLS_F32 / GLS_F16 of the last call
+    Pipeline<float> p32s[kSlots];
+    Pipeline<__half> p16s[kSlots];
+    Pipeline<float>& p32 = p32s[0];
+    Pipeline<__half>& p16 = p16s[0];
+    cudaStream_t slot_stream[kSlots] = {};
+    cudaEvent_t fork_ev = nullptr, join_ev[kSlots] = {};
+    int last_storage = -1;  // GLS_F32 / GLS_F16 of the last single-frame call
     int last_levels = 0;
     int last_w = 0, last_h = 0;
     bool last_denoise = false;
@@ -395,8 +403,10 @@ static gls_status make_target(Pipeline<S>& P, gls_image_view* out, int w, int h,
 
 template <class S>
 static gls_status demosaic_run(gls_converter* cv, const uint16_t* raw, int w, int h, size_t stride_bytes,
-                               const gls_demosaic_params* p, uint32_t flags, gls_image_view* out, cudaStream_t s) {
-    Pipeline<S>& P = *reinterpret_cast<Pipeline<S>*>(is_half<S>::value ? (void*)&cv->p16 : (void*)&cv->p32);
+                               const gls_demosaic_params* p, uint32_t flags, gls_image_view* out, cudaStream_t s,
+                               int slot = 0) {
+    Pipeline<S>& P =
+        *reinterpret_cast<Pipeline<S>*>(is_half<S>::value ? (void*)&cv->p16s[slot] : (void*)&cv->p32s[slot]);
     const bool host_io = flags & GLS_HOST_IO;
     const bool denoise = flags & GLS_DENOISE;
     GLS_TRY(P.ensure(w, h, p->levels));
@@ -510,11 +520,13 @@ static gls_status demosaic_run(gls_converter* cv, const uint16_t* raw, int w, in
         GLS_TRY(make_target<S, float>(P, out, w, h, host_io, t));
         GLS_TRY(finish_output<S, float>(cv, final_src, denoise, y2c, t, s));
     }
-    cv->last_storage = is_half<S>::value ? GLS_F16 : GLS_F32;
-    cv->last_w = w;
-    cv->last_h = h;
-    cv->last_denoise = denoise;
-    if (host_io || (flags & GLS_SYNC)) GLS_CUDA(cudaStreamSynchronize(s));
+    if (slot == 0) {
+        cv->last_storage = is_half<S>::value ? GLS_F16 : GLS_F32;
+        cv->last_w = w;
+        cv->last_h = h;
+        cv->last_denoise = denoise;
+        if (host_io || (flags & GLS_SYNC)) GLS_CUDA(cudaStreamSynchronize(s));
+    }
     return GLS_OK;
 }
 
@@ -587,8 +599,14 @@ gls_status gls_converter_destroy(gls_converter* conv) {
     clear_error();
     if (!conv) return GLS_OK;
     cudaSetDevice(conv->device);
-    conv->p32.release();
-    conv->p16.release();
+    cudaDeviceSynchronize();
+    for (int k = 0; k < kSlots; k++) {
+        conv->p32s[k].release();
+        conv->p16s[k].release();
+        if (conv->slot_stream[k]) cudaStreamDestroy(conv->slot_stream[k]);
+        if (conv->join_ev[k]) cudaEventDestroy(conv->join_ev[k]);
+    }
+    if (conv->fork_ev) cudaEventDestroy(conv->fork_ev);
     delete conv;
     return GLS_OK;
 }
@@ -615,13 +633,63 @@ gls_status gls_demosaic_batch(gls_converter* conv, gls_frame_desc* frames, int32
                               void* stream) {
     clear_error();
     if (!conv || (!frames && n_frames > 0) || n_frames < 0) return set_error(GLS_ERR_INVALID_ARG, "bad batch");
-    for (int i = 0; i < n_frames; i++) {
-        gls_status st = gls_demosaic(conv, frames[i].raw, frames[i].width, frames[i].height,
-                                     frames[i].raw_stride_bytes, frames[i].params, flags & ~GLS_SYNC, &frames[i].out,
-                                     stream);
+    if (flags & GLS_POSTPROCESS)
+        return set_error(GLS_ERR_UNSUPPORTED, "sRGB post-processing is not part of this path (linear camera RGB only)");
+    for (int i = 0; i < n_frames; i++) {  // validate every frame before any work is queued
+        gls_frame_desc& f = frames[i];
+        if (!f.raw) return set_error(GLS_ERR_INVALID_ARG, "frame %d: raw is NULL", i);
+        gls_status st = check_params(f.params, f.width, f.height);
         if (st != GLS_OK) return st;
+        if (f.raw_stride_bytes == 0) f.raw_stride_bytes = size_t(f.width) * 2;
+        if (f.raw_stride_bytes < size_t(f.width) * 2) return set_error(GLS_ERR_INVALID_ARG, "frame %d: raw stride", i);
+        if (f.out.dtype != GLS_F32 && f.out.dtype != GLS_F16)
+            return set_error(GLS_ERR_INVALID_ARG, "frame %d: output dtype must be F32 or F16", i);
     }
-    if (flags & GLS_SYNC) GLS_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    GLS_CUDA(cudaSetDevice(conv->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if ((flags & GLS_HOST_PCA) || n_frames == 1) {
+        // per-level host synchronisation serialises anyway: one frame after the other
+        for (int i = 0; i < n_frames; i++) {
+            gls_frame_desc& f = frames[i];
+            gls_status st = (flags & GLS_FP16_STORAGE)
+                                ? demosaic_run<__half>(conv, f.raw, f.width, f.height, f.raw_stride_bytes, f.params,
+                                                       flags & ~GLS_SYNC, &f.out, s)
+                                : demosaic_run<float>(conv, f.raw, f.width, f.height, f.raw_stride_bytes, f.params,
+                                                      flags & ~GLS_SYNC, &f.out, s);
+            if (st != GLS_OK) return st;
+        }
+        if (flags & (GLS_SYNC | GLS_HOST_IO)) GLS_CUDA(cudaStreamSynchronize(s));
+        return GLS_OK;
+    }
+    // fork: every slot stream waits for the work already queued on `s`
+    if (!conv->fork_ev) {
+        GLS_CUDA(cudaEventCreateWithFlags(&conv->fork_ev, cudaEventDisableTiming));
+        for (int k = 0; k < kSlots; k++) {
+            GLS_CUDA(cudaStreamCreateWithFlags(&conv->slot_stream[k], cudaStreamNonBlocking));
+            GLS_CUDA(cudaEventCreateWithFlags(&conv->join_ev[k], cudaEventDisableTiming));
+        }
+    }
+    const int nslots = n_frames < kSlots ? n_frames : kSlots;
+    GLS_CUDA(cudaEventRecord(conv->fork_ev, s));
+    for (int k = 0; k < nslots; k++) GLS_CUDA(cudaStreamWaitEvent(conv->slot_stream[k], conv->fork_ev, 0));
+    // frame i runs on slot i % nslots, in order within a slot
+    gls_status result = GLS_OK;
+    for (int i = 0; i < n_frames && result == GLS_OK; i++) {
+        gls_frame_desc& f = frames[i];
+        const int k = i % nslots;
+        result = (flags & GLS_FP16_STORAGE)
+                     ? demosaic_run<__half>(conv, f.raw, f.width, f.height, f.raw_stride_bytes, f.params,
+                                            flags & ~GLS_SYNC, &f.out, conv->slot_stream[k], k)
+                     : demosaic_run<float>(conv, f.raw, f.width, f.height, f.raw_stride_bytes, f.params,
+                                           flags & ~GLS_SYNC, &f.out, conv->slot_stream[k], k);
+    }
+    // join (also on error, so the caller's stream orders after whatever was queued)
+    for (int k = 0; k < nslots; k++) {
+        GLS_CUDA(cudaEventRecord(conv->join_ev[k], conv->slot_stream[k]));
+        GLS_CUDA(cudaStreamWaitEvent(s, conv->join_ev[k], 0));
+    }
+    if (result != GLS_OK) return result;
+    if (flags & (GLS_SYNC | GLS_HOST_IO)) GLS_CUDA(cudaStreamSynchronize(s));
     return GLS_OK;
 }
 
