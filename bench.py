@@ -280,10 +280,8 @@ def main():
         e2e_ms = max(g0.elapsed_time(g1) / n_e2e, 1e3 * e2e_wall)
 
     # max over ranks
-    vals = torch.tensor([ms, ms32, e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
-    ms, ms32, e2e_ms = [float(v) for v in vals.tolist()]
+    from glasscamerapublic_b200.shard import max_over_ranks
+    ms, ms32, e2e_ms = max_over_ranks([ms, ms32, e2e_ms], dist if world > 1 else None)
     ms_step = ms / args.steps
     value = world * B * args.steps / (ms / 1e3)
 

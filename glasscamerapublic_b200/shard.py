@@ -1,0 +1,40 @@
+"""Frame sharding across ranks (one process per GPU).
+
+The path has no exchange step: frames are independent, so a batch is split
+across ranks by pixel count and each rank converts its share on its own GPU
+(weak scaling, no data-path collective). The process group carries only the
+timing reduction: the slowest rank's device time is the job's time.
+"""
+from __future__ import annotations
+
+
+def assign_frames(sizes: list[tuple[int, int]], world: int) -> list[list[int]]:
+    """Longest-processing-time assignment of frames (by pixel count) to ranks.
+
+    Deterministic: frames are taken largest first (ties by index) and each
+    goes to the least-loaded rank (ties by rank). Returns, per rank, the
+    frame indices in ascending order.
+    """
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(sizes)), key=lambda i: (-sizes[i][0] * sizes[i][1], i))
+    load = [0] * world
+    out: list[list[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        out[r].append(i)
+        load[r] += sizes[i][0] * sizes[i][1]
+    return [sorted(x) for x in out]
+
+
+def max_over_ranks(values, dist=None):
+    """Element-wise max of a list of floats over all ranks (the job time is
+    the slowest rank's). With no process group, returns the values."""
+    if dist is None or not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return list(values)
+    import torch
+    t = torch.tensor(list(values), dtype=torch.float64)
+    if dist.get_backend() == "nccl":
+        t = t.cuda()
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu().tolist()]
