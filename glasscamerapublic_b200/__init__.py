@@ -123,6 +123,7 @@ _SIGNATURES = {
     "gls_converter_plane": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(ImageView)]),
     "gls_converter_pca_basis": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_float)]),
     "gls_copy_view": (C.c_int, [C.POINTER(ImageView), C.POINTER(ImageView), C.c_int32, C.c_void_p]),
+    "gls_pca_basis_noalloc": (C.c_int, [C.POINTER(ImageView), C.c_void_p, C.c_void_p]),
     "gls_converter_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
     "gls_converter_stats": (C.c_int, [C.c_void_p, C.POINTER(KernelStat), C.c_int32, C.POINTER(C.c_int32)]),
     "gls_converter_reset_stats": (C.c_int, [C.c_void_p]),

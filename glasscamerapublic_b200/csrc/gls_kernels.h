@@ -88,6 +88,10 @@ void launch_subtract_noise(Plane<S, 4> in, Plane<S, 4> coarse, Plane<S, 4> coars
                            Plane<S, 4> out, const SubtractArgs& a, cudaStream_t s);
 template <class S>
 void launch_pca_cov(Plane<S, 4> img, double* part, cudaStream_t s);
+// one block per 64-patch chunk: `rows` = ceil(patches / 64) partial rows
+template <class S>
+void launch_pca_cov_rows(Plane<S, 4> img, double* part, int rows, cudaStream_t s);
+constexpr int kPcaChunk = 64;
 void launch_pca_eigen(const double* part, int n_blocks, int n_patches, float* basis /*25x8*/, int* status,
                       cudaStream_t s);
 template <class S>

@@ -399,6 +399,14 @@ void launch_pca_cov(Plane<S, 4> img, double* part, cudaStream_t s) {
     k_pca_cov<S><<<blocks, 352, 0, s>>>(img, part);
 }
 
+template <class S>
+void launch_pca_cov_rows(Plane<S, 4> img, double* part, int rows, cudaStream_t s) {
+    init_pairs();
+    if (rows > 0) k_pca_cov<S><<<rows, 352, 0, s>>>(img, part);
+}
+template void launch_pca_cov_rows<float>(Plane<float, 4>, double*, int, cudaStream_t);
+template void launch_pca_cov_rows<__half>(Plane<__half, 4>, double*, int, cudaStream_t);
+
 void launch_pca_eigen(const double* part, int n_blocks, int n_patches, float* basis, int* status, cudaStream_t s) {
     k_pca_eigen<<<1, 1024, 0, s>>>(part, n_blocks, n_patches, basis, status);
 }

@@ -189,6 +189,23 @@ gls_status gls_copy_view(const gls_image_view* src, gls_image_view* dst, int32_t
  * row-major (pcaSpace[row][component], pyramid_processor.hpp:46). */
 gls_status gls_converter_pca_basis(gls_converter* conv, int32_t level, float* basis25x8);
 
+/* PCA patch basis (25 x 8 floats, row-major, written to basis25x8 in device
+ * memory) of one 4-channel image in device memory (luma in channel 0),
+ * computed without allocating device memory. No counterpart in the
+ * reference: it is gls_converter_pca_basis's computation for callers that
+ * cannot call cudaMalloc (a real-time capture thread that must not block in
+ * the allocator; an application whose device memory is all owned by
+ * another allocator). Its scratch is a fixed 11.5 MB array that every GPU
+ * loading this library holds until exit, so an image may have at most
+ * 262,144 patches of the 8-pixel grid (about 16.7 megapixels); larger
+ * images are rejected with GLS_ERR_INVALID_ARG. Runs on the calling
+ * thread's current device, asynchronously on `stream`. The first call on
+ * each device looks up the scratch array's device address; make that first
+ * call before any stream capture. All calls share the one array: calls
+ * whose GPU work overlaps (different streams, or different host threads)
+ * race on it and must be serialised by the caller. */
+gls_status gls_pca_basis_noalloc(const gls_image_view* image, float* basis25x8, void* stream);
+
 /* ---- launch accounting (no reference counterpart; the reference prints
  *      wall-clock timers, pipelineTest.cpp:161-169) ----
  * Every kernel launch of a converter is counted per kernel class. With
