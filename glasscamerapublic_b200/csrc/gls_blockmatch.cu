@@ -321,18 +321,268 @@ __global__ void __launch_bounds__(256, 2) k_block_match_fast(Plane<__half, 4> im
     }
 }
 
+// ---------------------------------------------------------------- FFMA2 form
+// The same FP16-path arithmetic with the four pixels of a thread taken as
+// two pairs, (p0, p1) and (p2, p3), and every per-pixel FP32 operation of a
+// pair issued as one packed FP32x2 instruction (fma/mul/add .rn.f32x2,
+// sm_100a). The neighbour's values enter as broadcast pairs. A pair's
+// spatial weights come from one float4 of a 22 x 21 table indexed by the
+// pair's first window row (rows outside a pixel's window carry weight 0 and
+// log-weight -inf, which zero both of its weights).
+typedef unsigned long long u64;
+
+__device__ __forceinline__ u64 pk2(float a, float b) {
+    u64 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void upk2(u64 r, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r)); }
+__device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
+    u64 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ u64 mul2(u64 a, u64 b) {
+    u64 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ u64 add2(u64 a, u64 b) {
+    u64 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+struct BmPairSmem {
+    uint4 pca[BX_H * BX_W];   // q - c, 8 halves
+    float4 ycc[BX_H * BX_W];  // Y, Cb, Cr, |q - c|^2
+    float4 sp[22 * 21];       // (sw(j)/sqrt(lk), sw(j-1)/sqrt(lk), -log2 sw(j), -log2 sw(j-1)), j = table row
+};
+
+struct BmPair {  // two pixels, each member of a pair register = one pixel
+    u64 p[8];             // p - c, per component
+    u64 kl, klm2, base;   // luma exponent terms
+    u64 c1, c2, no1, no2; // chroma: e = c * v - o  (no = -o)
+};
+
+template <bool A, bool B>
+__device__ __forceinline__ void bmp2_row(const BmPairSmem& sm, int base, int r, const BmPair& pa, const BmPair& pb,
+                                         u64 (&acc)[2][5]) {
+#pragma unroll 7
+    for (int i = 0; i < 21; i++) {
+        const uint4 u = sm.pca[base + i];
+        const float2 a0 = __half22float2(u2h_(u.x)), a1 = __half22float2(u2h_(u.y));
+        const float2 a2 = __half22float2(u2h_(u.z)), a3 = __half22float2(u2h_(u.w));
+        const float4 y = sm.ycc[base + i];
+        const u64 q[8] = {pk2(a0.x, a0.x), pk2(a0.y, a0.y), pk2(a1.x, a1.x), pk2(a1.y, a1.y),
+                          pk2(a2.x, a2.x), pk2(a2.y, a2.y), pk2(a3.x, a3.x), pk2(a3.y, a3.y)};
+        const u64 yy = pk2(y.x, y.x), cb = pk2(y.y, y.y), cr = pk2(y.z, y.z), nn = pk2(y.w, y.w);
+        auto pair = [&](const BmPair& P, const float4 s, u64 (&ac)[5]) {
+            u64 dot = mul2(q[0], P.p[0]);
+#pragma unroll
+            for (int c = 1; c < 8; c++) dot = fma2(q[c], P.p[c], dot);
+            const u64 ex = fma2(P.klm2, dot, fma2(P.kl, nn, P.base));
+            float e0, e1;
+            upk2(ex, e0, e1);
+            float l0, l1;
+            asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(l0) : "f"(fminf(e0, 2.f)));
+            asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(l1) : "f"(fminf(e1, 2.f)));
+            const u64 lws = pk2(l0, l1);
+            const u64 d1 = fma2(P.c1, cb, P.no1), d2 = fma2(P.c2, cr, P.no2);
+            // q = lws^2 + d1^2 + d2^2 - log2 sw;  wc = exp2(-q)
+            const u64 q = fma2(lws, lws, fma2(d1, d1, fma2(d2, d2, pk2(s.z, s.w))));
+            float n0, n1;
+            upk2(q, n0, n1);
+            const float w0 = ex2_approx(-n0), w1 = ex2_approx(-n1);
+            const u64 wc = pk2(w0, w1);
+            const u64 wy = mul2(pk2(s.x, s.y), lws);
+            ac[0] = fma2(wy, yy, ac[0]);
+            ac[1] = fma2(wc, cb, ac[1]);
+            ac[2] = fma2(wc, cr, ac[2]);
+            ac[3] = add2(ac[3], wy);
+            ac[4] = add2(ac[4], wc);
+        };
+        if (A) pair(pa, sm.sp[r * 21 + i], acc[0]);
+        if (B) pair(pb, sm.sp[(r - 2) * 21 + i], acc[1]);
+    }
+}
+
+// pcaProjection (demosaic.metal:774-796) fused into the tile producer: the
+// 5x5 luma patch of every window position times the 25 x 8 basis, as FP16
+// tensor-core MMAs (mma.sync m16n8k16, FP32 accumulate). 52 x 52 = 2704
+// positions = 169 chunks of 16 rows; K = 25 padded to 32 (two k-steps);
+// N = the 8 components. The luma tile (window region + 2) is staged once.
+constexpr int BX_LW = BX_W + 4, BX_LH = BX_H + 4;  // luma tile, origin (x0 - 12, y0 - 12)
+
+__device__ __forceinline__ uint32_t h2u(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
+
+__global__ void __launch_bounds__(256, 2) k_block_match_pair(Plane<__half, 4> img, Plane<__half, 2> grad,
+                                                             const float* __restrict__ basis, Plane<__half, 4> out,
+                                                             BlockMatchArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BmPairSmem& sm = *reinterpret_cast<BmPairSmem*>(smem_raw);
+    __half* luma = reinterpret_cast<__half*>(smem_raw + sizeof(BmPairSmem));  // BX_LH x BX_LW
+    __shared__ float cen[8];
+    __shared__ float bsm[25][8];
+    const int x0 = blockIdx.x * BX_TX, y0 = blockIdx.y * (BX_NP * BX_TY);
+    const int tid = threadIdx.y * BX_TX + threadIdx.x;
+    const float kLog2e = 1.4426950408889634f, lk = 2.f * kLog2e, isq = rsqrtf(lk);
+    for (int k = tid; k < 22 * 21; k += 256) {
+        const int j = k / 21, i = k % 21 - 10;
+        // window row j of the pair's first pixel, j - 1 of its second
+        const float w0 = j <= 20 ? spatial_weight(i, j - 10) : 0.f;
+        const float w1 = j >= 1 ? spatial_weight(i, j - 11) : 0.f;
+        sm.sp[k] = make_float4(w0 * isq, w1 * isq, -log2f(w0), -log2f(w1));
+    }
+    if (tid < 200) bsm[tid / 8][tid % 8] = basis[tid];
+    for (int k = tid; k < BX_LW * BX_LH; k += 256) {
+        const int ty = k / BX_LW, tx = k % BX_LW;
+        luma[k] = *img.pxc(x0 - 12 + tx, y0 - 12 + ty);
+    }
+    for (int k = tid; k < BX_W * BX_H; k += 256) {
+        const int ty = k / BX_W, tx = k % BX_W;
+        const f4 p = ld4<__half>(img.pxc(x0 - 10 + tx, y0 - 10 + ty));
+        sm.ycc[k] = make_float4(p.x, p.y, p.z, 0.f);
+    }
+    __syncthreads();
+    if (tid < 8) {  // centring vector: the tile-centre pixel's coefficients (FP32)
+        const int cx = BX_TX / 2 + 12, cy = BX_NP * BX_TY / 2 + 12;  // luma-tile coordinates
+        float c = 0.f;
+        for (int k = 0; k < 25; k++) c += bsm[k][tid] * __half2float(luma[(cy + k / 5 - 2) * BX_LW + cx + k % 5 - 2]);
+        cen[tid] = c;
+    }
+    // B fragments (basis, k x n, "col" layout): rows 2t, 2t+1, 2t+8, 2t+9 of column g, per k-step
+    const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
+    uint32_t bf[2][2];
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+        auto bk = [&](int k) { return k < 25 ? bsm[k][g] : 0.f; };
+        const int k0 = 16 * s + 2 * t;
+        bf[s][0] = h2u(__floats2half2_rn(bk(k0), bk(k0 + 1)));
+        bf[s][1] = h2u(__floats2half2_rn(bk(k0 + 8), bk(k0 + 9)));
+    }
+    __syncthreads();
+    uint32_t* pca32 = reinterpret_cast<uint32_t*>(sm.pca);  // [position][4] half2
+    for (int ch = warp; ch < (BX_W * BX_H) / 16; ch += 8) {
+        const int m0 = ch * 16 + g, m1 = m0 + 8;  // the two rows of this thread
+        // patch centre in the luma tile: the clamped image position of the
+        // window position, as a clamped read of a projected plane would see
+        auto lidx = [&](int m) {
+            const int px = clampi(x0 - 10 + m % BX_W, 0, img.w - 1) - (x0 - 12);
+            const int py = clampi(y0 - 10 + m / BX_W, 0, img.h - 1) - (y0 - 12);
+            return py * BX_LW + px;
+        };
+        const int l0 = lidx(m0), l1 = lidx(m1);
+        auto av = [&](int l, int k) {  // patch element k of the position at luma index l
+            return k < 25 ? luma[l + (k / 5 - 2) * BX_LW + (k % 5 - 2)] : __float2half(0.f);
+        };
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            const int k0 = 16 * s + 2 * t;
+            const uint32_t a0 = h2u(__halves2half2(av(l0, k0), av(l0, k0 + 1)));
+            const uint32_t a1 = h2u(__halves2half2(av(l1, k0), av(l1, k0 + 1)));
+            const uint32_t a2 = h2u(__halves2half2(av(l0, k0 + 8), av(l0, k0 + 9)));
+            const uint32_t a3 = h2u(__halves2half2(av(l1, k0 + 8), av(l1, k0 + 9)));
+            asm volatile(
+                "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                "{%0,%1,%2,%3};"
+                : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+                : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(bf[s][0]), "r"(bf[s][1]));
+        }
+        // rows m0 (c0, c1) and m1 (c2, c3), components 2t, 2t+1; centre, round, store
+        const __half2 h0 = __floats2half2_rn(c[0] - cen[2 * t], c[1] - cen[2 * t + 1]);
+        const __half2 h1 = __floats2half2_rn(c[2] - cen[2 * t], c[3] - cen[2 * t + 1]);
+        pca32[m0 * 4 + t] = h2u(h0);
+        pca32[m1 * 4 + t] = h2u(h1);
+        const float2 f0 = __half22float2(h0), f1 = __half22float2(h1);
+        float n0 = f0.x * f0.x + f0.y * f0.y, n1 = f1.x * f1.x + f1.y * f1.y;
+        n0 += __shfl_xor_sync(0xffffffffu, n0, 1);
+        n0 += __shfl_xor_sync(0xffffffffu, n0, 2);
+        n1 += __shfl_xor_sync(0xffffffffu, n1, 1);
+        n1 += __shfl_xor_sync(0xffffffffu, n1, 2);
+        if (t == 0) {
+            sm.ycc[m0].w = n0;
+            sm.ycc[m1].w = n1;
+        }
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.x, y = y0 + BX_NP * threadIdx.y;
+    float pc[BX_NP][8], kl[BX_NP], base[BX_NP], c1[BX_NP], c2[BX_NP], o1[BX_NP], o2[BX_NP];
+#pragma unroll
+    for (int p = 0; p < BX_NP; p++) {
+        const int c = (BX_NP * threadIdx.y + p + 10) * BX_W + threadIdx.x + 10;
+        const float4 in = sm.ycc[c];
+        const uint4 u = sm.pca[c];
+        const float2 a0 = __half22float2(u2h_(u.x)), a1 = __half22float2(u2h_(u.y));
+        const float2 a2 = __half22float2(u2h_(u.z)), a3 = __half22float2(u2h_(u.w));
+        pc[p][0] = a0.x; pc[p][1] = a0.y; pc[p][2] = a1.x; pc[p][3] = a1.y;
+        pc[p][4] = a2.x; pc[p][5] = a2.y; pc[p][6] = a3.x; pc[p][7] = a3.y;
+        const BmConst k =
+            bm_const<__half>(a, grad, img.w, img.h, min(x, img.w - 1), min(y + p, img.h - 1), in.x, in.y, in.z);
+        kl[p] = fmaxf(-2.f * kLog2e * k.s * k.s, -1e30f);
+        base[p] = fmaf(kl[p], in.w, 0.5f * log2f(lk));
+        const float sq = sqrtf(lk);
+        c1[p] = sq * k.c1;
+        c2[p] = sq * k.c2;
+        o1[p] = c1[p] * in.y;
+        o2[p] = c2[p] * in.z;
+    }
+    BmPair PA, PB;
+    for (int c = 0; c < 8; c++) {
+        PA.p[c] = pk2(pc[0][c], pc[1][c]);
+        PB.p[c] = pk2(pc[2][c], pc[3][c]);
+    }
+    PA.kl = pk2(kl[0], kl[1]);
+    PB.kl = pk2(kl[2], kl[3]);
+    PA.klm2 = pk2(-2.f * kl[0], -2.f * kl[1]);
+    PB.klm2 = pk2(-2.f * kl[2], -2.f * kl[3]);
+    PA.base = pk2(base[0], base[1]);
+    PB.base = pk2(base[2], base[3]);
+    PA.c1 = pk2(c1[0], c1[1]);
+    PB.c1 = pk2(c1[2], c1[3]);
+    PA.c2 = pk2(c2[0], c2[1]);
+    PB.c2 = pk2(c2[2], c2[3]);
+    PA.no1 = pk2(-o1[0], -o1[1]);
+    PB.no1 = pk2(-o1[2], -o1[3]);
+    PA.no2 = pk2(-o2[0], -o2[1]);
+    PB.no2 = pk2(-o2[2], -o2[3]);
+    u64 acc[2][5];
+    for (int k = 0; k < 5; k++) acc[0][k] = acc[1][k] = pk2(0.f, 0.f);
+    const int col = threadIdx.x, row0 = BX_NP * threadIdx.y;
+    auto rb = [&](int r) { return (row0 + r) * BX_W + col; };
+    bmp2_row<true, false>(sm, rb(0), 0, PA, PB, acc);
+    bmp2_row<true, false>(sm, rb(1), 1, PA, PB, acc);
+    for (int r = 2; r <= 21; r++) bmp2_row<true, true>(sm, rb(r), r, PA, PB, acc);
+    bmp2_row<false, true>(sm, rb(22), 22, PA, PB, acc);
+    bmp2_row<false, true>(sm, rb(23), 23, PA, PB, acc);
+    float v[2][5][2];
+    for (int q = 0; q < 2; q++)
+        for (int k = 0; k < 5; k++) upk2(acc[q][k], v[q][k][0], v[q][k][1]);
+    if (x < out.w) {
+#pragma unroll
+        for (int p = 0; p < BX_NP; p++) {
+            const int q = p >> 1, m = p & 1;
+            if (y + p < out.h)
+                st4<__half>(out.px(x, y + p), f4{v[q][0][m] / v[q][3][m], v[q][1][m] / v[q][4][m],
+                                                 v[q][2][m] / v[q][4][m], v[q][3][m]});
+        }
+    }
+}
+
 template <class S>
-void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, Plane<S, 4> out, const BlockMatchArgs& a,
-                        cudaStream_t s) {
+void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, const float* basis, Plane<S, 4> out,
+                        const BlockMatchArgs& a, cudaStream_t s) {
     if constexpr (is_half<S>::value) {
+        const size_t smem = sizeof(BmPairSmem) + sizeof(__half) * BX_LW * BX_LH;
         static bool attr = false;
         if (!attr) {
-            cudaFuncSetAttribute(k_block_match_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(BmFastSmem)));
+            cudaFuncSetAttribute(k_block_match_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
             attr = true;
         }
         dim3 b(BX_TX, BX_TY);
         dim3 g((img.w + BX_TX - 1) / BX_TX, (img.h + BX_NP * BX_TY - 1) / (BX_NP * BX_TY));
-        k_block_match_fast<<<g, b, sizeof(BmFastSmem), s>>>(img, grad, pca, out, a);
+        k_block_match_pair<<<g, b, smem, s>>>(img, grad, basis, out, a);
     } else {
         static bool attr = false;
         if (!attr) {
@@ -346,9 +596,9 @@ void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, Plan
     }
 }
 
-template void launch_block_match<float>(Plane<float, 4>, Plane<float, 2>, Plane<float, 8>, Plane<float, 4>,
-                                        const BlockMatchArgs&, cudaStream_t);
-template void launch_block_match<__half>(Plane<__half, 4>, Plane<__half, 2>, Plane<__half, 8>, Plane<__half, 4>,
-                                         const BlockMatchArgs&, cudaStream_t);
+template void launch_block_match<float>(Plane<float, 4>, Plane<float, 2>, Plane<float, 8>, const float*,
+                                        Plane<float, 4>, const BlockMatchArgs&, cudaStream_t);
+template void launch_block_match<__half>(Plane<__half, 4>, Plane<__half, 2>, Plane<__half, 8>, const float*,
+                                         Plane<__half, 4>, const BlockMatchArgs&, cudaStream_t);
 
 }  // namespace gls

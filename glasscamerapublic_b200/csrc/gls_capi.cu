@@ -329,7 +329,7 @@ static gls_status pyramid_run(gls_converter* cv, Pipeline<S>& P, Plane<S, 4> img
             launch_pca_eigen(part, n_blocks, n_patches, basis + i * 200, status + i, s);
         }
         Plane<S, 8> pcap = plane<S, 8>(P.pca, wi, hi);
-        {
+        if (!is_half<S>::value) {  // the FP16 path projects inside the block-matching kernel
             KScope k(cv->prof, KC_PCA_PROJECT, s);
             launch_pca_project<S>(layer, basis + i * 200, pcap, s);
         }
@@ -346,7 +346,7 @@ static gls_status pyramid_run(gls_converter* cv, Pipeline<S>& P, Plane<S, 4> img
         ba.gradient_threshold = dp.gradient_threshold;
         ba.lsc = p->lens_shading_correction;
         KScope k(cv->prof, KC_BLOCK_MATCH, s);
-        launch_block_match<S>(layer, grd[i], pcap, plane<S, 4>(P.den[i], wi, hi), ba, s);
+        launch_block_match<S>(layer, grd[i], pcap, basis + i * 200, plane<S, 4>(P.den[i], wi, hi), ba, s);
     }
     GLS_CUDA(cudaGetLastError());
     cv->last_levels = L;

@@ -96,8 +96,10 @@ void launch_pca_eigen(const double* part, int n_blocks, int n_patches, float* ba
                       cudaStream_t s);
 template <class S>
 void launch_pca_project(Plane<S, 4> img, const float* basis, Plane<S, 8> out, cudaStream_t s);
+// FP32 path: reads the projected `pca` plane; FP16 path: projects on tensor
+// cores inside the kernel from `basis` (the pca plane is not used)
 template <class S>
-void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, Plane<S, 4> out,
+void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, const float* basis, Plane<S, 4> out,
                         const BlockMatchArgs& a, cudaStream_t s);
 
 // host-side eigen-solve of the same accumulators (the reference's per-level
