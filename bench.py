@@ -106,12 +106,15 @@ class ClockSampler:
 
 
 def cpu_baseline(wl, params_fn, seconds: float):
-    """The oracle's FP32 run (the CPU restatement of the reference path) on
-    all host cores, over a bounded sample: a 1008x756 frame of the same
-    scene recipe and 5-level schedule (1/16 of the 12 MP area), repeated for
-    about `seconds`; frames/s scaled to 12 MP by the pixel-count ratio."""
+    """The reference's path on all host cores, over a bounded sample: a
+    1008x756 frame of the same scene recipe and 5-level schedule (1/16 of
+    the 12 MP area), repeated for about `seconds`; frames/s scaled to 12 MP
+    by the pixel-count ratio. It runs the reference's own Metal kernels
+    compiled for the CPU (oracle/_ref, kind "reference") where they were
+    built, else the oracle's FP32 restatement (kind "port")."""
     sys.path.insert(0, str(ROOT / "tests"))
     import _oracle as O
+    import _ref as R
     from glasscamerapublic_b200 import scene
     sw, sh = wl.width // 4, wl.height // 4
     swl = scene.Workload("cpu_sample", sw, sh, levels=wl.levels, black=wl.black, white=wl.white, gain=wl.gain,
@@ -119,24 +122,32 @@ def cpu_baseline(wl, params_fn, seconds: float):
     raw, _ = scene.make_raw(swl)
     p = params_fn(swl)
     threads = os.cpu_count() or 1
-    O.lib().orc_set_threads(threads)
+    if R.available():
+        kind, what = "reference", "reference Metal kernels compiled for the CPU"
+        R.lib().ref_set_threads(threads)
+        run = lambda: R.raw_pipeline(raw, p, denoise=True)
+    else:
+        kind, what = "port", "FP32 oracle"
+        O.lib().orc_set_threads(threads)
+        run = lambda: O.raw_pipeline(raw, p, denoise=True, f64=False)
     t0 = time.perf_counter()
     n = 0
     while True:
-        O.raw_pipeline(raw, p, denoise=True, f64=False)
+        run()
         n += 1
         if time.perf_counter() - t0 >= seconds:
             break
     dt = time.perf_counter() - t0
     fps_sample = n / dt
     scale = (sw * sh) / (wl.width * wl.height)
-    return {"value": fps_sample * scale, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{n} x {sw}x{sh} frame(s), 5 levels, FP32 oracle, {dt:.1f}s; frames/s scaled by area x{scale:.4f}"}
+    return {"value": fps_sample * scale, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{n} x {sw}x{sh} frame(s), 5 levels, {what}, {dt:.1f}s; frames/s scaled by area x{scale:.4f}"}
 
 
 def run_reference(args, rank):
-    """The reference arm: the reference's algorithm on host cores (the
-    oracle port; the Metal reference cannot run here)."""
+    """The reference arm: the reference's path on the host cores. The Metal
+    runtime cannot run here; the reference's own kernel source, compiled
+    for the CPU (oracle/_ref), stands in for it, else the oracle port."""
     if rank != 0:
         return
     from glasscamerapublic_b200 import scene
@@ -151,9 +162,10 @@ def run_reference(args, rank):
     v = float(np.median(vals)) if vals else last["value"]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f16/f32 (the reference's half/float kernels)",
+            "data": "synthetic",
             "config": {"workload": WORKLOAD, "frame": "4032x3024 RGGB 12-bit", "levels": 5},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": last["cores"], "kind": "port",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": last["cores"], "kind": last["kind"],
                              "sample": last["sample"]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

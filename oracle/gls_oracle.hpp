@@ -780,7 +780,7 @@ inline void jacobi_eigen(int n, std::vector<double>& a, std::vector<double>& v) 
 // e0, e1, ... against the columns before them. Every column's sign is fixed
 // so that its largest-magnitude entry (first on ties) is positive.
 inline void select_basis(const double ev[25], const double evec[25][25], std::array<std::array<double, 8>, 25>& basis) {
-    const double lam0 = std::max(ev[0], 0.0);
+    const double lam0 = std::max(ev[0], double(0));
     const double tol = 1e-9 * lam0;
     int cand = 0;
     bool kept = true;

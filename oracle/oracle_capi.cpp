@@ -130,6 +130,74 @@ int orc_pyramid_denoise(const float* ycc, const float* grad, int w, int h, const
     return 0;
 }
 
+// ---- single stages from given inputs (for the stage-by-stage pin against
+// the reference's own kernels, oracle/ref_harness.cpp)
+
+int orc_scale(const uint16_t* raw, int w, int h, const gls_demosaic_params* gp, int f64, float* scaled) {
+    const Params p = to_params(gp);
+    if (f64) copy_out(scale_raw<double>(raw, w, w, h, p), scaled);
+    else copy_out(scale_raw<float>(raw, w, w, h, p), scaled);
+    return 0;
+}
+
+int orc_sobel_blur(const float* scaled, int w, int h, const gls_demosaic_params* gp, int f64, float* grad) {
+    const Params p = to_params(gp);
+    static const Taps t1 = gaussian_bilinear_taps(1.5f), t2 = gaussian_bilinear_taps(4.5f);
+    auto run = [&](auto tag) {
+        using T = decltype(tag);
+        auto s = copy_in<T, 1>(scaled, w, h);
+        copy_out(gradient_blur(s, sobel(s), t1, t2, raw_variance(p.raw_nlf)[1]), grad);
+    };
+    if (f64) run(double());
+    else run(float());
+    return 0;
+}
+
+int orc_raw_denoise(const float* scaled, const float* grad, int w, int h, const gls_demosaic_params* gp, int f64,
+                    float* scaled_out) {
+    const Params p = to_params(gp);
+    auto run = [&](auto tag) {
+        using T = decltype(tag);
+        auto s = copy_in<T, 1>(scaled, w, h);
+        auto g = copy_in<T, 2>(grad, w, h);
+        auto rgba = bayer_to_rgba(s, p.bayer);
+        auto ds = despeckle_raw_rgba(rgba, g, p.raw_nlf.b);
+        auto cd = cross_denoise_raw_rgba(ds, p.raw_nlf.b, p.raw_strength);
+        rgba_to_bayer(cd, p.bayer, s);
+        copy_out(s, scaled_out);
+    };
+    if (f64) run(double());
+    else run(float());
+    return 0;
+}
+
+int orc_demosaic_rgb(const float* scaled, const float* grad, int w, int h, const gls_demosaic_params* gp, int f64,
+                     float* rgb) {
+    const Params p = to_params(gp);
+    auto run = [&](auto tag) {
+        using T = decltype(tag);
+        auto s = copy_in<T, 1>(scaled, w, h);
+        auto g = copy_in<T, 2>(grad, w, h);
+        auto out = demosaic(s, g, p.bayer, raw_variance(p.raw_nlf));
+        blend_highlights(out, T(1));
+        copy_out(out, rgb);
+    };
+    if (f64) run(double());
+    else run(float());
+    return 0;
+}
+
+int orc_despeckle(const float* ycc, int w, int h, const gls_demosaic_params* gp, int f64, float* out) {
+    const Params p = to_params(gp);
+    auto run = [&](auto tag) {
+        using T = decltype(tag);
+        copy_out(despeckle_luma_median_chroma(copy_in<T, 4>(ycc, w, h), p.pyr_nlf[0].a, p.pyr_nlf[0].b), out);
+    };
+    if (f64) run(double());
+    else run(float());
+    return 0;
+}
+
 int orc_gaussian_taps(float radius, float* taps, int max_taps, int* n) {
     Taps t = gaussian_bilinear_taps(radius);
     *n = int(t.t.size());

@@ -138,3 +138,32 @@ def jacobi(a: np.ndarray):
     vec = np.zeros((n, n))
     lib().orc_jacobi(n, _dp(a), _dp(ev), _dp(vec))
     return ev, vec
+
+
+# ---- stage entry points (same inputs as the reference harness's stages)
+def _stage_setup(L):
+    fp = C.POINTER(C.c_float)
+    P = C.POINTER(DemosaicParams)
+    L.orc_scale.argtypes = [C.c_void_p, C.c_int, C.c_int, P, C.c_int, fp]
+    L.orc_sobel_blur.argtypes = [fp, C.c_int, C.c_int, P, C.c_int, fp]
+    L.orc_raw_denoise.argtypes = [fp, fp, C.c_int, C.c_int, P, C.c_int, fp]
+    L.orc_demosaic_rgb.argtypes = [fp, fp, C.c_int, C.c_int, P, C.c_int, fp]
+    L.orc_despeckle.argtypes = [fp, C.c_int, C.c_int, P, C.c_int, fp]
+
+
+def stage(name, *arrays, p, w, h, out_shape, f64=False, raw=None):
+    L = lib()
+    if not hasattr(L, "_stages_ready"):
+        _stage_setup(L)
+        L._stages_ready = True
+    out = np.zeros(out_shape, np.float32)
+    args = [(_fp(np.ascontiguousarray(a, np.float32))) for a in arrays]
+    keep = [np.ascontiguousarray(a, np.float32) for a in arrays]
+    args = [_fp(k) for k in keep]
+    fn = getattr(L, "orc_" + name)
+    if raw is not None:
+        raw = np.ascontiguousarray(raw, np.uint16)
+        assert fn(raw.ctypes.data, w, h, C.byref(p), int(f64), _fp(out)) == 0
+    else:
+        assert fn(*args, w, h, C.byref(p), int(f64), _fp(out)) == 0
+    return out

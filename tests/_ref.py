@@ -1,0 +1,115 @@
+"""ctypes binding of oracle/_ref/libglsref.so: the reference's own Metal
+kernels (demosaic.metal) compiled as C++ and run on the CPU, stage by stage
+(see oracle/ref_harness.cpp). Built by `make -C oracle ref` where the
+reference tree is present; the shared object travels with the repository
+snapshot, so tests that need it skip only where it was never built."""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from glasscamerapublic_b200 import DemosaicParams
+
+REF_LIB = Path(__file__).resolve().parents[1] / "oracle" / "_ref" / "libglsref.so"
+_lib = None
+
+
+def available() -> bool:
+    return REF_LIB.exists()
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        L = C.CDLL(str(REF_LIB))
+        fp = C.POINTER(C.c_float)
+        dp = C.POINTER(C.c_double)
+        P = C.POINTER(DemosaicParams)
+        L.ref_scale.argtypes = [C.c_void_p, C.c_int, C.c_int, P, fp]
+        L.ref_sobel_blur.argtypes = [fp, C.c_int, C.c_int, P, fp]
+        L.ref_raw_denoise.argtypes = [fp, fp, C.c_int, C.c_int, P, fp]
+        L.ref_demosaic_rgb.argtypes = [fp, fp, C.c_int, C.c_int, P, fp]
+        L.ref_transform.argtypes = [fp, C.c_int, C.c_int, fp, fp]
+        L.ref_despeckle.argtypes = [fp, C.c_int, C.c_int, P, fp]
+        L.ref_pyramid_denoise.argtypes = [fp, fp, C.c_int, C.c_int, P, fp, fp, dp]
+        L.ref_raw_pipeline.argtypes = [C.c_void_p, C.c_int, C.c_int, P, C.c_int, fp]
+        L.ref_set_threads.argtypes = [C.c_int]
+        _lib = L
+    return _lib
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+def scale(raw, p):
+    raw = np.ascontiguousarray(raw, np.uint16)
+    h, w = raw.shape
+    out = np.zeros((h, w), np.float32)
+    lib().ref_scale(raw.ctypes.data, w, h, C.byref(p), _fp(out))
+    return out
+
+
+def sobel_blur(scaled, p):
+    s = _f32(scaled)
+    h, w = s.shape
+    out = np.zeros((h, w, 2), np.float32)
+    lib().ref_sobel_blur(_fp(s), w, h, C.byref(p), _fp(out))
+    return out
+
+
+def raw_denoise(scaled, grad, p):
+    s, g = _f32(scaled), _f32(grad)
+    h, w = s.shape
+    out = np.zeros((h, w), np.float32)
+    lib().ref_raw_denoise(_fp(s), _fp(g), w, h, C.byref(p), _fp(out))
+    return out
+
+
+def demosaic_rgb(scaled, grad, p):
+    s, g = _f32(scaled), _f32(grad)
+    h, w = s.shape
+    out = np.zeros((h, w, 4), np.float32)
+    lib().ref_demosaic_rgb(_fp(s), _fp(g), w, h, C.byref(p), _fp(out))
+    return out
+
+
+def transform(img, m9):
+    a = _f32(img)
+    m = _f32(np.asarray(m9).ravel())
+    h, w = a.shape[:2]
+    out = np.zeros((h, w, 4), np.float32)
+    lib().ref_transform(_fp(a), w, h, _fp(m), _fp(out))
+    return out
+
+
+def despeckle(ycc, p):
+    a = _f32(ycc)
+    h, w = a.shape[:2]
+    out = np.zeros((h, w, 4), np.float32)
+    lib().ref_despeckle(_fp(a), w, h, C.byref(p), _fp(out))
+    return out
+
+
+def pyramid_denoise(ycc, grad, p):
+    a, g = _f32(ycc), _f32(grad)
+    h, w = a.shape[:2]
+    out = np.zeros((h, w, 4), np.float32)
+    bases = np.zeros((p.levels, 25, 8), np.float64)
+    lib().ref_pyramid_denoise(_fp(a), _fp(g), w, h, C.byref(p), _fp(out), None,
+                              bases.ctypes.data_as(C.POINTER(C.c_double)))
+    return out, bases
+
+
+def raw_pipeline(raw, p, denoise=True):
+    raw = np.ascontiguousarray(raw, np.uint16)
+    h, w = raw.shape
+    out = np.zeros((h, w, 4), np.float32)
+    assert lib().ref_raw_pipeline(raw.ctypes.data, w, h, C.byref(p), int(denoise), _fp(out)) == 0
+    return out
