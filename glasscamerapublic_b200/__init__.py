@@ -11,6 +11,8 @@ import ctypes as C
 import os
 from pathlib import Path
 
+import numpy as np
+
 PKG_DIR = Path(__file__).resolve().parent
 LIB_PATH = PKG_DIR / "libglscam.so"
 
@@ -103,6 +105,13 @@ class KernelStat(C.Structure):
     _fields_ = [("name", C.c_char_p), ("launches", C.c_uint64), ("ms", C.c_double)]
 
 
+# gls_keypoint / gls_match as numpy record types (the reference's KeyPoint
+# and DMatch layouts)
+KEYPOINT_DTYPE = np.dtype([("x", np.float32), ("y", np.float32), ("size", np.float32), ("angle", np.float32),
+                           ("response", np.float32), ("octave", np.int32), ("class_id", np.int32)])
+MATCH_DTYPE = np.dtype([("query_idx", np.int32), ("train_idx", np.int32), ("distance", np.float32)])
+
+
 class GlsError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"gls status {code}: {msg}")
@@ -129,6 +138,24 @@ _SIGNATURES = {
     "gls_converter_reset_stats": (C.c_int, [C.c_void_p]),
     "gls_calibration_fill": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(DemosaicParams)]),
     "gls_gaussian_bilinear_taps": (C.c_int, [C.c_float, C.POINTER(C.c_float), C.c_int32, C.POINTER(C.c_int32)]),
+    "gls_surf_create": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_float,
+                                  C.POINTER(C.c_void_p)]),
+    "gls_surf_destroy": (C.c_int, [C.c_void_p]),
+    "gls_surf_detect_and_compute": (C.c_int, [C.c_void_p, C.POINTER(ImageView), C.c_int32, C.c_uint32, C.c_void_p]),
+    "gls_surf_features": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
+                                    C.POINTER(C.c_int32), C.c_void_p]),
+    "gls_surf_match": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.POINTER(C.c_int32),
+                                 C.c_void_p]),
+    "gls_surf_find_homography": (C.c_int, [C.c_void_p, C.c_float, C.c_int32, C.POINTER(C.c_float),
+                                           C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_void_p]),
+    "gls_find_homography": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int32, C.c_float, C.c_int32,
+                                      C.POINTER(C.c_float), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_void_p]),
+    "gls_scale_homography": (C.c_int, [C.POINTER(C.c_float), C.c_float, C.POINTER(C.c_float)]),
+    "gls_raw_channels": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_size_t, C.c_int32, C.c_float,
+                                   C.c_float, C.c_float, C.c_uint32, C.POINTER(ImageView), C.c_uint32, C.c_void_p]),
+    "gls_register_and_fuse": (C.c_int, [C.POINTER(ImageView), C.POINTER(ImageView), C.POINTER(ImageView),
+                                        C.POINTER(C.c_float), C.c_int32, C.c_void_p]),
+    "gls_register_image": (C.c_int, [C.POINTER(ImageView), C.POINTER(ImageView), C.POINTER(C.c_float), C.c_void_p]),
 }
 
 _lib = None

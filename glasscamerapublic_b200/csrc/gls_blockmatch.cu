@@ -187,145 +187,10 @@ __global__ void __launch_bounds__(256) k_block_match_plain(Plane<S, 4> img, Plan
 //     exp under fast math here).
 constexpr int BX_NP = 4, BX_TX = 32, BX_TY = 8, BX_W = BX_TX + 20, BX_H = BX_NP * BX_TY + 20;
 
-struct BmFastSmem {
-    uint4 pca[BX_H * BX_W];   // q - c, 8 halves
-    float4 ycc[BX_H * BX_W];  // Y, Cb, Cr, |q - c|^2
-    float2 sp[21 * 21];       // (sw / sqrt(2 log2 e), log2 sw)
-};
-
-struct BmFastPix {
-    float4 p0, p1;   // p - c
-    float kl, klm2;  // kl = -2 log2(e) s^2, klm2 = -2 kl
-    float base;      // kl |p'|^2 + 0.5 log2(2 log2 e)
-    float c1, c2, o1, o2;
-};
-
-// One window row r (0 .. 23) of the thread's column; pixel p uses it when
-// p <= r <= p + 20 (bit p of MASK), with window row offset r - p.
-template <int MASK>
-__device__ __forceinline__ void bmx_row(const BmFastSmem& sm, int base, int r, const BmFastPix (&P)[BX_NP],
-                                        float (&acc)[BX_NP][5]) {
-#pragma unroll 7  // full unrolling spills past the 128-register budget of 2 blocks/SM
-    for (int i = 0; i < 21; i++) {
-        const uint4 u = sm.pca[base + i];
-        const float2 a0 = __half22float2(u2h_(u.x)), a1 = __half22float2(u2h_(u.y));
-        const float2 a2 = __half22float2(u2h_(u.z)), a3 = __half22float2(u2h_(u.w));
-        const float4 y = sm.ycc[base + i];
-#pragma unroll
-        for (int p = 0; p < BX_NP; p++) {
-            if (!(MASK & (1 << p))) continue;
-            const BmFastPix& q = P[p];
-            const float2 sw = sm.sp[(r - p) * 21 + i];
-            float dot = a0.x * q.p0.x;
-            dot = fmaf(a0.y, q.p0.y, dot);
-            dot = fmaf(a1.x, q.p0.z, dot);
-            dot = fmaf(a1.y, q.p0.w, dot);
-            dot = fmaf(a2.x, q.p1.x, dot);
-            dot = fmaf(a2.y, q.p1.y, dot);
-            dot = fmaf(a3.x, q.p1.z, dot);
-            dot = fmaf(a3.y, q.p1.w, dot);
-            const float lws = ex2_approx(fminf(fmaf(q.klm2, dot, fmaf(q.kl, y.w, q.base)), 2.f));
-            const float e1 = fmaf(q.c1, y.y, -q.o1), e2 = fmaf(q.c2, y.z, -q.o2);
-            const float wc = ex2_approx(fmaf(-lws, lws, fmaf(-e1, e1, fmaf(-e2, e2, sw.y))));
-            const float wy = sw.x * lws;
-            acc[p][0] = fmaf(wy, y.x, acc[p][0]);
-            acc[p][1] = fmaf(wc, y.y, acc[p][1]);
-            acc[p][2] = fmaf(wc, y.z, acc[p][2]);
-            acc[p][3] += wy;
-            acc[p][4] += wc;
-        }
-    }
-}
-
-__global__ void __launch_bounds__(256, 2) k_block_match_fast(Plane<__half, 4> img, Plane<__half, 2> grad,
-                                                             Plane<__half, 8> pca, Plane<__half, 4> out,
-                                                             BlockMatchArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    BmFastSmem& sm = *reinterpret_cast<BmFastSmem*>(smem_raw);
-    __shared__ float cen[8];
-    const int x0 = blockIdx.x * BX_TX, y0 = blockIdx.y * (BX_NP * BX_TY);
-    const int tid = threadIdx.y * BX_TX + threadIdx.x;
-    const float kLog2e = 1.4426950408889634f, lk = 2.f * kLog2e, isq = rsqrtf(lk);
-    for (int k = tid; k < 441; k += 256) {
-        const float w = spatial_weight(k % 21 - 10, k / 21 - 10);
-        sm.sp[k] = make_float2(w * isq, log2f(w));
-    }
-    if (tid < 8) {  // centring vector: the tile-centre pixel's coefficients
-        const int cx = clampi(x0 + BX_TX / 2, 0, img.w - 1), cy = clampi(y0 + BX_NP * BX_TY / 2, 0, img.h - 1);
-        cen[tid] = __half2float(pca.px(cx, cy)[tid]);
-    }
-    __syncthreads();
-    for (int k = tid; k < BX_W * BX_H; k += 256) {
-        const int ty = k / BX_W, tx = k % BX_W;
-        const int sx = clampi(x0 - 10 + tx, 0, img.w - 1), sy = clampi(y0 - 10 + ty, 0, img.h - 1);
-        const uint4 u = *reinterpret_cast<const uint4*>(pca.px(sx, sy));
-        const float2 a0 = __half22float2(u2h_(u.x)), a1 = __half22float2(u2h_(u.y));
-        const float2 a2 = __half22float2(u2h_(u.z)), a3 = __half22float2(u2h_(u.w));
-        const __half2 h0 = __floats2half2_rn(a0.x - cen[0], a0.y - cen[1]);
-        const __half2 h1 = __floats2half2_rn(a1.x - cen[2], a1.y - cen[3]);
-        const __half2 h2 = __floats2half2_rn(a2.x - cen[4], a2.y - cen[5]);
-        const __half2 h3 = __floats2half2_rn(a3.x - cen[6], a3.y - cen[7]);
-        // the norm of the values as stored (rounded), so |p'-q'|^2 is exact in them
-        const float2 b0 = __half22float2(h0), b1 = __half22float2(h1), b2 = __half22float2(h2), b3 = __half22float2(h3);
-        const float n = b0.x * b0.x + b0.y * b0.y + b1.x * b1.x + b1.y * b1.y + b2.x * b2.x + b2.y * b2.y +
-                        b3.x * b3.x + b3.y * b3.y;
-        uint4 hv;
-        hv.x = *reinterpret_cast<const uint32_t*>(&h0);
-        hv.y = *reinterpret_cast<const uint32_t*>(&h1);
-        hv.z = *reinterpret_cast<const uint32_t*>(&h2);
-        hv.w = *reinterpret_cast<const uint32_t*>(&h3);
-        sm.pca[k] = hv;
-        const f4 p = ld4<__half>(img.px(sx, sy));
-        sm.ycc[k] = make_float4(p.x, p.y, p.z, n);
-    }
-    __syncthreads();
-    const int x = x0 + threadIdx.x, y = y0 + BX_NP * threadIdx.y;
-    BmFastPix P[BX_NP];
-#pragma unroll
-    for (int p = 0; p < BX_NP; p++) {
-        const int c = (BX_NP * threadIdx.y + p + 10) * BX_W + threadIdx.x + 10;
-        const float4 in = sm.ycc[c];
-        const uint4 u = sm.pca[c];
-        const float2 a0 = __half22float2(u2h_(u.x)), a1 = __half22float2(u2h_(u.y));
-        const float2 a2 = __half22float2(u2h_(u.z)), a3 = __half22float2(u2h_(u.w));
-        const BmConst k =
-            bm_const<__half>(a, grad, img.w, img.h, min(x, img.w - 1), min(y + p, img.h - 1), in.x, in.y, in.z);
-        BmFastPix& q = P[p];
-        q.p0 = make_float4(a0.x, a0.y, a1.x, a1.y);
-        q.p1 = make_float4(a2.x, a2.y, a3.x, a3.y);
-        q.kl = fmaxf(-2.f * kLog2e * k.s * k.s, -1e30f);
-        q.klm2 = -2.f * q.kl;
-        q.base = fmaf(q.kl, in.w, 0.5f * log2f(lk));
-        const float sq = sqrtf(lk);
-        q.c1 = sq * k.c1;
-        q.c2 = sq * k.c2;
-        q.o1 = q.c1 * in.y;
-        q.o2 = q.c2 * in.z;
-    }
-    float acc[BX_NP][5] = {};
-    const int col = threadIdx.x, row0 = BX_NP * threadIdx.y;
-    auto rb = [&](int r) { return (row0 + r) * BX_W + col; };
-    bmx_row<0x1>(sm, rb(0), 0, P, acc);
-    bmx_row<0x3>(sm, rb(1), 1, P, acc);
-    bmx_row<0x7>(sm, rb(2), 2, P, acc);
-    for (int r = 3; r <= 20; r++) bmx_row<0xF>(sm, rb(r), r, P, acc);
-    bmx_row<0xE>(sm, rb(21), 21, P, acc);
-    bmx_row<0xC>(sm, rb(22), 22, P, acc);
-    bmx_row<0x8>(sm, rb(23), 23, P, acc);
-    if (x < out.w) {
-#pragma unroll
-        for (int p = 0; p < BX_NP; p++)
-            if (y + p < out.h)
-                st4<__half>(out.px(x, y + p),
-                            f4{acc[p][0] / acc[p][3], acc[p][1] / acc[p][4], acc[p][2] / acc[p][4], acc[p][3]});
-    }
-}
-
 // ---------------------------------------------------------------- FFMA2 form
-// The same FP16-path arithmetic with the four pixels of a thread taken as
-// two pairs, (p0, p1) and (p2, p3), and every per-pixel FP32 operation of a
-// pair issued as one packed FP32x2 instruction (fma/mul/add .rn.f32x2,
-// sm_100a). The neighbour's values enter as broadcast pairs. A pair's
+// The four pixels of a thread are taken as two pairs, (p0, p1) and
+// (p2, p3), and every per-pixel FP32 operation of a pair is issued as one
+// packed FP32x2 instruction (fma/mul/add .rn.f32x2, sm_100a). The neighbour's values enter as broadcast pairs. A pair's
 // spatial weights come from one float4 of a 22 x 21 table indexed by the
 // pair's first window row (rows outside a pixel's window carry weight 0 and
 // log-weight -inf, which zero both of its weights).

@@ -233,6 +233,103 @@ gls_status gls_calibration_fill(int32_t camera, int32_t iso, gls_demosaic_params
  * most max_taps taps; *n_taps receives the count. */
 gls_status gls_gaussian_bilinear_taps(float radius, float* taps, int32_t max_taps, int32_t* n_taps);
 
+/* ==== Registration and fusion (ImageRegistration/, PyramidFusion/) ==== */
+
+/* KeyPoint (ImageRegistration/feature2d.hpp:25-47), 28 bytes. angle is in
+ * radians, as the reference stores it; size == -1 marks a keypoint whose
+ * orientation could not be sampled (SURF.cpp:529-554). */
+typedef struct gls_keypoint {
+    float x, y, size, angle, response;
+    int32_t octave, class_id;
+} gls_keypoint;
+
+/* DMatch (ImageRegistration/SURF.hpp:29-42) */
+typedef struct gls_match {
+    int32_t query_idx, train_idx;
+    float distance;
+} gls_match;
+
+typedef struct gls_surf gls_surf;
+
+/* Feature slots a detector holds (detectAndCompute results kept on the
+ * device for matching). */
+#define GLS_SURF_SLOTS 8
+/* Most keypoints one detection keeps before the max_features cut
+ * (KeyPointMaxima::MaxCount, SURF.cpp:870-874). */
+#define GLS_SURF_MAX_KEYPOINTS 64000
+
+/* SURF::makeInstance (SURF.hpp:45-47, SURF.cpp:1082-1112): a detector for
+ * width x height single-channel F32 images on a CUDA device. max_features
+ * < 0 keeps every keypoint. The reference's defaults are 4 octaves, 2
+ * layers per octave, threshold 0.02. */
+gls_status gls_surf_create(int32_t device, int32_t width, int32_t height, int32_t max_features, int32_t n_octaves,
+                           int32_t n_octave_layers, float hessian_threshold, gls_surf** out);
+gls_status gls_surf_destroy(gls_surf* s);
+
+/* SURF::detectAndCompute (SURF.hpp:57-58, SURF.cpp:1380-1450, one
+ * section): integral image, fast-Hessian detector, KeypointGreater order,
+ * max_features cut, orientation and 64-D descriptor, into feature slot
+ * `slot`. img: F32, 1 channel, width x height, device memory or host
+ * memory with GLS_HOST_IO. Asynchronous on `stream` unless GLS_SYNC or
+ * GLS_HOST_IO. */
+gls_status gls_surf_detect_and_compute(gls_surf* s, const gls_image_view* img, int32_t slot, uint32_t flags,
+                                       void* stream);
+
+/* Copies a slot's keypoints, and its descriptors ([n][64] floats) when desc
+ * is not NULL, to host memory; synchronises the stream. *n receives the
+ * keypoint count; at most `capacity` are written. */
+gls_status gls_surf_features(gls_surf* s, int32_t slot, gls_keypoint* kps, float* desc, int32_t capacity, int32_t* n,
+                             void* stream);
+
+/* SURF::matchKeyPoints (SURF.cpp:931-974, SURF.metal:423-487): for every
+ * keypoint of query_slot its nearest descriptor in train_slot, sorted by
+ * distance then query index (refineMatch). The result stays in the
+ * detector for gls_surf_find_homography; with matches != NULL it is also
+ * copied to host memory (synchronising) and *n receives the count. */
+gls_status gls_surf_match(gls_surf* s, int32_t query_slot, int32_t train_slot, gls_match* matches, int32_t capacity,
+                          int32_t* n, void* stream);
+
+/* FindHomography (Homography.cpp:72-116) over the last match result, as
+ * SURF::findMatches pairs it (query point -> train point): RANSAC with
+ * max_iterations 4-point least-squares models (samples from std::mt19937
+ * with its default seed, uniform integers by mask-and-reject), inliers at
+ * squared error < threshold refitted by FindLeastSquaresHomography. Runs
+ * on the GPU; H (row-major, 9 floats) and the inlier indices are copied to
+ * host memory (synchronising). *n_inliers receives the count; inliers may
+ * be NULL. */
+gls_status gls_surf_find_homography(gls_surf* s, float threshold, int32_t max_iterations, float* H,
+                                    int32_t* inliers, int32_t* n_inliers, void* stream);
+
+/* The same for n host point pairs (x1, y1, x2, y2), with the detector as
+ * the device context. */
+gls_status gls_find_homography(gls_surf* ctx, const float* pairs, int32_t n, float threshold, int32_t max_iterations,
+                               float* H, int32_t* inliers, int32_t* n_inliers, void* stream);
+
+/* ScaleHomography (Homography.hpp:29-37): S H S^-1 with S = diag(2, 2, 1);
+ * like the reference, the scale argument does not enter. */
+gls_status gls_scale_homography(const float* H, float scale, float* out);
+
+/* RawChannels (PyramidFusion/pyramidFusion.cpp:106-143): the Bayer
+ * channels selected by channel_mask (bit c: 0 = R, 1 = G, 2 = B, 3 = G2 by
+ * the host table demosaic.hpp:128-133) at half resolution, through
+ * toneCurve(clamp(exposure (v - black) / white, 0, 1), 3.5), as F32 planes
+ * out[c] (device memory, (width/2) x (height/2)). raw is device memory, or
+ * host memory with GLS_HOST_IO. */
+gls_status gls_raw_channels(gls_surf* ctx, const uint16_t* raw, int32_t width, int32_t height, size_t stride_bytes,
+                            int32_t bayer_pattern, float black_level, float white_level, float exposure_multiplier,
+                            uint32_t channel_mask, gls_image_view* out, uint32_t flags, void* stream);
+
+/* registerAndFuse (SURF.metal:489-516, RegisterAndFuseKernel
+ * demosaic_kernels.hpp:690-710): out = ((count - 1) fused + input(H p)) /
+ * count per pixel, input sampled bilinearly with clamp-to-edge at H (x, y).
+ * fused / out: F32 RGBA (out may alias fused); input: F32 or F16 RGBA of
+ * any size; H: host, row-major. */
+gls_status gls_register_and_fuse(const gls_image_view* fused, const gls_image_view* input, gls_image_view* out,
+                                 const float* H, int32_t count, void* stream);
+
+/* registerImage (SURF.metal:518-538): out = input(H p). */
+gls_status gls_register_image(const gls_image_view* input, gls_image_view* out, const float* H, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
