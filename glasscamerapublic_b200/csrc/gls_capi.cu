@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "gls_common.cuh"
+#include "gls_devbuf.h"
 #include "gls_host.h"
 #include "gls_kernels.h"
 
@@ -27,43 +28,6 @@ gls_status set_error(gls_status code, const char* fmt, ...) {
     return code;
 }
 void clear_error() { g_last_error.clear(); }
-
-#define GLS_CUDA(...)                                                                                   \
-    do {                                                                                                \
-        cudaError_t e_ = (__VA_ARGS__);                                                                     \
-        if (e_ != cudaSuccess)                                                                          \
-            return set_error(e_ == cudaErrorMemoryAllocation ? GLS_ERR_OOM : GLS_ERR_CUDA, "%s: %s (%s:%d)", \
-                             #__VA_ARGS__, cudaGetErrorString(e_), __FILE__, __LINE__);                        \
-    } while (0)
-
-#define GLS_TRY(...)                     \
-    do {                                 \
-        gls_status s_ = (__VA_ARGS__);   \
-        if (s_ != GLS_OK) return s_;     \
-    } while (0)
-
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-    gls_status ensure(size_t b) {
-        if (b <= bytes) return GLS_OK;
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-        cudaError_t e = cudaMalloc(&p, b);
-        if (e != cudaSuccess) {
-            p = nullptr;
-            return set_error(GLS_ERR_OOM, "cudaMalloc(%zu) failed: %s", b, cudaGetErrorString(e));
-        }
-        bytes = b;
-        return GLS_OK;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-    }
-};
 
 template <class S, int C>
 static Plane<S, C> plane(DevBuf& b, int w, int h) {

@@ -142,6 +142,8 @@ class Workload:
 WORKLOADS = {
     "cfg1_1024x768": Workload("cfg1_1024x768", 1024, 768, levels=4, gain=0.8, read=3.0, iso=200, seed=1000),
     "cfg2_4032x3024": Workload("cfg2_4032x3024", 4032, 3024, levels=5, gain=2.0, read=5.0, iso=1600, seed=2000),
+    "cfg3_burst_4032x3024": Workload("cfg3_burst_4032x3024", 4032, 3024, levels=5, gain=1.5, read=4.0, iso=800,
+                                     seed=3000, extra={"frames": 8}),
 }
 
 MIXED_SIZES = [(4032, 3024), (6000, 4000), (5472, 3648), (8368, 5584)]
@@ -195,6 +197,95 @@ def make_raw(wl: Workload, frame: int = 0):
     clean = clean_scene(wl.width, wl.height, seed)
     raw = add_noise(mosaic(clean, wl.pattern), wl.black, wl.white, wl.gain, wl.read, seed)
     return raw, clean
+
+
+def burst_homographies(n: int, w: int, h: int, seed: int, max_rot_deg: float = 1.0, max_shift: float = 20.0,
+                       max_persp: float = 1e-5) -> list:
+    """Frame i's homography H_i (3x3 float64) mapping reference-frame pixels
+    to frame-i pixels, p_i ~ H_i p_ref; frame 0 is the reference (identity).
+    Rotation about the image centre within +-max_rot_deg, shift within
+    +-max_shift px, perspective terms within +-max_persp."""
+    rng = np.random.Generator(np.random.PCG64(seed ^ 0xB0B))
+    out = [np.eye(3)]
+    cx, cy = (w - 1) / 2.0, (h - 1) / 2.0
+    for _ in range(1, n):
+        a = np.deg2rad(rng.uniform(-max_rot_deg, max_rot_deg))
+        tx, ty = rng.uniform(-max_shift, max_shift, size=2)
+        px, py = rng.uniform(-max_persp, max_persp, size=2)
+        c, s_ = np.cos(a), np.sin(a)
+        T0 = np.array([[1, 0, -cx], [0, 1, -cy], [0, 0, 1.0]])
+        R = np.array([[c, -s_, 0], [s_, c, 0], [0, 0, 1.0]])
+        T1 = np.array([[1, 0, cx + tx], [0, 1, cy + ty], [0, 0, 1.0]])
+        P = np.array([[1, 0, 0], [0, 1, 0], [px, py, 1.0]])
+        H = T1 @ R @ T0 @ P
+        out.append(H / H[2, 2])
+    return out
+
+
+def warp_rgb(img: np.ndarray, H_ref_to_frame: np.ndarray) -> np.ndarray:
+    """Frame = reference image seen through H: frame(x) = ref(H^-1 x),
+    bilinear, clamp-to-edge."""
+    h, w = img.shape[:2]
+    Hi = np.linalg.inv(H_ref_to_frame)
+    ys, xs = np.mgrid[0:h, 0:w].astype(np.float64)
+    den = Hi[2, 0] * xs + Hi[2, 1] * ys + Hi[2, 2]
+    u = np.clip((Hi[0, 0] * xs + Hi[0, 1] * ys + Hi[0, 2]) / den, 0, w - 1)
+    v = np.clip((Hi[1, 0] * xs + Hi[1, 1] * ys + Hi[1, 2]) / den, 0, h - 1)
+    x0 = np.minimum(np.floor(u).astype(np.int64), w - 2)
+    y0 = np.minimum(np.floor(v).astype(np.int64), h - 2)
+    fx = (u - x0)[..., None]
+    fy = (v - y0)[..., None]
+    a = img[y0, x0] * (1 - fx) + img[y0, x0 + 1] * fx
+    b = img[y0 + 1, x0] * (1 - fx) + img[y0 + 1, x0 + 1] * fx
+    return (a * (1 - fy) + b * fy).astype(np.float32)
+
+
+def textured_scene(w: int, h: int, seed: int, blobs_per_mpx: float = 400.0) -> np.ndarray:
+    """clean_scene plus small square and round blobs (2 to 24 px across,
+    about blobs_per_mpx per megapixel): the local structure a feature
+    detector registers on."""
+    img = clean_scene(w, h, seed).astype(np.float64)
+    rng = np.random.Generator(np.random.PCG64(seed ^ 0xB10B))
+    n = int(blobs_per_mpx * w * h / 1e6)
+    mean = img.mean()
+    for _ in range(n):
+        r = rng.uniform(1.0, 12.0)
+        cx, cy = rng.uniform(0, w), rng.uniform(0, h)
+        x0, x1 = int(max(cx - r, 0)), int(min(cx + r + 1, w))
+        y0, y1 = int(max(cy - r, 0)), int(min(cy + r + 1, h))
+        if x1 <= x0 or y1 <= y0:
+            continue
+        col = rng.uniform(0.2, 3.0, size=3) * mean
+        if rng.uniform() < 0.5:
+            yy, xx = np.mgrid[y0:y1, x0:x1]
+            m = (xx - cx) ** 2 + (yy - cy) ** 2 <= r * r
+            img[y0:y1, x0:x1][m] = col
+        else:
+            img[y0:y1, x0:x1] = col
+    return np.clip(img, 0.0, 1.0).astype(np.float32)
+
+
+def make_burst(wl: Workload, n: int | None = None):
+    """A burst of n raw frames of one textured scene, frame i warped by H_i
+    (burst_homographies): (raws, cleans, homographies)."""
+    n = n or int(wl.extra.get("frames", 8))
+    ref = textured_scene(wl.width, wl.height, wl.seed)
+    Hs = burst_homographies(n, wl.width, wl.height, wl.seed)
+    raws, cleans = [], []
+    for i, H in enumerate(Hs):
+        c = ref if i == 0 else warp_rgb(ref, H)
+        cleans.append(c)
+        raws.append(add_noise(mosaic(c, wl.pattern), wl.black, wl.white, wl.gain, wl.read, wl.seed + i))
+    return raws, cleans, Hs
+
+
+def corner_error(H_est, H_true, w: int, h: int) -> float:
+    """Largest distance (px) between the image corners mapped by the two
+    homographies."""
+    pts = np.array([[0, 0, 1], [w - 1, 0, 1], [0, h - 1, 1], [w - 1, h - 1, 1]], np.float64).T
+    a = np.asarray(H_est, np.float64) @ pts
+    b = np.asarray(H_true, np.float64) @ pts
+    return float(np.max(np.hypot(a[0] / a[2] - b[0] / b[2], a[1] / a[2] - b[1] / b[2])))
 
 
 def target_rgb(clean: np.ndarray) -> np.ndarray:

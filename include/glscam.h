@@ -281,6 +281,12 @@ gls_status gls_surf_detect_and_compute(gls_surf* s, const gls_image_view* img, i
 gls_status gls_surf_features(gls_surf* s, int32_t slot, gls_keypoint* kps, float* desc, int32_t capacity, int32_t* n,
                              void* stream);
 
+/* Device view of a detector plane: GLS_SURF_PLANE_INTEGRAL is the summed-area
+ * table of the last detection, (width+1) x (height+1) F32 with a zero first
+ * row and column (integralImageKernel, SURF.cpp:776-825). */
+enum { GLS_SURF_PLANE_INTEGRAL = 0 };
+gls_status gls_surf_plane(gls_surf* s, int32_t which, gls_image_view* view);
+
 /* SURF::matchKeyPoints (SURF.cpp:931-974, SURF.metal:423-487): for every
  * keypoint of query_slot its nearest descriptor in train_slot, sorted by
  * distance then query index (refineMatch). The result stays in the
