@@ -14,10 +14,10 @@
 //            and the Taylor series of atan through u^13 (truncation
 //            < 2e-10 on |u| <= 0.268); quadrant and sign restored per
 //            C99 Annex F (signed zeros, infinities, NaN);
-//      sin/cos: Cody-Waite reduction by pi/2 (two-part constant), then the
-//            Taylor series through r^9 (sin) and r^10 (cos) on |r| <= pi/4.
-//    Accuracy is within a few float ulps of the correctly rounded values
-//    (tests compare them with a double-precision evaluation).
+//      sin/cos: reduction by pi/2 in double, then the Taylor series through
+//            r^9 (sin) and r^10 (cos) on |r| <= pi/4.
+//    Accuracy: atan2f within 3 float ulps, sinf/cosf within 2 ulps (tests
+//    compare them with a double-precision evaluation).
 #pragma once
 
 #include <cmath>
@@ -124,13 +124,13 @@ GLS_HD float cos_core(float r) {
     return fadd(1.0f, fmul(z, p));
 }
 
-// quadrant reduction: x = k pi/2 + r
+// quadrant reduction: x = k pi/2 + r, with r formed in double (the
+// product k pi/2 and the difference are exact to ~1e-16 for |x| < 2^20)
 GLS_HD int reduce_pi_2(float x, float* r) {
-    constexpr float kInvPi_2 = 0.63661977236758134308f;
-    constexpr float kPi_2Hi = 1.5707963705062866211f;    // float(pi/2)
-    constexpr float kPi_2Lo = -4.3711388286737929e-08f;  // pi/2 - kPi_2Hi
-    const float k = std::rint(fmul(x, kInvPi_2));
-    *r = fsub(fsub(x, fmul(k, kPi_2Hi)), fmul(k, kPi_2Lo));
+    constexpr double kInvPi_2 = 0.63661977236758134308;
+    constexpr double kPi_2d = 1.57079632679489661923;
+    const double k = std::rint(dmul(double(x), kInvPi_2));
+    *r = float(dsub(double(x), dmul(k, kPi_2d)));
     return int(k) & 3;
 }
 
