@@ -152,6 +152,9 @@ _SIGNATURES = {
                                            C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_void_p]),
     "gls_find_homography": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int32, C.c_float, C.c_int32,
                                       C.POINTER(C.c_float), C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_void_p]),
+    "gls_surf_register_frames": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32),
+                                           C.c_int32, C.c_float, C.c_int32, C.c_int32, C.POINTER(C.c_float),
+                                           C.c_void_p]),
     "gls_scale_homography": (C.c_int, [C.POINTER(C.c_float), C.c_float, C.POINTER(C.c_float)]),
     "gls_raw_channels": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_size_t, C.c_int32, C.c_float,
                                    C.c_float, C.c_float, C.c_uint32, C.POINTER(ImageView), C.c_uint32, C.c_void_p]),

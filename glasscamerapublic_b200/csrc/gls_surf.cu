@@ -18,8 +18,10 @@
 // determinant plane is ever written to HBM.
 #include <algorithm>
 #include <cfloat>
+#include <climits>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <random>
 #include <set>
@@ -573,15 +575,32 @@ __global__ void __launch_bounds__(kDescThreads) k_describe(DescArgs a) {
 }
 
 // ------------------------------------------------------------ matching
+// A batch of matching / homography jobs: each pairs a query slot (the
+// reference frame's features) with a train slot; blockIdx.y is the job.
+constexpr int kMaxJobs = 64;
+struct MatchJob {
+    const float* d1;
+    const int* n1;
+    const gls_keypoint* k1;
+    const float* d2;
+    const int* n2;
+    const gls_keypoint* k2;
+};
+struct MatchJobs {
+    MatchJob j[kMaxJobs];
+};
+
 // matchKeyPoints (SURF.metal:441-487): 24 lanes per query scan the train
 // descriptors j = lane, lane + 24, ...; the L2 norm accumulates in four
 // float lanes (SURF.metal:423-431). One warp per query.
-__global__ void __launch_bounds__(128) k_match(const float* __restrict__ d1, const int* __restrict__ n1p,
-                                               const float* __restrict__ d2, const int* __restrict__ n2p,
-                                               gls_match* __restrict__ out) {
+__global__ void __launch_bounds__(128) k_match(MatchJobs jobs, int cap, gls_match* __restrict__ out_all) {
+    const MatchJob& J = jobs.j[blockIdx.y];
+    gls_match* out = out_all + size_t(blockIdx.y) * cap;
+    const float* __restrict__ d1 = J.d1;
+    const float* __restrict__ d2 = J.d2;
     const int lane = threadIdx.x & 31;
     const int i = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
-    const int n1 = *n1p, n2 = *n2p;
+    const int n1 = *J.n1, n2 = *J.n2;
     if (i >= n1) return;
     const float* p1 = d1 + size_t(i) * 64;
     float dmin = FLT_MAX;
@@ -624,12 +643,16 @@ __global__ void __launch_bounds__(128) k_match(const float* __restrict__ d1, con
 // refineMatch order (SURF.cpp:917-929): distance, then query index; the
 // sorted matches become point pairs (query pt, train pt) as findMatches
 // builds them (SURF.hpp:65-75).
-__global__ void __launch_bounds__(256) k_match_rank(const gls_match* __restrict__ m, const int* __restrict__ n1p,
-                                                    const gls_keypoint* __restrict__ k1,
-                                                    const gls_keypoint* __restrict__ k2, gls_match* __restrict__ sorted,
-                                                    float4* __restrict__ pairs) {
+__global__ void __launch_bounds__(256) k_match_rank(MatchJobs jobs, int cap, const gls_match* __restrict__ m_all,
+                                                    gls_match* __restrict__ sorted_all, float4* __restrict__ pairs_all) {
     __shared__ gls_match tile[256];
-    const int n = *n1p;
+    const MatchJob& J = jobs.j[blockIdx.y];
+    const gls_match* __restrict__ m = m_all + size_t(blockIdx.y) * cap;
+    gls_match* __restrict__ sorted = sorted_all + size_t(blockIdx.y) * cap;
+    float4* __restrict__ pairs = pairs_all + size_t(blockIdx.y) * cap;
+    const gls_keypoint* __restrict__ k1 = J.k1;
+    const gls_keypoint* __restrict__ k2 = J.k2;
+    const int n = *J.n1;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (blockIdx.x * blockDim.x >= n) return;
     gls_match me{};
@@ -655,174 +678,241 @@ __global__ void __launch_bounds__(256) k_match_rank(const gls_match* __restrict_
 
 // ------------------------------------------------------------ homography
 // FindLeastSquaresHomography (LeastSquaresHomography.cpp:355-423) with the
-// Jacobi solver of :218-353; hypot(p, q) is sqrt(p^2 + q^2).
+// Jacobi solver of :218-353; hypot(p, q) is sqrt(p^2 + q^2). One warp
+// solves one system: the rotations of a Jacobi step update disjoint element
+// pairs, one pair per lane, so the warp produces the sequential loop's
+// results bit for bit.
 __device__ __forceinline__ double hypot_d(double a, double b) { return dsqrt(dadd(dmul(a, a), dmul(b, b))); }
 
-__device__ void jacobi9(double* a /*81, destroyed*/, double* W, double* V) {
+constexpr unsigned kFull = 0xffffffffu;
+
+struct LsWarp {  // shared scratch of one warp
+    double a[81], V[81], W[9], T[9];
+    double cen[4], mad[4];  // (cm0, cm1, cM0, cM1) and (sm0, sm1, sM0, sM1)
+    double nrm[4][4];       // the 4 sample points, normalised (a0, a1, b0, b1)
+    int indR[9], indC[9];
+};
+
+__device__ __forceinline__ void jac_rot(double& v0, double& v1, double c, double s) {
+    const double a0 = v0, b0 = v1;
+    v0 = dsub(dmul(a0, c), dmul(b0, s));
+    v1 = dadd(dmul(a0, s), dmul(b0, c));
+}
+
+// column m > k of the largest |a[k][m]| (the first on ties)
+__device__ __forceinline__ int max_in_row(const double* a, int k) {
+    int m = k + 1;
+    double mv = fabs(a[k * 9 + m]);
+    for (int i = k + 2; i < 9; i++) {
+        const double val = fabs(a[k * 9 + i]);
+        if (mv < val) mv = val, m = i;
+    }
+    return m;
+}
+
+// row m < k of the largest |a[m][k]| (the first on ties)
+__device__ __forceinline__ int max_in_col(const double* a, int k) {
+    int m = 0;
+    double mv = fabs(a[k]);
+    for (int i = 1; i < k; i++) {
+        const double val = fabs(a[i * 9 + k]);
+        if (mv < val) mv = val, m = i;
+    }
+    return m;
+}
+
+// Jacobi eigen-solve of the symmetric S.a (destroyed): eigenvalues S.W
+// sorted descending, eigenvectors as the rows of S.V. Called by a whole warp.
+__device__ void jacobi9_warp(LsWarp& S) {
     constexpr int N = 9;
-    const double eps = DBL_EPSILON;
-    for (int i = 0; i < N * N; i++) V[i] = 0.0;
-    for (int i = 0; i < N; i++) V[i * N + i] = 1.0;
-    int indR[N], indC[N];
-    auto upd = [&](int k) {
-        if (k < N - 1) {
-            int m = k + 1;
-            double mv = fabs(a[k * N + m]);
-            for (int i = k + 2; i < N; i++) {
-                const double val = fabs(a[k * N + i]);
-                if (mv < val) mv = val, m = i;
-            }
-            indR[k] = m;
-        }
-        if (k > 0) {
-            int m = 0;
-            double mv = fabs(a[k]);
-            for (int i = 1; i < k; i++) {
-                const double val = fabs(a[i * N + k]);
-                if (mv < val) mv = val, m = i;
-            }
-            indC[k] = m;
-        }
-    };
-    indR[N - 1] = 0;
-    indC[0] = 0;
-    for (int k = 0; k < N; k++) {
-        W[k] = a[k * N + k];
-        upd(k);
+    const int lane = threadIdx.x & 31;
+    double* a = S.a;
+    if (lane < N) {
+        for (int i = 0; i < N; i++) S.V[lane * N + i] = i == lane ? 1.0 : 0.0;
+        S.W[lane] = a[lane * N + lane];
+        if (lane < N - 1) S.indR[lane] = max_in_row(a, lane);
+        if (lane > 0) S.indC[lane] = max_in_col(a, lane);
     }
-    auto rot = [](double& v0, double& v1, double c, double s) {
-        const double a0 = v0, b0 = v1;
-        v0 = dsub(dmul(a0, c), dmul(b0, s));
-        v1 = dadd(dmul(a0, s), dmul(b0, c));
-    };
+    __syncwarp();
     for (int it = 0; it < N * N * 30; it++) {
-        int k = 0;
-        double mv = fabs(a[indR[0]]);
-        for (int i = 1; i < N - 1; i++) {
-            const double val = fabs(a[i * N + indR[i]]);
-            if (mv < val) mv = val, k = i;
+        int k = 0, l = 0, stop = 0;
+        double c = 0.0, s = 0.0;
+        if (lane == 0) {
+            double mv = fabs(a[S.indR[0]]);
+            for (int i = 1; i < N - 1; i++) {
+                const double val = fabs(a[i * N + S.indR[i]]);
+                if (mv < val) mv = val, k = i;
+            }
+            l = S.indR[k];
+            for (int i = 1; i < N; i++) {
+                const double val = fabs(a[S.indC[i] * N + i]);
+                if (mv < val) mv = val, k = S.indC[i], l = i;
+            }
+            const double p = a[k * N + l];
+            if (fabs(p) <= DBL_EPSILON) {
+                stop = 1;
+            } else {
+                const double y = dmul(dsub(S.W[l], S.W[k]), 0.5);
+                double t = dadd(fabs(y), hypot_d(p, y));
+                s = hypot_d(p, t);
+                c = ddiv(t, s);
+                s = ddiv(p, s);
+                t = dmul(ddiv(p, t), p);
+                if (y < 0) {
+                    s = -s;
+                    t = -t;
+                }
+                a[k * N + l] = 0.0;
+                S.W[k] = dsub(S.W[k], t);
+                S.W[l] = dadd(S.W[l], t);
+            }
         }
-        int l = indR[k];
-        for (int i = 1; i < N; i++) {
-            const double val = fabs(a[indC[i] * N + i]);
-            if (mv < val) mv = val, k = indC[i], l = i;
+        stop = __shfl_sync(kFull, stop, 0);
+        if (stop) break;
+        k = __shfl_sync(kFull, k, 0);
+        l = __shfl_sync(kFull, l, 0);
+        c = __shfl_sync(kFull, c, 0);
+        s = __shfl_sync(kFull, s, 0);
+        __syncwarp();
+        if (lane < N) {  // k < l always: indR points right, indC points up
+            if (lane != k && lane != l) {
+                if (lane < k) jac_rot(a[lane * N + k], a[lane * N + l], c, s);
+                else if (lane < l) jac_rot(a[k * N + lane], a[lane * N + l], c, s);
+                else jac_rot(a[k * N + lane], a[l * N + lane], c, s);
+            }
+            jac_rot(S.V[k * N + lane], S.V[l * N + lane], c, s);
         }
-        const double p = a[k * N + l];
-        if (fabs(p) <= eps) break;
-        const double y = dmul(dsub(W[l], W[k]), 0.5);
-        double t = dadd(fabs(y), hypot_d(p, y));
-        double s = hypot_d(p, t);
-        const double c = ddiv(t, s);
-        s = ddiv(p, s);
-        t = dmul(ddiv(p, t), p);
-        if (y < 0) {
-            s = -s;
-            t = -t;
+        __syncwarp();
+        if (lane < 2) {
+            const int idx = lane == 0 ? k : l;
+            if (idx < N - 1) S.indR[idx] = max_in_row(a, idx);
+            if (idx > 0) S.indC[idx] = max_in_col(a, idx);
         }
-        a[k * N + l] = 0.0;
-        W[k] = dsub(W[k], t);
-        W[l] = dadd(W[l], t);
-        for (int i = 0; i < k; i++) rot(a[i * N + k], a[i * N + l], c, s);
-        for (int i = k + 1; i < l; i++) rot(a[k * N + i], a[i * N + l], c, s);
-        for (int i = l + 1; i < N; i++) rot(a[k * N + i], a[l * N + i], c, s);
-        for (int i = 0; i < N; i++) rot(V[k * N + i], V[l * N + i], c, s);
-        upd(k);
-        upd(l);
+        __syncwarp();
     }
-    for (int k = 0; k < N - 1; k++) {
-        int m = k;
-        for (int i = k + 1; i < N; i++)
-            if (W[m] < W[i]) m = i;
-        if (k != m) {
-            double tw = W[m];
-            W[m] = W[k];
-            W[k] = tw;
-            for (int i = 0; i < N; i++) {
-                const double tv = V[m * N + i];
-                V[m * N + i] = V[k * N + i];
-                V[k * N + i] = tv;
+    if (lane == 0) {
+        for (int k = 0; k < N - 1; k++) {
+            int m = k;
+            for (int i = k + 1; i < N; i++)
+                if (S.W[m] < S.W[i]) m = i;
+            if (k != m) {
+                const double tw = S.W[m];
+                S.W[m] = S.W[k];
+                S.W[k] = tw;
+                for (int i = 0; i < N; i++) {
+                    const double tv = S.V[m * N + i];
+                    S.V[m * N + i] = S.V[k * N + i];
+                    S.V[k * N + i] = tv;
+                }
             }
         }
     }
+    __syncwarp();
 }
 
-// Normalised DLT tail: eigen-solve LtL (upper triangle filled), de-normalise,
-// scale to H[2][2] = 1.
-__device__ void ls_finish(double* L, const double cM[2], const double cm[2], const double sM[2], const double sm[2],
-                          float* H) {
-    for (int i = 0; i < 9; i++)
-        for (int j = 0; j < i; j++) L[i * 9 + j] = L[j * 9 + i];
-    double W[9], V[81];
-    jacobi9(L, W, V);
-    const double* h0 = &V[72];
-    const double inv[9] = {sm[0], 0, cm[0], 0, sm[1], cm[1], 0, 0, 1};
-    const double nrm[9] = {ddiv(1.0, sM[0]), 0, ddiv(-cM[0], sM[0]), 0, ddiv(1.0, sM[1]), ddiv(-cM[1], sM[1]),
-                           0, 0, 1};
-    double T[9], R[9];
-    for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 3; j++) {
-            double acc = 0.0;
-            for (int k = 0; k < 3; k++) acc = dadd(acc, dmul(inv[i * 3 + k], h0[k * 3 + j]));
-            T[i * 3 + j] = acc;
-        }
-    for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 3; j++) {
-            double acc = 0.0;
-            for (int k = 0; k < 3; k++) acc = dadd(acc, dmul(T[i * 3 + k], nrm[k * 3 + j]));
-            R[i * 3 + j] = acc;
-        }
-    const float d = __double2float_rn(R[8]);
-    for (int i = 0; i < 9; i++) H[i] = fdiv(__double2float_rn(R[i]), d);
+// entry j of the rows Lx, Ly of LeastSquaresHomography.cpp:396-397
+__device__ __forceinline__ double lx_entry(int j, double a0, double a1, double b0) {
+    switch (j) {
+        case 0: return a0;
+        case 1: return a1;
+        case 2: return 1.0;
+        case 6: return dmul(-b0, a0);
+        case 7: return dmul(-b0, a1);
+        case 8: return -b0;
+        default: return 0.0;
+    }
+}
+__device__ __forceinline__ double ly_entry(int j, double a0, double a1, double b1) {
+    switch (j) {
+        case 3: return a0;
+        case 4: return a1;
+        case 5: return 1.0;
+        case 6: return dmul(-b1, a0);
+        case 7: return dmul(-b1, a1);
+        case 8: return -b1;
+        default: return 0.0;
+    }
 }
 
-__device__ __forceinline__ void lrow(double a0, double a1, double b0, double b1, double* Lx, double* Ly) {
-    Lx[0] = a0, Lx[1] = a1, Lx[2] = 1, Lx[3] = 0, Lx[4] = 0, Lx[5] = 0;
-    Lx[6] = dmul(-b0, a0), Lx[7] = dmul(-b0, a1), Lx[8] = -b0;
-    Ly[0] = 0, Ly[1] = 0, Ly[2] = 0, Ly[3] = a0, Ly[4] = a1, Ly[5] = 1;
-    Ly[6] = dmul(-b1, a0), Ly[7] = dmul(-b1, a1), Ly[8] = -b1;
+// upper-triangle entry e (0..44) -> (j, k), j <= k
+__device__ __forceinline__ void tri_index(int e, int& j, int& k) {
+    j = 0;
+    while (e >= 9 - j) {
+        e -= 9 - j;
+        j++;
+    }
+    k = j + e;
 }
 
-// The 4-point model of one RANSAC sample (single thread); false where the
-// reference throws (a degenerate spread).
-__device__ bool ls4(const float4* P, const int* idx, float* H) {
-    double cM[2] = {0, 0}, cm[2] = {0, 0}, sM[2] = {0, 0}, sm[2] = {0, 0};
-    float4 p[4];
-    for (int i = 0; i < 4; i++) p[i] = P[idx[i]];
-    for (int i = 0; i < 4; i++) {
-        cm[0] = dadd(cm[0], double(p[i].z));
-        cm[1] = dadd(cm[1], double(p[i].w));
-        cM[0] = dadd(cM[0], double(p[i].x));
-        cM[1] = dadd(cM[1], double(p[i].y));
+// The tail of the normalised DLT on S.a (full symmetric LtL), S.cen and
+// S.mad: least eigenvector, de-normalisation, scale to H[2][2] = 1. Warp.
+__device__ void ls_finish_warp(LsWarp& S, float* H) {
+    const int lane = threadIdx.x & 31;
+    jacobi9_warp(S);
+    const double* h0 = &S.V[72];
+    const double cm0 = S.cen[0], cm1 = S.cen[1], cM0 = S.cen[2], cM1 = S.cen[3];
+    const double sm0 = S.mad[0], sm1 = S.mad[1], sM0 = S.mad[2], sM1 = S.mad[3];
+    if (lane < 9) {
+        const double inv[9] = {sm0, 0, cm0, 0, sm1, cm1, 0, 0, 1};
+        const int i = lane / 3, j = lane % 3;
+        double acc = 0.0;
+        for (int k = 0; k < 3; k++) acc = dadd(acc, dmul(inv[i * 3 + k], h0[k * 3 + j]));
+        S.T[lane] = acc;
     }
-    for (int c = 0; c < 2; c++) {
-        cm[c] = ddiv(cm[c], 4.0);
-        cM[c] = ddiv(cM[c], 4.0);
+    __syncwarp();
+    double r = 0.0;
+    if (lane < 9) {
+        const double nrm[9] = {ddiv(1.0, sM0), 0, ddiv(-cM0, sM0), 0, ddiv(1.0, sM1), ddiv(-cM1, sM1), 0, 0, 1};
+        const int i = lane / 3, j = lane % 3;
+        for (int k = 0; k < 3; k++) r = dadd(r, dmul(S.T[i * 3 + k], nrm[k * 3 + j]));
     }
-    for (int i = 0; i < 4; i++) {
-        sm[0] = dadd(sm[0], fabs(dsub(double(p[i].z), cm[0])));
-        sm[1] = dadd(sm[1], fabs(dsub(double(p[i].w), cm[1])));
-        sM[0] = dadd(sM[0], fabs(dsub(double(p[i].x), cM[0])));
-        sM[1] = dadd(sM[1], fabs(dsub(double(p[i].y), cM[1])));
+    const double r8 = __shfl_sync(kFull, r, 8);
+    if (lane < 9) H[lane] = fdiv(__double2float_rn(r), __double2float_rn(r8));
+    __syncwarp();
+}
+
+// The 4-point model of one RANSAC sample; false where the reference throws
+// (a degenerate spread). Warp.
+__device__ bool ls4_warp(LsWarp& S, const float4* __restrict__ P, const int* __restrict__ idx, float* H) {
+    const int lane = threadIdx.x & 31;
+    auto comp = [](const float4& p, int c) { return c == 0 ? p.z : c == 1 ? p.w : c == 2 ? p.x : p.y; };
+    if (lane < 4) {
+        double acc = 0.0;
+        for (int i = 0; i < 4; i++) acc = dadd(acc, double(comp(P[idx[i]], lane)));
+        S.cen[lane] = ddiv(acc, 4.0);
     }
-    for (int c = 0; c < 2; c++) {
-        sm[c] = ddiv(sm[c], 4.0);
-        sM[c] = ddiv(sM[c], 4.0);
+    __syncwarp();
+    if (lane < 4) {
+        double acc = 0.0;
+        for (int i = 0; i < 4; i++) acc = dadd(acc, fabs(dsub(double(comp(P[idx[i]], lane)), S.cen[lane])));
+        S.mad[lane] = ddiv(acc, 4.0);
     }
+    __syncwarp();
     const double eps = DBL_EPSILON;
-    if (fabs(sm[0]) < eps || fabs(sm[1]) < eps || fabs(sM[0]) < eps || fabs(sM[1]) < eps) return false;
-    double L[81];
-    for (int i = 0; i < 81; i++) L[i] = 0.0;
-    for (int i = 0; i < 4; i++) {
-        const double a0 = ddiv(dsub(double(p[i].x), cM[0]), sM[0]);
-        const double a1 = ddiv(dsub(double(p[i].y), cM[1]), sM[1]);
-        const double b0 = ddiv(dsub(double(p[i].z), cm[0]), sm[0]);
-        const double b1 = ddiv(dsub(double(p[i].w), cm[1]), sm[1]);
-        double Lx[9], Ly[9];
-        lrow(a0, a1, b0, b1, Lx, Ly);
-        for (int j = 0; j < 9; j++)
-            for (int k = j; k < 9; k++) L[j * 9 + k] = dadd(L[j * 9 + k], dadd(dmul(Lx[j], Lx[k]), dmul(Ly[j], Ly[k])));
+    if (fabs(S.mad[0]) < eps || fabs(S.mad[1]) < eps || fabs(S.mad[2]) < eps || fabs(S.mad[3]) < eps) return false;
+    if (lane < 4) {
+        const float4 p = P[idx[lane]];
+        S.nrm[lane][0] = ddiv(dsub(double(p.x), S.cen[2]), S.mad[2]);
+        S.nrm[lane][1] = ddiv(dsub(double(p.y), S.cen[3]), S.mad[3]);
+        S.nrm[lane][2] = ddiv(dsub(double(p.z), S.cen[0]), S.mad[0]);
+        S.nrm[lane][3] = ddiv(dsub(double(p.w), S.cen[1]), S.mad[1]);
     }
-    ls_finish(L, cM, cm, sM, sm, H);
+    __syncwarp();
+    for (int e = lane; e < 45; e += 32) {
+        int j, k;
+        tri_index(e, j, k);
+        double acc = 0.0;
+        for (int q = 0; q < 4; q++) {
+            const double* v = S.nrm[q];
+            const double xj = lx_entry(j, v[0], v[1], v[2]), xk = lx_entry(k, v[0], v[1], v[2]);
+            const double yj = ly_entry(j, v[0], v[1], v[3]), yk = ly_entry(k, v[0], v[1], v[3]);
+            acc = dadd(acc, dadd(dmul(xj, xk), dmul(yj, yk)));
+        }
+        S.a[j * 9 + k] = acc;
+        S.a[k * 9 + j] = acc;  // completeSymm
+    }
+    __syncwarp();
+    ls_finish_warp(S, H);
     return true;
 }
 
@@ -835,67 +925,106 @@ __device__ __forceinline__ float h_error(const float* H, float4 p) {
     return fadd(fmul(dx, dx), fmul(dy, dy));
 }
 
-// RANSAC hypotheses (RTL/RANSAC.hpp:47-66, 101-108): one block per
+// One RANSAC problem per job: its point pairs, their count and the sample
+// table drawn for that count.
+struct RansacJob {
+    const float4* pairs;
+    const int* samples;
+    int n;
+};
+struct RansacJobs {
+    RansacJob j[kMaxJobs];
+};
+
+// RANSAC hypotheses (RTL/RANSAC.hpp:47-66, 101-108): one warp per
 // iteration fits its sample and counts the errors above the threshold.
-__global__ void __launch_bounds__(128) k_ransac_models(const float4* __restrict__ pairs, int n,
-                                                       const int* __restrict__ samples, float threshold,
-                                                       float* __restrict__ models, int* __restrict__ losses) {
-    __shared__ float H[9];
-    __shared__ int cnt;
-    const int it = blockIdx.x;
-    if (threadIdx.x == 0) {
-        float h[9];
-        if (!ls4(pairs, samples + 4 * it, h)) {
-            for (int i = 0; i < 9; i++) h[i] = (i % 4 == 0) ? 1.0f : 0.0f;
-        }
-        for (int i = 0; i < 9; i++) H[i] = h[i];
-        cnt = 0;
+constexpr int kHypWarps = 4;
+__global__ void __launch_bounds__(32 * kHypWarps) k_ransac_models(RansacJobs jobs, int iters, float threshold,
+                                                                  float* __restrict__ models_all,
+                                                                  int* __restrict__ losses_all) {
+    __shared__ LsWarp S[kHypWarps];
+    __shared__ float Hs[kHypWarps][9];
+    const RansacJob& J = jobs.j[blockIdx.y];
+    const float4* __restrict__ pairs = J.pairs;
+    const int* __restrict__ samples = J.samples;
+    const int n = J.n;
+    float* __restrict__ models = models_all + size_t(blockIdx.y) * iters * 9;
+    int* __restrict__ losses = losses_all + size_t(blockIdx.y) * iters;
+    const int w = threadIdx.x / 32, lane = threadIdx.x & 31;
+    const int it = blockIdx.x * kHypWarps + w;
+    if (it >= iters) return;  // warp-uniform
+    float* H = Hs[w];
+    if (!ls4_warp(S[w], pairs, samples + 4 * it, H)) {
+        if (lane < 9) H[lane] = (lane % 4 == 0) ? 1.0f : 0.0f;
+        __syncwarp();
     }
-    __syncthreads();
     int c = 0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) c += fabsf(h_error(H, pairs[i])) > threshold ? 1 : 0;
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(&cnt, c);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        losses[it] = cnt;
-        for (int i = 0; i < 9; i++) models[it * 9 + i] = H[i];
-    }
+    for (int i = lane; i < n; i += 32) c += fabsf(h_error(H, pairs[i])) > threshold ? 1 : 0;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
+    if (lane == 0) losses[it] = c;
+    if (lane < 9) models[it * 9 + lane] = H[lane];
 }
 
 // The first model with the least loss, its inliers (|error| < threshold,
 // in index order) and, with 4 or more, their least-squares refit
-// (Homography.cpp:90-113). One block.
+// (Homography.cpp:90-113). One block; the sequential sums read the inliers
+// staged in shared memory.
 constexpr int kFinalThreads = 256;
-__global__ void __launch_bounds__(kFinalThreads) k_ransac_final(const float4* __restrict__ pairs, int n,
-                                                                 const float* __restrict__ models,
-                                                                 const int* __restrict__ losses, int iters,
-                                                                 float threshold, int* __restrict__ inliers,
-                                                                 int* __restrict__ n_inliers, float* __restrict__ Hout,
-                                                                 float* __restrict__ loss_out) {
-    __shared__ int best_s;
-    __shared__ float H[9];
+constexpr int kStage = 512;
+__global__ void __launch_bounds__(kFinalThreads) k_ransac_final(RansacJobs jobs, int cap,
+                                                                 const float* __restrict__ models_all,
+                                                                 const int* __restrict__ losses_all, int iters,
+                                                                 float threshold, int* __restrict__ inliers_all,
+                                                                 int* __restrict__ n_inliers_all,
+                                                                 float* __restrict__ H_all,
+                                                                 float* __restrict__ loss_all) {
+    const int job = blockIdx.x;
+    const float4* __restrict__ pairs = jobs.j[job].pairs;
+    const int n = jobs.j[job].n;
+    const float* __restrict__ models = models_all + size_t(job) * iters * 9;
+    const int* __restrict__ losses = losses_all + size_t(job) * iters;
+    int* __restrict__ inliers = inliers_all + size_t(job) * cap;
+    int* __restrict__ n_inliers = n_inliers_all + job;
+    float* __restrict__ Hout = H_all + size_t(job) * 9;
+    float* __restrict__ loss_out = loss_all + job;
+    __shared__ int best_s, base_s;
+    __shared__ float H[9], Hf[9];
     __shared__ int wsum[kFinalThreads / 32];
-    __shared__ int base_s;
-    __shared__ double cM[2], cm[2], sM[2], sm[2];
+    __shared__ LsWarp S;
+    __shared__ float4 stage[kStage];
+    __shared__ double4 nstage[kStage];
     __shared__ double L[81];
-    __shared__ int degenerate;
+    __shared__ int red_loss[kFinalThreads / 32], red_idx[kFinalThreads / 32];
     const int t = threadIdx.x;
-    if (t == 0) {
-        int b = 0;
-        for (int i = 1; i < iters; i++)
-            if (losses[i] < losses[b]) b = i;
-        best_s = b;
-        base_s = 0;
+    {  // the first iteration with the least loss: (loss, index) minimum
+        int bl = INT_MAX, bi = INT_MAX;
+        for (int i = t; i < iters; i += kFinalThreads) {
+            const int v = losses[i];
+            if (v < bl) bl = v, bi = i;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const int ol = __shfl_xor_sync(kFull, bl, o), oi = __shfl_xor_sync(kFull, bi, o);
+            if (ol < bl || (ol == bl && oi < bi)) bl = ol, bi = oi;
+        }
+        if ((t & 31) == 0) {
+            red_loss[t >> 5] = bl;
+            red_idx[t >> 5] = bi;
+        }
+        __syncthreads();
+        if (t == 0) {
+            for (int w = 1; w < kFinalThreads / 32; w++)
+                if (red_loss[w] < bl || (red_loss[w] == bl && red_idx[w] < bi)) bl = red_loss[w], bi = red_idx[w];
+            best_s = bi;
+            base_s = 0;
+        }
     }
     __syncthreads();
     if (t < 9) H[t] = models[best_s * 9 + t];
     __syncthreads();
-    // ordered compaction of the inliers
-    for (int i0 = 0; i0 < n; i0 += kFinalThreads) {
+    for (int i0 = 0; i0 < n; i0 += kFinalThreads) {  // ordered compaction of the inliers
         const int i = i0 + t;
         const int f = (i < n && fabsf(h_error(H, pairs[i])) < threshold) ? 1 : 0;
-        const unsigned bal = __ballot_sync(0xffffffffu, f);
+        const unsigned bal = __ballot_sync(kFull, f);
         const int lane = t & 31, w = t >> 5;
         if (lane == 0) wsum[w] = __popc(bal);
         __syncthreads();
@@ -915,73 +1044,72 @@ __global__ void __launch_bounds__(kFinalThreads) k_ransac_final(const float4* __
         *n_inliers = m;
         *loss_out = float(losses[best_s]);
     }
-    float Hf[9];
+    auto comp = [](const float4& p, int c) { return c == 0 ? p.z : c == 1 ? p.w : c == 2 ? p.x : p.y; };
     bool refit = false;
     if (m >= 4) {
-        // centroids and mean absolute deviations, each a sequential sum
-        if (t < 4) {
+        // centroids, then mean absolute deviations: sequential sums over the
+        // inliers in index order
+        for (int pass = 0; pass < 2; pass++) {
             double acc = 0.0;
-            for (int r = 0; r < m; r++) {
-                const float4 p = pairs[inliers[r]];
-                const float v = t == 0 ? p.z : t == 1 ? p.w : t == 2 ? p.x : p.y;
-                acc = dadd(acc, double(v));
-            }
-            acc = ddiv(acc, double(m));
-            if (t < 2) cm[t] = acc;
-            else cM[t - 2] = acc;
-        }
-        __syncthreads();
-        if (t < 4) {
-            double acc = 0.0;
-            const double c = t < 2 ? cm[t] : cM[t - 2];
-            for (int r = 0; r < m; r++) {
-                const float4 p = pairs[inliers[r]];
-                const float v = t == 0 ? p.z : t == 1 ? p.w : t == 2 ? p.x : p.y;
-                acc = dadd(acc, fabs(dsub(double(v), c)));
-            }
-            acc = ddiv(acc, double(m));
-            if (t < 2) sm[t] = acc;
-            else sM[t - 2] = acc;
-        }
-        __syncthreads();
-        if (t == 0) {
-            const double eps = DBL_EPSILON;
-            degenerate = (fabs(sm[0]) < eps || fabs(sm[1]) < eps || fabs(sM[0]) < eps || fabs(sM[1]) < eps) ? 1 : 0;
-        }
-        __syncthreads();
-        if (!degenerate) {
-            if (t < 45) {  // upper-triangle entry (j, k), a sequential sum over the inliers
-                int j = 0, r = t;
-                while (r >= 9 - j) {
-                    r -= 9 - j;
-                    j++;
+            for (int c0 = 0; c0 < m; c0 += kStage) {
+                const int cnt = min(kStage, m - c0);
+                __syncthreads();
+                for (int i = t; i < cnt; i += kFinalThreads) stage[i] = pairs[inliers[c0 + i]];
+                __syncthreads();
+                if (t < 4) {
+                    if (pass == 0)
+                        for (int i = 0; i < cnt; i++) acc = dadd(acc, double(comp(stage[i], t)));
+                    else
+                        for (int i = 0; i < cnt; i++) acc = dadd(acc, fabs(dsub(double(comp(stage[i], t)), S.cen[t])));
                 }
-                const int k = j + r;
-                double acc = 0.0;
-                for (int q = 0; q < m; q++) {
-                    const float4 p = pairs[inliers[q]];
-                    const double a0 = ddiv(dsub(double(p.x), cM[0]), sM[0]);
-                    const double a1 = ddiv(dsub(double(p.y), cM[1]), sM[1]);
-                    const double b0 = ddiv(dsub(double(p.z), cm[0]), sm[0]);
-                    const double b1 = ddiv(dsub(double(p.w), cm[1]), sm[1]);
-                    double Lx[9], Ly[9];
-                    lrow(a0, a1, b0, b1, Lx, Ly);
-                    acc = dadd(acc, dadd(dmul(Lx[j], Lx[k]), dmul(Ly[j], Ly[k])));
-                }
-                L[j * 9 + k] = acc;
+            }
+            if (t < 4) {
+                if (pass == 0) S.cen[t] = ddiv(acc, double(m));
+                else S.mad[t] = ddiv(acc, double(m));
             }
             __syncthreads();
-            if (t == 0) {
-                double Ll[81], c0[2] = {cM[0], cM[1]}, c1[2] = {cm[0], cm[1]}, s0[2] = {sM[0], sM[1]},
-                                s1[2] = {sm[0], sm[1]};
-                for (int i = 0; i < 81; i++) Ll[i] = L[i];
-                ls_finish(Ll, c0, c1, s0, s1, Hf);
-                refit = true;
+        }
+        const double eps = DBL_EPSILON;
+        const bool degenerate =
+            fabs(S.mad[0]) < eps || fabs(S.mad[1]) < eps || fabs(S.mad[2]) < eps || fabs(S.mad[3]) < eps;
+        if (!degenerate) {
+            double acc = 0.0;
+            int j = 0, k = 0;
+            if (t < 45) tri_index(t, j, k);
+            for (int c0 = 0; c0 < m; c0 += kStage) {
+                const int cnt = min(kStage, m - c0);
+                __syncthreads();
+                for (int i = t; i < cnt; i += kFinalThreads) {
+                    const float4 p = pairs[inliers[c0 + i]];
+                    nstage[i] = make_double4(ddiv(dsub(double(p.x), S.cen[2]), S.mad[2]),
+                                             ddiv(dsub(double(p.y), S.cen[3]), S.mad[3]),
+                                             ddiv(dsub(double(p.z), S.cen[0]), S.mad[0]),
+                                             ddiv(dsub(double(p.w), S.cen[1]), S.mad[1]));
+                }
+                __syncthreads();
+                if (t < 45)
+                    for (int q = 0; q < cnt; q++) {
+                        const double4 v = nstage[q];
+                        const double xj = lx_entry(j, v.x, v.y, v.z), xk = lx_entry(k, v.x, v.y, v.z);
+                        const double yj = ly_entry(j, v.x, v.y, v.w), yk = ly_entry(k, v.x, v.y, v.w);
+                        acc = dadd(acc, dadd(dmul(xj, xk), dmul(yj, yk)));
+                    }
             }
+            if (t < 45) {
+                L[j * 9 + k] = acc;
+                L[k * 9 + j] = acc;  // completeSymm
+            }
+            __syncthreads();
+            if (t < 32) {
+                for (int i = t; i < 81; i += 32) S.a[i] = L[i];
+                __syncwarp();
+                ls_finish_warp(S, Hf);
+            }
+            refit = true;
+            __syncthreads();
         }
     }
-    if (t == 0)
-        for (int i = 0; i < 9; i++) Hout[i] = refit ? Hf[i] : H[i];
+    if (t < 9) Hout[t] = refit ? Hf[t] : H[t];
 }
 
 // ------------------------------------------------------------ raw channels
@@ -1193,10 +1321,11 @@ struct gls_surf {
     int capacity = 1500;  // keypoints kept per slot
     DevBuf img, sum, colT, cand, cand_count, tables;
     SurfSlotState slot[GLS_SURF_SLOTS];
-    DevBuf matches, matches_sorted, pairs, match_count;
-    int match_query = -1, match_train = -1, match_n = -1;
-    DevBuf samples, models, losses, inliers, n_inliers, Hdev, loss;
-    int samples_n = -1, samples_iters = -1;
+    DevBuf matches, matches_sorted, pairs;  // [jobs][pair_cap]
+    int pair_cap = 0;
+    int match_query = -1, match_train = -1;  // the slots of the last single match (job 0)
+    std::map<std::pair<int, int>, DevBuf> sample_tables;
+    DevBuf models, losses, inliers, n_inliers, Hdev, loss;
     DevBuf raw, lut;
     float lut_black = NAN, lut_white = NAN, lut_exp = NAN;
     std::vector<float> lut_host;
@@ -1288,33 +1417,55 @@ std::vector<int> ransac_samples(int iterations, int n) {
     return out;
 }
 
-gls_status run_ransac(gls_surf* s, int n, float threshold, int iters, float* H, int32_t* inliers, int32_t* n_inl,
-                      cudaStream_t st) {
-    if (n < 4) return set_error(GLS_ERR_DEGENERATE, "RANSAC needs at least 4 point pairs, got %d", n);
-    if (s->samples_n != n || s->samples_iters != iters) {
+// the RANSAC sample table for n pairs (cached per (n, iterations))
+gls_status sample_table(gls_surf* s, int n, int iters, const int** out, cudaStream_t st) {
+    auto key = std::make_pair(n, iters);
+    auto it = s->sample_tables.find(key);
+    if (it == s->sample_tables.end()) {
         const std::vector<int> smp = ransac_samples(iters, n);
-        GLS_TRY(s->samples.ensure(smp.size() * sizeof(int)));
-        GLS_CUDA(cudaMemcpyAsync(s->samples.p, smp.data(), smp.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        DevBuf b;
+        GLS_TRY(b.ensure(smp.size() * sizeof(int)));
+        GLS_CUDA(cudaMemcpyAsync(b.p, smp.data(), smp.size() * sizeof(int), cudaMemcpyHostToDevice, st));
         GLS_CUDA(cudaStreamSynchronize(st));
-        s->samples_n = n;
-        s->samples_iters = iters;
+        it = s->sample_tables.emplace(key, b).first;
     }
-    GLS_TRY(s->models.ensure(size_t(iters) * 9 * sizeof(float)));
-    GLS_TRY(s->losses.ensure(size_t(iters) * sizeof(int)));
-    GLS_TRY(s->inliers.ensure(size_t(n) * sizeof(int)));
-    GLS_TRY(s->n_inliers.ensure(sizeof(int)));
-    GLS_TRY(s->Hdev.ensure(9 * sizeof(float)));
-    GLS_TRY(s->loss.ensure(sizeof(float)));
-    const float4* pairs = reinterpret_cast<const float4*>(s->pairs.p);
-    k_ransac_models<<<iters, 128, 0, st>>>(pairs, n, reinterpret_cast<const int*>(s->samples.p), threshold,
-                                           reinterpret_cast<float*>(s->models.p), reinterpret_cast<int*>(s->losses.p));
+    *out = reinterpret_cast<const int*>(it->second.p);
+    return GLS_OK;
+}
+
+// RANSAC + refit for jobs 0..J-1 whose pairs are in s->pairs (cap per job)
+// and whose pair counts are ns[j]; leaves H [J][9], inliers, counts on the
+// device.
+gls_status run_ransac(gls_surf* s, const std::vector<int>& ns, float threshold, int iters, cudaStream_t st) {
+    const int J = int(ns.size());
+    const size_t cap = size_t(std::max(s->pair_cap, 1));
+    RansacJobs rj{};
+    for (int j = 0; j < J; j++) {
+        if (ns[j] < 4) return set_error(GLS_ERR_DEGENERATE, "RANSAC needs at least 4 point pairs, got %d", ns[j]);
+        rj.j[j].pairs = reinterpret_cast<const float4*>(s->pairs.p) + size_t(j) * cap;
+        rj.j[j].n = ns[j];
+        GLS_TRY(sample_table(s, ns[j], iters, &rj.j[j].samples, st));
+    }
+    GLS_TRY(s->models.ensure(size_t(J) * iters * 9 * sizeof(float)));
+    GLS_TRY(s->losses.ensure(size_t(J) * iters * sizeof(int)));
+    GLS_TRY(s->inliers.ensure(size_t(J) * cap * sizeof(int)));
+    GLS_TRY(s->n_inliers.ensure(size_t(J) * sizeof(int)));
+    GLS_TRY(s->Hdev.ensure(size_t(J) * 9 * sizeof(float)));
+    GLS_TRY(s->loss.ensure(size_t(J) * sizeof(float)));
+    k_ransac_models<<<dim3((iters + kHypWarps - 1) / kHypWarps, J), 32 * kHypWarps, 0, st>>>(
+        rj, iters, threshold, reinterpret_cast<float*>(s->models.p), reinterpret_cast<int*>(s->losses.p));
     GLS_TRY(launch_check(s, "k_ransac_models"));
-    k_ransac_final<<<1, kFinalThreads, 0, st>>>(pairs, n, reinterpret_cast<const float*>(s->models.p),
+    k_ransac_final<<<J, kFinalThreads, 0, st>>>(rj, int(cap), reinterpret_cast<const float*>(s->models.p),
                                                 reinterpret_cast<const int*>(s->losses.p), iters, threshold,
                                                 reinterpret_cast<int*>(s->inliers.p),
                                                 reinterpret_cast<int*>(s->n_inliers.p),
                                                 reinterpret_cast<float*>(s->Hdev.p), reinterpret_cast<float*>(s->loss.p));
     GLS_TRY(launch_check(s, "k_ransac_final"));
+    return GLS_OK;
+}
+
+// copies job 0's homography and inliers to the host (synchronising)
+gls_status ransac_result(gls_surf* s, float* H, int32_t* inliers, int32_t* n_inl, cudaStream_t st) {
     int ni = 0;
     GLS_CUDA(cudaMemcpyAsync(H, s->Hdev.p, 9 * sizeof(float), cudaMemcpyDeviceToHost, st));
     GLS_CUDA(cudaMemcpyAsync(&ni, s->n_inliers.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1322,6 +1473,39 @@ gls_status run_ransac(gls_surf* s, int n, float threshold, int iters, float* H, 
     if (n_inl) *n_inl = ni;
     if (inliers && ni > 0)
         GLS_CUDA(cudaMemcpy(inliers, s->inliers.p, size_t(ni) * sizeof(int), cudaMemcpyDeviceToHost));
+    return GLS_OK;
+}
+
+gls_status ensure_pairs(gls_surf* s, int jobs, int cap) {
+    s->pair_cap = std::max(s->pair_cap, cap);
+    const size_t c = size_t(std::max(s->pair_cap, 1));
+    GLS_TRY(s->matches.ensure(size_t(jobs) * c * sizeof(gls_match)));
+    GLS_TRY(s->matches_sorted.ensure(size_t(jobs) * c * sizeof(gls_match)));
+    GLS_TRY(s->pairs.ensure(size_t(jobs) * c * sizeof(float4)));
+    return GLS_OK;
+}
+
+// match jobs (query slot, train slot) into matches / pairs job by job
+gls_status run_match(gls_surf* s, const std::vector<std::pair<int, int>>& qt, cudaStream_t st) {
+    const int J = int(qt.size());
+    if (s->pair_cap != s->capacity) s->pair_cap = 0;
+    GLS_TRY(ensure_pairs(s, J, s->capacity));
+    MatchJobs mj{};
+    for (int j = 0; j < J; j++) {
+        const SurfSlotState &q = s->slot[qt[j].first], &t = s->slot[qt[j].second];
+        mj.j[j] = {reinterpret_cast<const float*>(q.desc.p), reinterpret_cast<const int*>(q.count.p),
+                   reinterpret_cast<const gls_keypoint*>(q.kps.p), reinterpret_cast<const float*>(t.desc.p),
+                   reinterpret_cast<const int*>(t.count.p), reinterpret_cast<const gls_keypoint*>(t.kps.p)};
+    }
+    const int cap = s->pair_cap;
+    const int warps = 4;
+    k_match<<<dim3((s->capacity + warps - 1) / warps, J), 32 * warps, 0, st>>>(
+        mj, cap, reinterpret_cast<gls_match*>(s->matches.p));
+    GLS_TRY(launch_check(s, "k_match"));
+    k_match_rank<<<dim3((s->capacity + 255) / 256, J), 256, 0, st>>>(
+        mj, cap, reinterpret_cast<const gls_match*>(s->matches.p), reinterpret_cast<gls_match*>(s->matches_sorted.p),
+        reinterpret_cast<float4*>(s->pairs.p));
+    GLS_TRY(launch_check(s, "k_match_rank"));
     return GLS_OK;
 }
 
@@ -1380,9 +1564,10 @@ gls_status gls_surf_destroy(gls_surf* s) {
     if (!s) return GLS_OK;
     cudaSetDevice(s->device);
     for (DevBuf* b : {&s->img, &s->sum, &s->colT, &s->cand, &s->cand_count, &s->tables, &s->matches,
-                      &s->matches_sorted, &s->pairs, &s->match_count, &s->samples, &s->models, &s->losses,
-                      &s->inliers, &s->n_inliers, &s->Hdev, &s->loss, &s->raw, &s->lut})
+                      &s->matches_sorted, &s->pairs, &s->models, &s->losses, &s->inliers, &s->n_inliers, &s->Hdev,
+                      &s->loss, &s->raw, &s->lut})
         b->release();
+    for (auto& kv : s->sample_tables) kv.second.release();
     for (auto& sl : s->slot) {
         sl.kps.release();
         sl.desc.release();
@@ -1525,22 +1710,7 @@ gls_status gls_surf_match(gls_surf* s, int32_t query_slot, int32_t train_slot, g
     if (!s->slot[query_slot].valid || !s->slot[train_slot].valid)
         return set_error(GLS_ERR_INVALID_ARG, "slot holds no detection");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    const size_t cap = size_t(std::max(s->capacity, 1));
-    GLS_TRY(s->matches.ensure(cap * sizeof(gls_match)));
-    GLS_TRY(s->matches_sorted.ensure(cap * sizeof(gls_match)));
-    GLS_TRY(s->pairs.ensure(cap * sizeof(float4)));
-    const SurfSlotState &q = s->slot[query_slot], &t = s->slot[train_slot];
-    const int warps = 4;
-    k_match<<<(s->capacity + warps - 1) / warps, 32 * warps, 0, st>>>(
-        reinterpret_cast<const float*>(q.desc.p), reinterpret_cast<const int*>(q.count.p),
-        reinterpret_cast<const float*>(t.desc.p), reinterpret_cast<const int*>(t.count.p),
-        reinterpret_cast<gls_match*>(s->matches.p));
-    GLS_TRY(launch_check(s, "k_match"));
-    k_match_rank<<<(s->capacity + 255) / 256, 256, 0, st>>>(
-        reinterpret_cast<const gls_match*>(s->matches.p), reinterpret_cast<const int*>(q.count.p),
-        reinterpret_cast<const gls_keypoint*>(q.kps.p), reinterpret_cast<const gls_keypoint*>(t.kps.p),
-        reinterpret_cast<gls_match*>(s->matches_sorted.p), reinterpret_cast<float4*>(s->pairs.p));
-    GLS_TRY(launch_check(s, "k_match_rank"));
+    GLS_TRY(run_match(s, {{query_slot, train_slot}}, st));
     s->match_query = query_slot;
     s->match_train = train_slot;
     if (matches || n) {
@@ -1566,7 +1736,8 @@ gls_status gls_surf_find_homography(gls_surf* s, float threshold, int32_t max_it
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     int n = 0;
     GLS_TRY(slot_count(s, s->match_query, st, &n));
-    return run_ransac(s, n, threshold, max_iterations, H, inliers, n_inliers, st);
+    GLS_TRY(run_ransac(s, {n}, threshold, max_iterations, st));
+    return ransac_result(s, H, inliers, n_inliers, st);
 }
 
 gls_status gls_find_homography(gls_surf* ctx, const float* pairs, int32_t n, float threshold, int32_t max_iterations,
@@ -1577,10 +1748,52 @@ gls_status gls_find_homography(gls_surf* ctx, const float* pairs, int32_t n, flo
     if (max_iterations < 1) return set_error(GLS_ERR_INVALID_ARG, "max_iterations must be positive");
     if (n < 4) return set_error(GLS_ERR_DEGENERATE, "RANSAC needs at least 4 point pairs, got %d", n);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    GLS_TRY(ctx->pairs.ensure(size_t(n) * sizeof(float4)));
+    GLS_TRY(ensure_pairs(ctx, 1, n));
     GLS_CUDA(cudaMemcpyAsync(ctx->pairs.p, pairs, size_t(n) * sizeof(float4), cudaMemcpyHostToDevice, st));
     ctx->match_query = ctx->match_train = -1;  // the pair buffer now holds host pairs
-    return run_ransac(ctx, n, threshold, max_iterations, H, inliers, n_inliers, st);
+    GLS_TRY(run_ransac(ctx, {n}, threshold, max_iterations, st));
+    return ransac_result(ctx, H, inliers, n_inliers, st);
+}
+
+gls_status gls_surf_register_frames(gls_surf* s, const int32_t* ref_slots, int32_t n_channels,
+                                    const int32_t* frame_slots, int32_t n_frames, float threshold,
+                                    int32_t max_iterations, int32_t scale_to_full, float* H, void* stream) {
+    clear_error();
+    GLS_TRY(check_surf(s));
+    if (!ref_slots || !frame_slots || !H) return set_error(GLS_ERR_INVALID_ARG, "NULL argument");
+    if (n_channels < 1 || n_frames < 1 || n_channels * n_frames > kMaxJobs)
+        return set_error(GLS_ERR_INVALID_ARG, "n_channels x n_frames must be 1..%d", kMaxJobs);
+    if (max_iterations < 1) return set_error(GLS_ERR_INVALID_ARG, "max_iterations must be positive");
+    auto ok = [&](int sl) { return sl >= 0 && sl < GLS_SURF_SLOTS && s->slot[sl].valid; };
+    for (int c = 0; c < n_channels; c++)
+        if (!ok(ref_slots[c])) return set_error(GLS_ERR_INVALID_ARG, "reference slot %d holds no detection", ref_slots[c]);
+    for (int i = 0; i < n_channels * n_frames; i++)
+        if (!ok(frame_slots[i])) return set_error(GLS_ERR_INVALID_ARG, "frame slot %d holds no detection", frame_slots[i]);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    std::vector<std::pair<int, int>> qt;
+    std::vector<int> ns;
+    for (int f = 0; f < n_frames; f++)
+        for (int c = 0; c < n_channels; c++) {
+            qt.push_back({ref_slots[c], frame_slots[f * n_channels + c]});
+            int n = 0;
+            GLS_TRY(slot_count(s, ref_slots[c], st, &n));
+            ns.push_back(n);
+        }
+    GLS_TRY(run_match(s, qt, st));
+    s->match_query = s->match_train = -1;
+    GLS_TRY(run_ransac(s, ns, threshold, max_iterations, st));
+    std::vector<float> Hj(qt.size() * 9);
+    GLS_CUDA(cudaMemcpyAsync(Hj.data(), s->Hdev.p, Hj.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+    GLS_CUDA(cudaStreamSynchronize(st));
+    for (int f = 0; f < n_frames; f++) {
+        float acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int c = 0; c < n_channels; c++)  // running average, pyramidFusion.cpp:338-339
+            for (int i = 0; i < 9; i++)
+                acc[i] = (Hj[size_t(f * n_channels + c) * 9 + i] + acc[i] * float(c)) / float(c + 1);
+        if (scale_to_full) GLS_TRY(gls_scale_homography(acc, 2.0f, acc));
+        std::memcpy(H + size_t(f) * 9, acc, sizeof(acc));
+    }
+    return GLS_OK;
 }
 
 gls_status gls_scale_homography(const float* H, float scale, float* out) {

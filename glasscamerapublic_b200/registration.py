@@ -16,7 +16,7 @@ import numpy as np
 from . import F16, F32, HOST_IO, KEYPOINT_DTYPE, MATCH_DTYPE, SYNC, ImageView, check, lib
 from .api import _is_torch, _ptr, _row_stride, _stream_handle
 
-SURF_SLOTS = 8
+SURF_SLOTS = 32
 
 
 def _view(a, channels: int) -> ImageView:
@@ -111,6 +111,21 @@ class SURF:
                                              inl.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(n),
                                              _stream_handle(stream)))
         return H.reshape(3, 3), inl[:n.value].copy()
+
+    def register_frames(self, ref_slots, frame_slots, threshold: float = 1.0, max_iterations: int = 2000,
+                        scale_to_full: bool = True, stream=None) -> np.ndarray:
+        """Batched burst registration: frame_slots[f][c] matched against
+        ref_slots[c]; per-frame homographies averaged over the channels
+        (and scaled to full resolution), [n_frames][3][3]."""
+        fs = np.ascontiguousarray(np.asarray(frame_slots, np.int32))
+        rs = np.ascontiguousarray(np.asarray(ref_slots, np.int32))
+        nf, nc = fs.shape
+        H = np.zeros((nf, 9), np.float32)
+        check(lib().gls_surf_register_frames(self._h, rs.ctypes.data_as(C.POINTER(C.c_int32)), nc,
+                                             fs.ctypes.data_as(C.POINTER(C.c_int32)), nf, float(threshold),
+                                             max_iterations, int(scale_to_full),
+                                             H.ctypes.data_as(C.POINTER(C.c_float)), _stream_handle(stream)))
+        return H.reshape(nf, 3, 3)
 
     def findMatches(self, query_slot: int, train_slot: int, stream=None):
         """SURF::findMatches (SURF.hpp:65-75) on two slots: (query pt,

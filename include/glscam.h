@@ -253,7 +253,7 @@ typedef struct gls_surf gls_surf;
 
 /* Feature slots a detector holds (detectAndCompute results kept on the
  * device for matching). */
-#define GLS_SURF_SLOTS 8
+#define GLS_SURF_SLOTS 32
 /* Most keypoints one detection keeps before the max_features cut
  * (KeyPointMaxima::MaxCount, SURF.cpp:870-874). */
 #define GLS_SURF_MAX_KEYPOINTS 64000
@@ -310,6 +310,19 @@ gls_status gls_surf_find_homography(gls_surf* s, float threshold, int32_t max_it
  * the device context. */
 gls_status gls_find_homography(gls_surf* ctx, const float* pairs, int32_t n, float threshold, int32_t max_iterations,
                                float* H, int32_t* inliers, int32_t* n_inliers, void* stream);
+
+/* Burst registration in one batch (the per-frame loop of
+ * pyramidFusion.cpp:318-346): for frame f and channel c, the features of
+ * slot frame_slots[f * n_channels + c] are matched against reference slot
+ * ref_slots[c] and FindHomography runs on the pairs; all n_frames x
+ * n_channels (at most 64) problems go to the GPU together. The channel
+ * homographies of a frame are averaged as the reference does
+ * (H = (H_c + H * c) / (c + 1)) and, with scale_to_full, mapped by
+ * ScaleHomography. H receives [n_frames][9] floats in host memory;
+ * synchronises the stream. */
+gls_status gls_surf_register_frames(gls_surf* s, const int32_t* ref_slots, int32_t n_channels,
+                                    const int32_t* frame_slots, int32_t n_frames, float threshold,
+                                    int32_t max_iterations, int32_t scale_to_full, float* H, void* stream);
 
 /* ScaleHomography (Homography.hpp:29-37): S H S^-1 with S = diag(2, 2, 1);
  * like the reference, the scale argument does not enter. */

@@ -222,3 +222,28 @@ def test_burst_registration_recovers_warps():
             assert err < 1.0, (i, err)
     finally:
         s.close()
+
+
+def test_register_frames_batch_equals_single_jobs():
+    # the batched burst registration gives the per-job results bit for bit
+    wl = scene.Workload("burst", 1024, 768, gain=1.5, read=4.0, iso=800, seed=3002)
+    raws, _, Hs = scene.make_burst(wl, 4)
+    s = SURF(512, 384, max_features=1500)
+    try:
+        planes = []
+        for f, r in enumerate(raws):
+            ch = s.raw_channels(r, 2, 512.0, 4095.0)
+            s.detect_slot(ch[1], 2 * f)
+            s.detect_slot(ch[3], 2 * f + 1)
+            planes.append(ch)
+        Hb = s.register_frames([0, 1], [[2 * f, 2 * f + 1] for f in range(1, 4)], 1.0, 2000, True)
+        for f in range(1, 4):
+            acc = np.zeros((3, 3), np.float32)
+            for c in range(2):
+                s.match_slots(c, 2 * f + c, host=False)
+                Hc, _ = s.find_homography_slots(1.0, 2000)
+                acc = (Hc + acc * np.float32(c)) / np.float32(c + 1)
+            assert np.array_equal(Hb[f - 1], ScaleHomography(acc, 2)), f
+            assert scene.corner_error(Hb[f - 1], Hs[f], 1024, 768) < 1.0
+    finally:
+        s.close()
