@@ -43,6 +43,9 @@ PLANE_DESPECKLED = 3
 PLANE_OUTPUT = 4
 PLANE_DENOISED_L0 = 8
 SURF_PLANE_INTEGRAL = 0
+ADJ_NPARAMS = 32
+ADJ_LUMA, ADJ_CHROMA, ADJ_NLF_AY, ADJ_NLF_BY, ADJ_NLF_AC, ADJ_NLF_BC = 0, 5, 10, 15, 20, 25
+ADJ_RAW_GREEN_A, ADJ_RAW_GREEN_B = 30, 31
 
 CAMERA_IPHONE14_WIDE = 0
 
@@ -139,6 +142,9 @@ _SIGNATURES = {
     "gls_converter_reset_stats": (C.c_int, [C.c_void_p]),
     "gls_calibration_fill": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(DemosaicParams)]),
     "gls_gaussian_bilinear_taps": (C.c_int, [C.c_float, C.POINTER(C.c_float), C.c_int32, C.POINTER(C.c_int32)]),
+    "gls_demosaic_denoise_vjp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_size_t,
+                                           C.POINTER(DemosaicParams), C.POINTER(ImageView), C.c_uint32,
+                                           C.POINTER(C.c_double), C.POINTER(C.c_float), C.c_void_p]),
     "gls_surf_create": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_float,
                                   C.POINTER(C.c_void_p)]),
     "gls_surf_destroy": (C.c_int, [C.c_void_p]),

@@ -177,6 +177,8 @@ struct gls_converter {
     int last_levels = 0;
     int last_w = 0, last_h = 0;
     bool last_denoise = false;
+    // adjoint scratch (gls_demosaic_denoise_vjp)
+    DevBuf adj_gden[2], adj_rec, adj_glayer, adj_gpca, adj_gup, adj_part, adj_loss, adj_target;
 };
 
 namespace gls {
@@ -531,6 +533,143 @@ static gls_status pyramid_only(gls_converter* cv, const gls_image_view* ycc, con
 }  // namespace gls
 
 // ============================================================== C ABI
+namespace gls {
+
+// The reverse sweep over the FP32 pipeline's retained planes (slot 0): the
+// loss head, then per level fine to coarse block matching transposed and,
+// below the coarsest level, the reconstruct step transposed into the next
+// level's denoised image. grad receives GLS_ADJ_NPARAMS values.
+static gls_status adjoint_run(gls_converter* cv, const gls_demosaic_params* p, const float* target, int tstride,
+                              double* loss, float* grad, cudaStream_t s) {
+    Pipeline<float>& P = cv->p32s[0];
+    const int W = P.W, H = P.H, L = p->levels;
+    const size_t n = size_t(W) * H;
+    GLS_TRY(cv->adj_gden[0].ensure(n * 3 * sizeof(float)));
+    GLS_TRY(cv->adj_gden[1].ensure(n * 3 * sizeof(float)));
+    GLS_TRY(cv->adj_rec.ensure(n * 12 * sizeof(float)));
+    GLS_TRY(cv->adj_glayer.ensure(n * 4 * sizeof(float)));
+    GLS_TRY(cv->adj_gpca.ensure(n * 8 * sizeof(float)));
+    GLS_TRY(cv->adj_gup.ensure(n * 3 * sizeof(float)));
+    std::vector<size_t> bm_off(L), sn_off(L);
+    size_t parts = 0;
+    for (int i = 0; i < L; i++) {
+        bm_off[i] = parts;
+        parts += size_t(adjoint_blocks(W >> i, H >> i)) * 6;
+        sn_off[i] = parts;
+        if (i < L - 1) parts += size_t(adjoint_sn_blocks(W >> i, H >> i)) * 2;
+    }
+    const int head_blocks = adjoint_sn_blocks(W, H);
+    GLS_TRY(cv->adj_part.ensure(std::max<size_t>(parts, 1) * sizeof(float)));
+    GLS_TRY(cv->adj_loss.ensure(size_t(head_blocks) * sizeof(double)));
+    float* part = static_cast<float*>(cv->adj_part.p);
+
+    float c2y[9], y2c[9];
+    cam_ycbcr(p->rgb_cam, p->xyz_rgb, c2y, y2c);
+    AdjointHeadArgs ha;
+    std::memcpy(ha.m, y2c, sizeof(y2c));
+    ha.inv_n = float(1.0 / (3.0 * double(n)));
+    float* gcur = static_cast<float*>(cv->adj_gden[0].p);
+    float* gnext = static_cast<float*>(cv->adj_gden[1].p);
+    launch_adj_head(static_cast<const float*>(P.den[0].p), target, tstride, W, H, ha, gcur,
+                    static_cast<double*>(cv->adj_loss.p), s);
+    for (int i = 0; i < L; i++) {
+        const int wi = W >> i, hi = H >> i;
+        const gls_denoise_params& dp = p->denoise[i];
+        const float* img_i = static_cast<const float*>(i == 0 ? P.B.p : P.img[i].p);
+        const float* layer = i < L - 1 ? static_cast<const float*>(P.sub[i].p) : img_i;
+        const float* grd = static_cast<const float*>(i == 0 ? P.grad.p : P.gradp[i].p);
+        const float* basis = static_cast<const float*>(P.basis.p) + i * 200;
+        launch_pca_project<float>(Plane<float, 4>{const_cast<float*>(layer), wi, hi, size_t(wi) * 4}, basis,
+                                  plane<float, 8>(P.pca, wi, hi), s);
+        AdjointLevelArgs la{};
+        la.w = wi;
+        la.h = hi;
+        la.layer = layer;
+        la.grad = grd;
+        la.pca = static_cast<const float*>(P.pca.p);
+        la.basis = basis;
+        la.g_den = gcur;
+        la.rec = static_cast<float*>(cv->adj_rec.p);
+        la.g_layer = static_cast<float*>(cv->adj_glayer.p);
+        la.g_pca = static_cast<float*>(cv->adj_gpca.p);
+        la.part = part + bm_off[i];
+        for (int c = 0; c < 3; c++) {
+            la.var_a[c] = p->pyramid_nlf[i].a[c];
+            la.var_b[c] = p->pyramid_nlf[i].b[c];
+        }
+        la.tm[0] = dp.luma;
+        la.tm[1] = dp.chroma;
+        la.tm[2] = dp.chroma;
+        la.chroma_boost = dp.chroma_boost;
+        la.gradient_boost = dp.gradient_boost;
+        la.gradient_threshold = dp.gradient_threshold;
+        launch_bm_bwd(la, s);
+        if (i < L - 1) {
+            AdjointSnArgs sa{};
+            sa.w = wi;
+            sa.h = hi;
+            sa.cw = W >> (i + 1);
+            sa.ch = H >> (i + 1);
+            sa.rx = float(sa.cw) / float(wi);
+            sa.ry = float(sa.ch) / float(hi);
+            sa.in = img_i;
+            sa.coarse = static_cast<const float*>(P.img[i + 1].p);
+            sa.coarse_den = static_cast<const float*>(P.den[i + 1].p);
+            sa.grad = grd;
+            sa.g_layer = la.g_layer;
+            sa.g_up = static_cast<float*>(cv->adj_gup.p);
+            sa.g_coarse_den = gnext;
+            sa.part = part + sn_off[i];
+            sa.luma_weight = 1.f;
+            sa.sharpening = dp.sharpening;
+            sa.nlf_a = p->pyramid_nlf[i].a[0] * dp.luma;
+            sa.nlf_b = p->pyramid_nlf[i].b[0] * dp.luma;
+            launch_sn_bwd(sa, s);
+            std::swap(gcur, gnext);
+        }
+    }
+    GLS_CUDA(cudaGetLastError());
+    std::vector<float> hp(parts);
+    std::vector<double> hl(head_blocks);
+    if (parts) GLS_CUDA(cudaMemcpyAsync(hp.data(), part, parts * sizeof(float), cudaMemcpyDeviceToHost, s));
+    GLS_CUDA(cudaMemcpyAsync(hl.data(), cv->adj_loss.p, hl.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    GLS_CUDA(cudaStreamSynchronize(s));
+    double g[GLS_ADJ_NPARAMS] = {};
+    for (int i = 0; i < L; i++) {
+        const int nb = adjoint_blocks(W >> i, H >> i);
+        double t[6] = {0, 0, 0, 0, 0, 0};
+        for (int b = 0; b < nb; b++)
+            for (int k = 0; k < 6; k++) t[k] += hp[bm_off[i] + size_t(b) * 6 + k];
+        g[GLS_ADJ_LUMA + i] += t[0];
+        g[GLS_ADJ_CHROMA + i] += t[1];
+        g[GLS_ADJ_NLF_AY + i] += t[2];
+        g[GLS_ADJ_NLF_BY + i] += t[3];
+        g[GLS_ADJ_NLF_AC + i] += t[4];
+        g[GLS_ADJ_NLF_BC + i] += t[5];
+        if (i < L - 1) {  // nlf_a = A_Y luma, nlf_b = B_Y luma
+            const int ns = adjoint_sn_blocks(W >> i, H >> i);
+            double ga = 0, gb = 0;
+            for (int b = 0; b < ns; b++) {
+                ga += hp[sn_off[i] + size_t(b) * 2];
+                gb += hp[sn_off[i] + size_t(b) * 2 + 1];
+            }
+            const double luma = p->denoise[i].luma;
+            g[GLS_ADJ_NLF_AY + i] += ga * luma;
+            g[GLS_ADJ_NLF_BY + i] += gb * luma;
+            g[GLS_ADJ_LUMA + i] += ga * p->pyramid_nlf[i].a[0] + gb * p->pyramid_nlf[i].b[0];
+        }
+    }
+    double lsum = 0;
+    for (double v : hl) lsum += v;
+    if (loss) *loss = lsum / (3.0 * double(n));
+    for (int k = 0; k < GLS_ADJ_NPARAMS; k++) grad[k] = float(g[k]);
+    grad[GLS_ADJ_RAW_GREEN_A] = NAN;  // not differentiated (the front end is held fixed)
+    grad[GLS_ADJ_RAW_GREEN_B] = NAN;
+    return GLS_OK;
+}
+
+}  // namespace gls
+
 extern "C" {
 
 const char* gls_last_error_message(void) { return g_last_error.c_str(); }
@@ -571,6 +710,9 @@ gls_status gls_converter_destroy(gls_converter* conv) {
         if (conv->join_ev[k]) cudaEventDestroy(conv->join_ev[k]);
     }
     if (conv->fork_ev) cudaEventDestroy(conv->fork_ev);
+    for (DevBuf* b : {&conv->adj_gden[0], &conv->adj_gden[1], &conv->adj_rec, &conv->adj_glayer, &conv->adj_gpca,
+                      &conv->adj_gup, &conv->adj_part, &conv->adj_loss, &conv->adj_target})
+        b->release();
     delete conv;
     return GLS_OK;
 }
@@ -793,6 +935,37 @@ gls_status gls_gaussian_bilinear_taps(float radius, float* taps, int32_t max_tap
     *n_taps = n < 0 ? -n : n;
     if (n < 0) return set_error(GLS_ERR_INVALID_ARG, "max_taps too small (%d needed)", -n);
     return GLS_OK;
+}
+
+
+gls_status gls_demosaic_denoise_vjp(gls_converter* conv, const uint16_t* raw, int32_t width, int32_t height,
+                                    size_t raw_stride_bytes, const gls_demosaic_params* params,
+                                    const gls_image_view* target, uint32_t flags, double* loss, float* grad,
+                                    void* stream) {
+    clear_error();
+    if (!conv || !raw || !params || !target || !target->data || !grad)
+        return set_error(GLS_ERR_INVALID_ARG, "NULL argument");
+    if (params->levels < 1 || params->levels > GLS_MAX_LEVELS) return set_error(GLS_ERR_INVALID_ARG, "bad levels");
+    if (target->width != width || target->height != height || target->dtype != GLS_F32 ||
+        (target->channels != 3 && target->channels != 4))
+        return set_error(GLS_ERR_INVALID_ARG, "target must be a %dx%d GLS_F32 RGB or RGBA view", width, height);
+    const size_t trow = size_t(width) * target->channels * 4;
+    const size_t tstride_b = target->stride_bytes ? target->stride_bytes : trow;
+    if (tstride_b < trow || tstride_b % 4) return set_error(GLS_ERR_INVALID_ARG, "bad target stride");
+    GLS_CUDA(cudaSetDevice(conv->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    gls_image_view out{};  // converter-owned FP32 output
+    out.dtype = GLS_F32;
+    const uint32_t fw = GLS_DENOISE | (flags & GLS_HOST_IO);
+    GLS_TRY(demosaic_run<float>(conv, raw, width, height, raw_stride_bytes, params, fw & ~GLS_SYNC, &out, s));
+    const float* tp = static_cast<const float*>(target->data);
+    if ((flags & GLS_HOST_IO) || tstride_b != trow) {
+        GLS_TRY(conv->adj_target.ensure(size_t(height) * trow));
+        GLS_CUDA(cudaMemcpy2DAsync(conv->adj_target.p, trow, target->data, tstride_b, trow, height,
+                                   (flags & GLS_HOST_IO) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
+        tp = static_cast<const float*>(conv->adj_target.p);
+    }
+    return adjoint_run(conv, params, tp, target->channels, loss, grad, s);
 }
 
 }  // extern "C"

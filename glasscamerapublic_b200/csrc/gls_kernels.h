@@ -102,6 +102,41 @@ template <class S>
 void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, const float* basis, Plane<S, 4> out,
                         const BlockMatchArgs& a, cudaStream_t s);
 
+// ---- adjoint of the pyramid (gls_adjoint.cu); FP32 planes, tightly packed
+struct AdjointLevelArgs {
+    int w, h;
+    const float* layer;  // 4 ch: the level's block-matching input
+    const float* grad;   // 2 ch
+    const float* pca;    // 8 ch, projected with `basis`
+    const float* basis;  // 25 x 8 (device)
+    const float* g_den;  // 3 ch: dL/d(block-matching output Y, Cb, Cr)
+    float* rec;          // 12 per pixel: centre record for the neighbour pass
+    float* g_layer;      // 4 ch out: dL/d layer (Y, Cb, Cr)
+    float* g_pca;        // 8 ch scratch
+    float* part;         // per-block dL/dtheta: luma, chroma, A_Y, B_Y, A_C, B_C
+    float var_a[3], var_b[3], tm[3];
+    float chroma_boost, gradient_boost, gradient_threshold;
+};
+struct AdjointHeadArgs {
+    float m[9];   // YCbCr -> camera RGB
+    float inv_n;  // 1 / (3 pixels)
+};
+struct AdjointSnArgs {
+    int w, h, cw, ch;  // fine and coarse sizes
+    float rx, ry;      // coarse / fine
+    const float *in, *coarse, *coarse_den, *grad, *g_layer;
+    float* g_up;          // 3 ch fine scratch
+    float* g_coarse_den;  // 3 ch out at the coarse level
+    float* part;          // per-block dL/d nlf_a, dL/d nlf_b
+    float luma_weight, sharpening, nlf_a, nlf_b;
+};
+void launch_adj_head(const float* den0, const float* target, int tstride, int w, int h, const AdjointHeadArgs& a,
+                     float* g_den, double* loss_part, cudaStream_t s);
+void launch_bm_bwd(const AdjointLevelArgs& a, cudaStream_t s);
+void launch_sn_bwd(const AdjointSnArgs& a, cudaStream_t s);
+int adjoint_blocks(int w, int h);
+int adjoint_sn_blocks(int w, int h);
+
 // host-side eigen-solve of the same accumulators (the reference's per-level
 // host PCA, pyramid_processor.cpp:148-149)
 void host_pca_basis(const double* part, int n_blocks, int n_patches, float* basis);

@@ -233,6 +233,41 @@ gls_status gls_calibration_fill(int32_t camera, int32_t iso, gls_demosaic_params
  * most max_taps taps; *n_taps receives the count. */
 gls_status gls_gaussian_bilinear_taps(float radius, float* taps, int32_t max_taps, int32_t* n_taps);
 
+/* ==== Adjoint (no reference counterpart) ====
+ * Gradient of L = mean over pixels and R, G, B of (output - target)^2, where
+ * output is the FP32 path's linear camera RGB of `raw` (demosaic + pyramid
+ * denoise + reconstruct), with respect to GLS_ADJ_NPARAMS scalars of
+ * gls_demosaic_params, laid out as:
+ *   [GLS_ADJ_LUMA + l]     denoise[l].luma
+ *   [GLS_ADJ_CHROMA + l]   denoise[l].chroma
+ *   [GLS_ADJ_NLF_AY + l]   pyramid_nlf[l].a[0]
+ *   [GLS_ADJ_NLF_BY + l]   pyramid_nlf[l].b[0]
+ *   [GLS_ADJ_NLF_AC + l]   pyramid_nlf[l].a[1] = a[2] (Cb and Cr tied)
+ *   [GLS_ADJ_NLF_BC + l]   pyramid_nlf[l].b[1] = b[2]
+ *   [GLS_ADJ_RAW_GREEN_A], [GLS_ADJ_RAW_GREEN_B]  raw_nlf green a, b
+ * for l < levels (entries of absent levels are 0). The forward runs first
+ * (as gls_demosaic with GLS_DENOISE on FP32 planes); the reverse sweep is
+ * hand-written CUDA over its retained planes, with each level's PCA basis
+ * held fixed. The raw-green entries are NaN: the front end (demosaic,
+ * despeckle) is not differentiated. target: GLS_F32 RGB or RGBA,
+ * width x height, device memory (host with GLS_HOST_IO, which also makes
+ * raw host memory). Synchronises the stream. */
+#define GLS_ADJ_NPARAMS 32
+enum {
+    GLS_ADJ_LUMA = 0,
+    GLS_ADJ_CHROMA = 5,
+    GLS_ADJ_NLF_AY = 10,
+    GLS_ADJ_NLF_BY = 15,
+    GLS_ADJ_NLF_AC = 20,
+    GLS_ADJ_NLF_BC = 25,
+    GLS_ADJ_RAW_GREEN_A = 30,
+    GLS_ADJ_RAW_GREEN_B = 31
+};
+gls_status gls_demosaic_denoise_vjp(gls_converter* conv, const uint16_t* raw, int32_t width, int32_t height,
+                                    size_t raw_stride_bytes, const gls_demosaic_params* params,
+                                    const gls_image_view* target, uint32_t flags, double* loss, float* grad,
+                                    void* stream);
+
 /* ==== Registration and fusion (ImageRegistration/, PyramidFusion/) ==== */
 
 /* KeyPoint (ImageRegistration/feature2d.hpp:25-47), 28 bytes. angle is in

@@ -958,9 +958,12 @@ struct PyramidOut {
 };
 
 // PyramidProcessor<levels>::denoise, pyramid_processor.cpp:96-172.
+// frozen (optional): per-level PCA bases to use instead of computing them
+// (the adjoint's gradient checks hold the bases fixed).
 template <class T>
 Plane4<T> pyramid_denoise(const Plane4<T>& image, const Plane2<T>& gradient, const Params& p,
-                          std::vector<Plane4<T>>* denoised_levels = nullptr, PyramidOut* info = nullptr) {
+                          std::vector<Plane4<T>>* denoised_levels = nullptr, PyramidOut* info = nullptr,
+                          const std::vector<std::array<std::array<double, 8>, 25>>* frozen = nullptr) {
     const int L = p.levels;
     std::vector<Plane4<T>> img(L);     // img[i] = level i input (img[0] = image)
     std::vector<Plane2<T>> grad(L);
@@ -983,7 +986,7 @@ Plane4<T> pyramid_denoise(const Plane4<T>& image, const Plane2<T>& gradient, con
         } else {
             layer = img[i];
         }
-        const auto basis = pca_basis(layer);
+        const auto basis = frozen ? (*frozen)[i] : pca_basis(layer);
         if (info) info->bases[i] = basis;
         const auto pca = pca_project(layer, basis);
         den[i] = block_match(layer, grad[i], pca, p.pyr_nlf[i], dp, p.lsc);

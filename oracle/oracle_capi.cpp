@@ -130,6 +130,34 @@ int orc_pyramid_denoise(const float* ycc, const float* grad, int w, int h, const
     return 0;
 }
 
+// MSE of the FP64 pyramid denoise + output transform against a target,
+// with the per-level PCA bases given (held fixed): the function whose
+// central differences check the adjoint. y2c: YCbCr -> camera RGB, 3x3
+// row-major; target: h x w x tch floats (RGB first).
+int orc_pyramid_loss(const float* ycc, const float* grad, int w, int h, const gls_demosaic_params* gp,
+                     const double* bases, const double* y2c, const float* target, int tch, double* loss) {
+    const Params p = to_params(gp);
+    std::vector<std::array<std::array<double, 8>, 25>> fb(p.levels);
+    for (int l = 0; l < p.levels; l++)
+        for (int r = 0; r < 25; r++)
+            for (int c = 0; c < 8; c++) fb[l][r][c] = bases[(l * 25 + r) * 8 + c];
+    auto img = copy_in<double, 4>(ycc, w, h);
+    auto g = copy_in<double, 2>(grad, w, h);
+    const auto den = pyramid_denoise<double>(img, g, p, nullptr, nullptr, &fb);
+    double acc = 0;
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) {
+            const double* d = den.px(x, y);
+            const float* t = target + (size_t(y) * w + x) * tch;
+            for (int r = 0; r < 3; r++) {
+                const double o = y2c[r * 3 + 0] * d[0] + y2c[r * 3 + 1] * d[1] + y2c[r * 3 + 2] * d[2];
+                acc += (o - t[r]) * (o - t[r]);
+            }
+        }
+    *loss = acc / (3.0 * double(w) * h);
+    return 0;
+}
+
 // ---- single stages from given inputs (for the stage-by-stage pin against
 // the reference's own kernels, oracle/ref_harness.cpp)
 

@@ -38,6 +38,7 @@ def lib() -> C.CDLL:
         L.orc_pca_basis.argtypes = [fp, C.c_int, C.c_int, dp]
         L.orc_jacobi.argtypes = [C.c_int, dp, dp, dp]
         L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_pyramid_loss.argtypes = [fp, fp, C.c_int, C.c_int, C.POINTER(DemosaicParams), dp, dp, fp, C.c_int, dp]
         _lib = L
     return _lib
 
@@ -167,3 +168,17 @@ def stage(name, *arrays, p, w, h, out_shape, f64=False, raw=None):
     else:
         assert fn(*args, w, h, C.byref(p), int(f64), _fp(out)) == 0
     return out
+
+
+def pyramid_loss(ycc, grad, p: DemosaicParams, bases, y2c, target) -> float:
+    """MSE of the FP64 pyramid (bases held fixed) + output transform vs target."""
+    ycc = np.ascontiguousarray(ycc, np.float32)
+    grad = np.ascontiguousarray(grad, np.float32)
+    t = np.ascontiguousarray(target, np.float32)
+    b = np.ascontiguousarray(bases, np.float64)
+    m = np.ascontiguousarray(np.asarray(y2c, np.float64).ravel())
+    h, w = ycc.shape[:2]
+    out = C.c_double(0)
+    assert lib().orc_pyramid_loss(_fp(ycc), _fp(grad), w, h, C.byref(p), _dp(b), _dp(m), _fp(t), t.shape[2],
+                                  C.byref(out)) == 0
+    return out.value
