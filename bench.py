@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--no-burst", action="store_true", help="skip the burst registration + fusion leg")
     ap.add_argument("--burst-frames", type=int, default=8)
     ap.add_argument("--burst-only", action="store_true", help="run only the burst leg (for profiler captures)")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (calibration-gradient) leg")
+    ap.add_argument("--adjoint-only", action="store_true", help="run only the adjoint leg (for profiler captures)")
     return ap.parse_args()
 
 
@@ -233,6 +235,68 @@ def burst_leg(args, rank, local, conv, stream):
     }
 
 
+def adjoint_leg(args, rank, local, conv, stream):
+    """Differentiable calibration (the 8 x 2048x1536 adjoint workload): per
+    frame, the FP32 raw -> RGB forward and the hand-written adjoint of the
+    pyramid (gls_demosaic_denoise_vjp), MSE against the known clean target,
+    gradient for the 30 per-level pyramid parameters. Device-timed; the
+    forward alone is timed too, so the adjoint's own cost is the
+    difference."""
+    import torch
+
+    from glasscamerapublic_b200 import scene
+    from glasscamerapublic_b200 import adjoint as A
+
+    n = 8
+    wl = scene.Workload("cfg5_2048x1536", 2048, 1536, levels=5, gain=1.0, read=4.0, iso=800, seed=5000 + 97 * rank)
+    params = scene.make_params(wl)
+    dev = f"cuda:{local}"
+    raws, targets = [], []
+    for f in range(n):
+        raw, clean = scene.make_raw(wl, frame=f)
+        raws.append(torch.from_numpy(raw.view(np.int16)).to(dev))
+        targets.append(torch.from_numpy(scene.target_rgb(clean).astype(np.float32)).to(dev))
+    out = torch.empty((wl.height, wl.width, 4), dtype=torch.float32, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        for f in range(2):
+            A.loss_and_grad(conv, raws[f], params, targets[f], stream=stream)
+        reps = max(1, min(args.steps, 3))
+        t0 = time.perf_counter()
+        e0.record(stream)
+        gsum = np.zeros(30)
+        lsum = 0.0
+        for _ in range(reps):
+            for f in range(n):
+                loss, grad = A.loss_and_grad(conv, raws[f], params, targets[f], stream=stream)
+                gsum += grad[:30]
+                lsum += loss
+        e1.record(stream)
+        stream.synchronize()
+        wall = (time.perf_counter() - t0) / reps
+        ms_vjp = max(e0.elapsed_time(e1) / reps, 1e3 * wall)
+        e0.record(stream)
+        for _ in range(reps):
+            for f in range(n):
+                conv.demosaic(raws[f], params, noiseReduction=True, fp16=False, out=out, out_fp16=False,
+                              stream=stream, sync=False)
+        e1.record(stream)
+        stream.synchronize()
+        ms_fwd = e0.elapsed_time(e1) / reps
+    return {
+        "workload": f"{n} x 2048x1536 RGGB 12-bit, 5 levels, FP32 forward + adjoint, MSE vs clean target",
+        "ms_per_batch": ms_vjp,
+        "ms_per_frame": ms_vjp / n,
+        "forward_ms_per_frame": ms_fwd / n,
+        "adjoint_ms_per_frame": (ms_vjp - ms_fwd) / n,
+        "params_differentiated": 30,
+        "mean_loss": lsum / (reps * n),
+        "grad_norm": float(np.linalg.norm(gsum / (reps * n))),
+        "note": "per-level luma/chroma strengths and YCbCr NLF (A_Y, B_Y, A_C, B_C); PCA bases held fixed; "
+                "raw-green NLF not differentiated",
+    }
+
+
 def run_reference(args, rank):
     """The reference arm: the reference's path on the host cores. The Metal
     runtime cannot run here; the reference's own kernel source, compiled
@@ -285,10 +349,11 @@ def main():
     conv = g.RawConverter(local)
     lib = g.lib()
     stream = torch.cuda.Stream()
-    if args.burst_only:
-        b = burst_leg(args, rank, local, conv, stream)
+    if args.burst_only or args.adjoint_only:
+        b = burst_leg(args, rank, local, conv, stream) if args.burst_only else adjoint_leg(args, rank, local, conv,
+                                                                                          stream)
         if rank == 0:
-            print(json.dumps({"burst_only": True, **b}), flush=True)
+            print(json.dumps({"burst_only" if args.burst_only else "adjoint_only": True, **b}), flush=True)
         conv.close()
         if world > 1:
             dist.destroy_process_group()
@@ -433,6 +498,10 @@ def main():
         b = burst_leg(args, rank, local, conv, stream)
         (b["ms_per_burst"],) = max_over_ranks([b["ms_per_burst"]], dist if world > 1 else None)
         line["burst"] = b
+    if not args.no_adjoint:
+        a = adjoint_leg(args, rank, local, conv, stream)
+        (a["ms_per_batch"],) = max_over_ranks([a["ms_per_batch"]], dist if world > 1 else None)
+        line["adjoint"] = a
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wl, scene.make_params, args.cpu_seconds)
     if rank == 0:

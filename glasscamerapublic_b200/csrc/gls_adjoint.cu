@@ -16,6 +16,7 @@
 // adjoint.
 //   * k_adj_head          dL/d den_0 = M^T 2 (out - target) / N, and the loss
 //   * k_bm_bwd_center     block matching, the pixel as the window centre:
+//                         from the forward's outputs and kernel norms,
 //                         recomputes its weights, then dL/d(its scales, its
 //                         own PCA coefficients and chroma), dL/dtheta, and a
 //                         per-pixel record for the neighbour pass
@@ -137,30 +138,12 @@ __global__ void __launch_bounds__(256) k_bm_bwd_center(AdjointLevelArgs a) {
         const float mag = sqrtf(gr.x * gr.x + gr.y * gr.y);
         const BmScales S = bm_scales(a, in.x, mag);
         const float L2 = S.L * S.L;
-        // sweep A: the forward sums
-        float fy = 0, fcb = 0, fcr = 0, ny = 0, nc = 0;
-        for (int j = 0; j < 21; j++)
-            for (int i = 0; i < 21; i++) {
-                const int q = (threadIdx.y + j) * AW_ + threadIdx.x + i;
-                const float4 s = sm.q[q][0], p0 = sm.q[q][1], p1 = sm.q[q][2];
-                const float sp[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
-                float d2 = 0.f;
-#pragma unroll
-                for (int k = 0; k < 8; k++) d2 += (sp[k] - ip[k]) * (sp[k] - ip[k]);
-                const float lw = expf(-2.f * d2 * L2);
-                const float c1 = (s.y - in.y) * S.K1, c2 = (s.z - in.z) * S.K2;
-                const float cw = expf(-2.f * (lw * lw + c1 * c1 + c2 * c2));
-                const float sw = sm.sw[j * 21 + i];
-                fy += sw * lw * s.x;
-                fcb += sw * cw * s.y;
-                fcr += sw * cw * s.z;
-                ny += sw * lw;
-                nc += sw * cw;
-            }
-        const float Yo = fy / ny, Cbo = fcb / nc, Cro = fcr / nc;
+        // the forward's sums: outputs and the two kernel norms
+        const float4 dv = *reinterpret_cast<const float4*>(a.den + pi * 4);
+        const float Yo = dv.x, Cbo = dv.y, Cro = dv.z, ny = dv.w, nc = a.nc[pi];
         const float3 g = *reinterpret_cast<const float3*>(a.g_den + pi * 3);
         const float gYn = g.x / ny, gCbn = g.y / nc, gCrn = g.z / nc;
-        // sweep B: gradients of the centre's own quantities
+        // gradients of the centre's own quantities, tap by tap
         float gL = 0, gK1 = 0, gK2 = 0, gcb = 0, gcr = 0;
         float gip[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         for (int j = 0; j < 21; j++)
@@ -171,10 +154,10 @@ __global__ void __launch_bounds__(256) k_bm_bwd_center(AdjointLevelArgs a) {
                 float d2 = 0.f;
 #pragma unroll
                 for (int k = 0; k < 8; k++) d2 += (sp[k] - ip[k]) * (sp[k] - ip[k]);
-                const float lw = expf(-2.f * d2 * L2);
+                const float lw = __expf(-2.f * d2 * L2);
                 const float dcb = s.y - in.y, dcr = s.z - in.z;
                 const float c1 = dcb * S.K1, c2 = dcr * S.K2;
-                const float cw = expf(-2.f * (lw * lw + c1 * c1 + c2 * c2));
+                const float cw = __expf(-2.f * (lw * lw + c1 * c1 + c2 * c2));
                 const float sw = sm.sw[j * 21 + i];
                 const float gw = gYn * (s.x - Yo);
                 const float gc = gCbn * (s.y - Cbo) + gCrn * (s.z - Cro);
@@ -232,7 +215,7 @@ struct NeighborSmem {
 // Block matching, the pixel q as a neighbour of every centre p whose
 // window reads it (p in the 21 x 21 box around q; at the image border,
 // every tap offset that clamps onto q).
-__global__ void __launch_bounds__(256) k_bm_bwd_neighbor(AdjointLevelArgs a) {
+__global__ void __launch_bounds__(256, 1) k_bm_bwd_neighbor(AdjointLevelArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     NeighborSmem& sm = *reinterpret_cast<NeighborSmem*>(smem_raw);
     const int W = a.w, H = a.h;
@@ -262,42 +245,57 @@ __global__ void __launch_bounds__(256) k_bm_bwd_neighbor(AdjointLevelArgs a) {
     const float sp[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
     float gs0 = 0, gs1 = 0, gs2 = 0;
     float gsp[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int py = max(qy - AH, 0); py <= min(qy + AH, H - 1); py++) {
-        int jlo, jhi;
-        if (!preimage(qy, py, AH, H, jlo, jhi)) continue;
-        for (int px = max(qx - AH, 0); px <= min(qx + AH, W - 1); px++) {
-            int ilo, ihi;
-            if (!preimage(qx, px, AH, W, ilo, ihi)) continue;
-            const int k = (py - y0 + AH) * AW_ + (px - x0 + AH);
-            const float4 r0 = sm.p[k][0], r1 = sm.p[k][1], r2 = sm.p[k][2], c0 = sm.p[k][3], c1v = sm.p[k][4];
-            const float gYn = r0.x, Yo = r0.y, gCbn = r0.z, Cbo = r0.w;
-            const float gCrn = r1.x, Cro = r1.y, L = r1.z, K1 = r1.w, K2 = r2.x, cbp = r2.y, crp = r2.z;
-            const float ip[8] = {c0.x, c0.y, c0.z, c0.w, c1v.x, c1v.y, c1v.z, c1v.w};
-            float d2 = 0.f;
+    // the contribution of centre p reading q through tap offset (i, j)
+    auto pair = [&](int k, int ilo, int ihi, int jlo, int jhi) {
+        const float4 r0 = sm.p[k][0], r1 = sm.p[k][1], r2 = sm.p[k][2], c0 = sm.p[k][3], c1v = sm.p[k][4];
+        const float gYn = r0.x, Yo = r0.y, gCbn = r0.z, Cbo = r0.w;
+        const float gCrn = r1.x, Cro = r1.y, L = r1.z, K1 = r1.w, K2 = r2.x, cbp = r2.y, crp = r2.z;
+        const float ip[8] = {c0.x, c0.y, c0.z, c0.w, c1v.x, c1v.y, c1v.z, c1v.w};
+        float d2 = 0.f;
 #pragma unroll
-            for (int m = 0; m < 8; m++) d2 += (sp[m] - ip[m]) * (sp[m] - ip[m]);
-            const float L2 = L * L;
-            const float lw = expf(-2.f * d2 * L2);
-            const float dcb = s.y - cbp, dcr = s.z - crp;
-            const float c1 = dcb * K1, c2 = dcr * K2;
-            const float cw = expf(-2.f * (lw * lw + c1 * c1 + c2 * c2));
-            const float gw = gYn * (s.x - Yo);
-            const float gc = gCbn * (s.y - Cbo) + gCrn * (s.z - Cro);
-            for (int j = jlo; j <= jhi; j++)
-                for (int i = ilo; i <= ihi; i++) {
-                    const float sw = sm.sw[(j + AH) * 21 + i + AH];
-                    const float wy = sw * lw, wc = sw * cw;
-                    gs0 += gYn * wy;
-                    gs1 += gCbn * wc;
-                    gs2 += gCrn * wc;
-                    const float garg = -2.f * gc * sw * cw;
-                    const float glw = gw * sw + 2.f * garg * lw;
-                    gs1 += 2.f * garg * c1 * K1;
-                    gs2 += 2.f * garg * c2 * K2;
-                    const float gd2 = -2.f * glw * lw * L2;
+        for (int m = 0; m < 8; m++) d2 += (sp[m] - ip[m]) * (sp[m] - ip[m]);
+        const float L2 = L * L;
+        const float lw = __expf(-2.f * d2 * L2);
+        const float dcb = s.y - cbp, dcr = s.z - crp;
+        const float c1 = dcb * K1, c2 = dcr * K2;
+        const float cw = __expf(-2.f * (lw * lw + c1 * c1 + c2 * c2));
+        const float gw = gYn * (s.x - Yo);
+        const float gc = gCbn * (s.y - Cbo) + gCrn * (s.z - Cro);
+        float gd2 = 0.f;
+        for (int j = jlo; j <= jhi; j++)
+            for (int i = ilo; i <= ihi; i++) {
+                const float sw = sm.sw[(j + AH) * 21 + i + AH];
+                const float wy = sw * lw, wc = sw * cw;
+                const float garg = -2.f * gc * sw * cw;
+                const float glw = gw * sw + 2.f * garg * lw;
+                gs0 += gYn * wy;
+                gs1 += gCbn * wc + 2.f * garg * c1 * K1;
+                gs2 += gCrn * wc + 2.f * garg * c2 * K2;
+                gd2 += -2.f * glw * lw * L2;
+            }
 #pragma unroll
-                    for (int m = 0; m < 8; m++) gsp[m] += 2.f * gd2 * (sp[m] - ip[m]);
-                }
+        for (int m = 0; m < 8; m++) gsp[m] += 2.f * gd2 * (sp[m] - ip[m]);
+    };
+    const int py0 = max(qy - AH, 0), py1 = min(qy + AH, H - 1);
+    const int px0 = max(qx - AH, 0), px1 = min(qx + AH, W - 1);
+    if (qx > 0 && qx < W - 1 && qy > 0 && qy < H - 1) {
+        // not on the image border: every centre reads q through exactly one tap
+        for (int py = py0; py <= py1; py++) {
+            const int j = qy - py;
+            for (int px = px0; px <= px1; px++) {
+                const int i = qx - px;
+                pair((py - y0 + AH) * AW_ + (px - x0 + AH), i, i, j, j);
+            }
+        }
+    } else {
+        for (int py = py0; py <= py1; py++) {
+            int jlo, jhi;
+            if (!preimage(qy, py, AH, H, jlo, jhi)) continue;
+            for (int px = px0; px <= px1; px++) {
+                int ilo, ihi;
+                if (!preimage(qx, px, AH, W, ilo, ihi)) continue;
+                pair((py - y0 + AH) * AW_ + (px - x0 + AH), ilo, ihi, jlo, jhi);
+            }
         }
     }
     float4* gl = reinterpret_cast<float4*>(a.g_layer + qi * 4);

@@ -169,6 +169,10 @@ __global__ void __launch_bounds__(256) k_block_match_plain(Plane<S, 4> img, Plan
     if (x < out.w) {
         if (yu < out.h) st4<S>(out.px(x, yu), f4{acc[0] / acc[3], acc[1] / acc[4], acc[2] / acc[4], acc[3]});
         if (yu + 1 < out.h) st4<S>(out.px(x, yu + 1), f4{acc[5] / acc[8], acc[6] / acc[9], acc[7] / acc[9], acc[8]});
+        if (a.nc_out) {
+            if (yu < out.h) a.nc_out[size_t(yu) * out.w + x] = acc[4];
+            if (yu + 1 < out.h) a.nc_out[size_t(yu + 1) * out.w + x] = acc[9];
+        }
     }
 }
 

@@ -41,6 +41,7 @@ struct Pipeline {
     int W = 0, H = 0, L = 0;
     DevBuf raw, scaled, grad, quad, A, B, pca, acc, basis, status;
     DevBuf img[GLS_MAX_LEVELS], gradp[GLS_MAX_LEVELS], sub[GLS_MAX_LEVELS], den[GLS_MAX_LEVELS];
+    DevBuf nc[GLS_MAX_LEVELS];  // chroma norms, kept only for the adjoint
     DevBuf out_f32, out_f16, stage_in, stage_grad;
     std::vector<double> host_acc;
     std::vector<float> host_basis;
@@ -80,6 +81,7 @@ struct Pipeline {
             gradp[i].release();
             sub[i].release();
             den[i].release();
+            nc[i].release();
         }
     }
 };
@@ -177,6 +179,7 @@ struct gls_converter {
     int last_levels = 0;
     int last_w = 0, last_h = 0;
     bool last_denoise = false;
+    bool keep_nc = false;  // the FP32 forward keeps its chroma norms (for the adjoint)
     // adjoint scratch (gls_demosaic_denoise_vjp)
     DevBuf adj_gden[2], adj_rec, adj_glayer, adj_gpca, adj_gup, adj_part, adj_loss, adj_target;
 };
@@ -311,6 +314,10 @@ static gls_status pyramid_run(gls_converter* cv, Pipeline<S>& P, Plane<S, 4> img
         ba.gradient_boost = dp.gradient_boost;
         ba.gradient_threshold = dp.gradient_threshold;
         ba.lsc = p->lens_shading_correction;
+        if (!is_half<S>::value && cv->keep_nc) {
+            GLS_TRY(P.nc[i].ensure(size_t(wi) * hi * sizeof(float)));
+            ba.nc_out = static_cast<float*>(P.nc[i].p);
+        }
         KScope k(cv->prof, KC_BLOCK_MATCH, s);
         launch_block_match<S>(layer, grd[i], pcap, basis + i * 200, plane<S, 4>(P.den[i], wi, hi), ba, s);
     }
@@ -584,6 +591,8 @@ static gls_status adjoint_run(gls_converter* cv, const gls_demosaic_params* p, c
         AdjointLevelArgs la{};
         la.w = wi;
         la.h = hi;
+        la.den = static_cast<const float*>(P.den[i].p);
+        la.nc = static_cast<const float*>(P.nc[i].p);
         la.layer = layer;
         la.grad = grd;
         la.pca = static_cast<const float*>(P.pca.p);
@@ -957,7 +966,10 @@ gls_status gls_demosaic_denoise_vjp(gls_converter* conv, const uint16_t* raw, in
     gls_image_view out{};  // converter-owned FP32 output
     out.dtype = GLS_F32;
     const uint32_t fw = GLS_DENOISE | (flags & GLS_HOST_IO);
-    GLS_TRY(demosaic_run<float>(conv, raw, width, height, raw_stride_bytes, params, fw & ~GLS_SYNC, &out, s));
+    conv->keep_nc = true;
+    const gls_status fst = demosaic_run<float>(conv, raw, width, height, raw_stride_bytes, params, fw, &out, s);
+    conv->keep_nc = false;
+    GLS_TRY(fst);
     const float* tp = static_cast<const float*>(target->data);
     if ((flags & GLS_HOST_IO) || tstride_b != trow) {
         GLS_TRY(conv->adj_target.ensure(size_t(height) * trow));

@@ -68,6 +68,7 @@ struct BlockMatchArgs {
     float tm[3];                  // threshold multipliers (luma, chroma, chroma)
     float chroma_boost, gradient_boost, gradient_threshold;
     float lsc;                    // lens shading correction (0 = off)
+    float* nc_out = nullptr;      // FP32 path: the chroma kernel norm per pixel, kept for the adjoint
 };
 
 struct SubtractArgs {
@@ -105,6 +106,8 @@ void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, cons
 // ---- adjoint of the pyramid (gls_adjoint.cu); FP32 planes, tightly packed
 struct AdjointLevelArgs {
     int w, h;
+    const float* den;    // 4 ch: the forward's block-matching output (Y, Cb, Cr, luma norm)
+    const float* nc;     // 1 ch: the forward's chroma norm
     const float* layer;  // 4 ch: the level's block-matching input
     const float* grad;   // 2 ch
     const float* pca;    // 8 ch, projected with `basis`
