@@ -162,7 +162,7 @@ def burst_leg(args, rank, local, conv, stream):
     import torch
 
     from glasscamerapublic_b200 import scene
-    from glasscamerapublic_b200.registration import SURF, RegisterAndFuseKernel
+    from glasscamerapublic_b200.registration import SURF, RegisterAndFuseKernel, fuse_pyramid
 
     wl = scene.WORKLOADS["cfg3_burst_4032x3024"]
     n = args.burst_frames
@@ -214,6 +214,20 @@ def burst_leg(args, rank, local, conv, stream):
             tot["raw_to_rgb"] += ev["a"].elapsed_time(ev["b"])
             tot["registration"] += ev["b"].elapsed_time(ev["c"])
             tot["fusion"] += ev["c"].elapsed_time(ev["d"])
+    # pyramid fusion of the same registered burst (uniform and robust weights)
+    pfused = torch.empty((H, W, 4), dtype=torch.float32, device=dev)
+    Hlist = [np.eye(3, dtype=np.float32)] + list(Hfull)
+    pf = {}
+    with torch.cuda.stream(stream):
+        for rob in (0.0, 100.0):
+            fuse_pyramid(surf, outs, Hlist, pfused, levels=5, robustness=rob, stream=stream)
+            stream.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fuse_pyramid(surf, outs, Hlist, pfused, levels=5, robustness=rob, stream=stream)
+            e1.record(stream)
+            stream.synchronize()
+            pf[rob] = (e0.elapsed_time(e1), pfused.cpu().numpy()[..., :3])
     errs = [scene.corner_error(Hf, Ht, W, H) for Hf, Ht in zip(Hfull, Hs[1:])]
     target = scene.target_rgb(cleans[0])
     fused_np = fused.cpu().numpy()[..., :3]
@@ -229,6 +243,9 @@ def burst_leg(args, rank, local, conv, stream):
         "registration_ms_per_frame": res["registration"] / (n - 1),
         "corner_error_px": {"max": max(errs), "mean": float(np.mean(errs))},
         "fused_psnr_db": scene.psnr(fused_np[crop], target[crop]),
+        "pyramid_fusion": {"ms_uniform": pf[0.0][0], "ms_robust": pf[100.0][0], "levels": 5,
+                           "psnr_uniform_db": scene.psnr(pf[0.0][1][crop], target[crop]),
+                           "psnr_robust_db": scene.psnr(pf[100.0][1][crop], target[crop])},
         "single_frame_psnr_db": scene.psnr(single[crop], target[crop]),
         "note": "SURF on G and G2 at 2016x1512, 1500 features; all frames x channels matched and RANSAC'd "
                 "(2000 iterations, FP64 least squares) in one batch on the GPU; one host sync per burst",

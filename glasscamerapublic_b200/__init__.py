@@ -166,6 +166,8 @@ _SIGNATURES = {
                                    C.c_float, C.c_float, C.c_uint32, C.POINTER(ImageView), C.c_uint32, C.c_void_p]),
     "gls_register_and_fuse": (C.c_int, [C.POINTER(ImageView), C.POINTER(ImageView), C.POINTER(ImageView),
                                         C.POINTER(C.c_float), C.c_int32, C.c_void_p]),
+    "gls_fuse_pyramid": (C.c_int, [C.c_void_p, C.POINTER(ImageView), C.c_int32, C.POINTER(C.c_float), C.c_int32,
+                                   C.c_float, C.POINTER(ImageView), C.c_void_p]),
     "gls_register_image": (C.c_int, [C.POINTER(ImageView), C.POINTER(ImageView), C.POINTER(C.c_float), C.c_void_p]),
 }
 

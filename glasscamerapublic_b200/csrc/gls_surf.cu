@@ -1306,6 +1306,14 @@ __global__ void __launch_bounds__(256) k_register(WarpArgs a) {
 
 }  // namespace gls
 
+namespace gls {
+struct FusionScratch;
+FusionScratch* fusion_scratch_new();
+void fusion_scratch_delete(FusionScratch* f);
+gls_status fuse_pyramid_impl(FusionScratch* F, const gls_image_view* frames, int n, const float* H, int levels,
+                             float robustness, gls_image_view* out, cudaStream_t s);
+}  // namespace gls
+
 // ============================================================ host object
 using namespace gls;
 
@@ -1329,6 +1337,7 @@ struct gls_surf {
     DevBuf raw, lut;
     float lut_black = NAN, lut_white = NAN, lut_exp = NAN;
     std::vector<float> lut_host;
+    FusionScratch* fusion = nullptr;
     uint64_t launches = 0;
 };
 
@@ -1568,6 +1577,7 @@ gls_status gls_surf_destroy(gls_surf* s) {
                       &s->loss, &s->raw, &s->lut})
         b->release();
     for (auto& kv : s->sample_tables) kv.second.release();
+    if (s->fusion) fusion_scratch_delete(s->fusion);
     for (auto& sl : s->slot) {
         sl.kps.release();
         sl.desc.release();
@@ -1916,6 +1926,26 @@ gls_status gls_register_and_fuse(const gls_image_view* fused, const gls_image_vi
     clear_error();
     if (count < 1) return set_error(GLS_ERR_INVALID_ARG, "count must be >= 1");
     return warp(fused, input, out, H, count, stream);
+}
+
+gls_status gls_fuse_pyramid(gls_surf* ctx, const gls_image_view* frames, int32_t n_frames, const float* H,
+                            int32_t levels, float robustness, gls_image_view* out, void* stream) {
+    clear_error();
+    GLS_TRY(check_surf(ctx));
+    if (!frames || !out || !out->data || (n_frames > 1 && !H)) return set_error(GLS_ERR_INVALID_ARG, "NULL argument");
+    if (n_frames < 1) return set_error(GLS_ERR_INVALID_ARG, "no frames");
+    if (levels < 1 || levels > GLS_MAX_LEVELS) return set_error(GLS_ERR_INVALID_ARG, "levels must be 1..%d", GLS_MAX_LEVELS);
+    if (!(robustness >= 0.f)) return set_error(GLS_ERR_INVALID_ARG, "robustness must be >= 0");
+    const int W = frames[0].width, Hh = frames[0].height;
+    if ((W >> (levels - 1)) < 1 || (Hh >> (levels - 1)) < 1) return set_error(GLS_ERR_INVALID_ARG, "too many levels");
+    if (out->width != W || out->height != Hh || out->channels != 4 || (out->dtype != GLS_F32 && out->dtype != GLS_F16))
+        return set_error(GLS_ERR_INVALID_ARG, "out must be a %dx%d RGBA GLS_F32 or GLS_F16 view", W, Hh);
+    const size_t oes = out->dtype == GLS_F32 ? 4 : 2;
+    if ((out->stride_bytes && out->stride_bytes % (4 * oes)) || (reinterpret_cast<uintptr_t>(out->data) % (4 * oes)))
+        return set_error(GLS_ERR_INVALID_ARG, "out rows must be aligned to whole RGBA pixels");
+    if (!ctx->fusion) ctx->fusion = fusion_scratch_new();
+    return fuse_pyramid_impl(ctx->fusion, frames, n_frames, H, levels, robustness, out,
+                             reinterpret_cast<cudaStream_t>(stream));
 }
 
 gls_status gls_register_image(const gls_image_view* input, gls_image_view* out, const float* H, void* stream) {

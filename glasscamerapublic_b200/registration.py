@@ -200,3 +200,18 @@ def register_image(input_image, out, homography, stream=None):
     check(lib().gls_register_image(C.byref(iv), C.byref(ov), h.ctypes.data_as(C.POINTER(C.c_float)),
                                    _stream_handle(stream)))
     return out
+
+
+def fuse_pyramid(ctx: SURF, frames, homographies, out, levels: int = 5, robustness: float = 0.0, stream=None):
+    """Pyramid burst fusion (gls_fuse_pyramid): frames[0] is the reference,
+    frames[f] is warped by homographies[f] (reference -> frame); CUDA
+    tensors (RGBA F32/F16), out RGBA F32/F16 CUDA tensor."""
+    n = len(frames)
+    views = (ImageView * n)(*[_view(f, 4) for f in frames])
+    H = np.zeros((n, 9), np.float32)
+    for f in range(1, n):
+        H[f] = np.asarray(homographies[f], np.float32).ravel()
+    ov = _view(out, 4)
+    check(lib().gls_fuse_pyramid(ctx.handle, views, n, H.ctypes.data_as(C.POINTER(C.c_float)), levels,
+                                 float(robustness), C.byref(ov), _stream_handle(stream)))
+    return out

@@ -384,6 +384,21 @@ gls_status gls_register_and_fuse(const gls_image_view* fused, const gls_image_vi
 /* registerImage (SURF.metal:518-538): out = input(H p). */
 gls_status gls_register_image(const gls_image_view* input, gls_image_view* out, const float* H, void* stream);
 
+/* Pyramid burst fusion (the reference declares this API but leaves it
+ * unimplemented, pyramid_processor.hpp:51-55, 64-70; this is the library's
+ * design). frames[0] is the reference; frame f > 0 is pull-warped into it
+ * by H[f] (row-major 3x3, reference -> frame, as registerAndFuse takes;
+ * H[0] is not read). Each warped frame is split into a `levels`-level
+ * Laplacian pyramid with the denoiser's down- and up-sampling; per level
+ * and pixel the frames are averaged with weights
+ * exp(-robustness * |band - reference band|^2) (the reference weighs 1),
+ * and the fused pyramid is collapsed. robustness = 0 gives uniform weights,
+ * whose result is the flat mean of the warped frames (registerAndFuse's,
+ * up to float rounding). frames: RGBA GLS_F32 or GLS_F16 device views;
+ * out: width x height RGBA GLS_F32 or GLS_F16 device view (alpha 0). */
+gls_status gls_fuse_pyramid(gls_surf* ctx, const gls_image_view* frames, int32_t n_frames, const float* H,
+                            int32_t levels, float robustness, gls_image_view* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
