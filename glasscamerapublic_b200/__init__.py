@@ -34,6 +34,7 @@ POSTPROCESS = 1 << 1
 FP16_STORAGE = 1 << 2
 HOST_IO = 1 << 3
 SYNC = 1 << 4
+GRAPH = 1 << 6
 HOST_PCA = 1 << 5
 
 PLANE_SCALED_RAW = 0

@@ -3,6 +3,7 @@
 // (raw_converter.cpp:148-248) and PyramidProcessor<levels>::denoise
 // (pyramid_processor.cpp:96-172); the kernels are in gls_front.cu and
 // gls_pyramid.cu.
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -180,6 +181,9 @@ struct gls_converter {
     int last_w = 0, last_h = 0;
     bool last_denoise = false;
     bool keep_nc = false;  // the FP32 forward keeps its chroma norms (for the adjoint)
+    // the last GLS_GRAPH batch: its signature and executable graph
+    std::vector<uint64_t> graph_key;
+    cudaGraphExec_t graph_exec = nullptr;
     // adjoint scratch (gls_demosaic_denoise_vjp)
     DevBuf adj_gden[2], adj_rec, adj_glayer, adj_gpca, adj_gup, adj_part, adj_loss, adj_target;
 };
@@ -679,6 +683,72 @@ static gls_status adjoint_run(gls_converter* cv, const gls_demosaic_params* p, c
 
 }  // namespace gls
 
+namespace gls {
+
+// Signature of a batch for graph replay: pointers, sizes, strides, output
+// views, flags and the bytes of every parameter block (kernel arguments are
+// baked into the graph). Empty when an output is converter-owned.
+static std::vector<uint64_t> batch_key(const gls_frame_desc* frames, int n, uint32_t flags) {
+    std::vector<uint64_t> k;
+    k.push_back(uint64_t(n));
+    k.push_back(flags);
+    for (int i = 0; i < n; i++) {
+        const gls_frame_desc& f = frames[i];
+        if (!f.out.data) return {};
+        k.push_back(uint64_t(uintptr_t(f.raw)));
+        k.push_back((uint64_t(uint32_t(f.width)) << 32) | uint32_t(f.height));
+        k.push_back(f.raw_stride_bytes);
+        k.push_back(uint64_t(uintptr_t(f.out.data)));
+        k.push_back((uint64_t(uint32_t(f.out.dtype)) << 32) | uint32_t(f.out.channels));
+        k.push_back(f.out.stride_bytes);
+        uint64_t h = 1469598103934665603ull;  // FNV-1a over the parameter block
+        const unsigned char* b = reinterpret_cast<const unsigned char*>(f.params);
+        for (size_t j = 0; j < sizeof(gls_demosaic_params); j++) h = (h ^ b[j]) * 1099511628211ull;
+        k.push_back(h);
+    }
+    return k;
+}
+
+// Frames to slot streams, largest first onto the least-loaded slot (the
+// longest-processing-time rule), then the fork / per-slot runs / join on s.
+static gls_status enqueue_batch(gls_converter* conv, gls_frame_desc* frames, int n, uint32_t flags, cudaStream_t s) {
+    const int nslots = n < kSlots ? n : kSlots;
+    std::vector<int> order(n), slot_of(n);
+    for (int i = 0; i < n; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return size_t(frames[a].width) * frames[a].height > size_t(frames[b].width) * frames[b].height;
+    });
+    std::vector<size_t> load(nslots, 0);
+    for (int i : order) {
+        int k = 0;
+        for (int j = 1; j < nslots; j++)
+            if (load[j] < load[k]) k = j;
+        slot_of[i] = k;
+        load[k] += size_t(frames[i].width) * frames[i].height;
+    }
+    GLS_CUDA(cudaEventRecord(conv->fork_ev, s));
+    for (int k = 0; k < nslots; k++) GLS_CUDA(cudaStreamWaitEvent(conv->slot_stream[k], conv->fork_ev, 0));
+    gls_status result = GLS_OK;
+    for (int oi = 0; oi < n && result == GLS_OK; oi++) {
+        const int i = order[oi];
+        gls_frame_desc& f = frames[i];
+        const int k = slot_of[i];
+        result = (flags & GLS_FP16_STORAGE)
+                     ? demosaic_run<__half>(conv, f.raw, f.width, f.height, f.raw_stride_bytes, f.params, flags,
+                                            &f.out, conv->slot_stream[k], k)
+                     : demosaic_run<float>(conv, f.raw, f.width, f.height, f.raw_stride_bytes, f.params, flags,
+                                           &f.out, conv->slot_stream[k], k);
+    }
+    // join (also on error, so the caller's stream orders after whatever was queued)
+    for (int k = 0; k < nslots; k++) {
+        GLS_CUDA(cudaEventRecord(conv->join_ev[k], conv->slot_stream[k]));
+        GLS_CUDA(cudaStreamWaitEvent(s, conv->join_ev[k], 0));
+    }
+    return result;
+}
+
+}  // namespace gls
+
 extern "C" {
 
 const char* gls_last_error_message(void) { return g_last_error.c_str(); }
@@ -719,6 +789,7 @@ gls_status gls_converter_destroy(gls_converter* conv) {
         if (conv->join_ev[k]) cudaEventDestroy(conv->join_ev[k]);
     }
     if (conv->fork_ev) cudaEventDestroy(conv->fork_ev);
+    if (conv->graph_exec) cudaGraphExecDestroy(conv->graph_exec);
     for (DevBuf* b : {&conv->adj_gden[0], &conv->adj_gden[1], &conv->adj_rec, &conv->adj_glayer, &conv->adj_gpca,
                       &conv->adj_gup, &conv->adj_part, &conv->adj_loss, &conv->adj_target})
         b->release();
@@ -776,7 +847,6 @@ gls_status gls_demosaic_batch(gls_converter* conv, gls_frame_desc* frames, int32
         if (flags & (GLS_SYNC | GLS_HOST_IO)) GLS_CUDA(cudaStreamSynchronize(s));
         return GLS_OK;
     }
-    // fork: every slot stream waits for the work already queued on `s`
     if (!conv->fork_ev) {
         GLS_CUDA(cudaEventCreateWithFlags(&conv->fork_ev, cudaEventDisableTiming));
         for (int k = 0; k < kSlots; k++) {
@@ -784,24 +854,43 @@ gls_status gls_demosaic_batch(gls_converter* conv, gls_frame_desc* frames, int32
             GLS_CUDA(cudaEventCreateWithFlags(&conv->join_ev[k], cudaEventDisableTiming));
         }
     }
-    const int nslots = n_frames < kSlots ? n_frames : kSlots;
-    GLS_CUDA(cudaEventRecord(conv->fork_ev, s));
-    for (int k = 0; k < nslots; k++) GLS_CUDA(cudaStreamWaitEvent(conv->slot_stream[k], conv->fork_ev, 0));
-    // frame i runs on slot i % nslots, in order within a slot
-    gls_status result = GLS_OK;
-    for (int i = 0; i < n_frames && result == GLS_OK; i++) {
-        gls_frame_desc& f = frames[i];
-        const int k = i % nslots;
-        result = (flags & GLS_FP16_STORAGE)
-                     ? demosaic_run<__half>(conv, f.raw, f.width, f.height, f.raw_stride_bytes, f.params,
-                                            flags & ~GLS_SYNC, &f.out, conv->slot_stream[k], k)
-                     : demosaic_run<float>(conv, f.raw, f.width, f.height, f.raw_stride_bytes, f.params,
-                                           flags & ~GLS_SYNC, &f.out, conv->slot_stream[k], k);
+    const bool graph = flags & GLS_GRAPH;
+    std::vector<uint64_t> key;
+    if (graph) {
+        if (flags & (GLS_HOST_IO | GLS_HOST_PCA))
+            return set_error(GLS_ERR_INVALID_ARG, "GLS_GRAPH needs device buffers and the device PCA");
+        if (!s) return set_error(GLS_ERR_INVALID_ARG, "GLS_GRAPH needs a stream other than the legacy default stream");
+        if (conv->prof.on) return set_error(GLS_ERR_INVALID_ARG, "GLS_GRAPH cannot run with profiling enabled");
+        key = batch_key(frames, n_frames, flags);
+        if (!key.empty() && conv->graph_exec && key == conv->graph_key) {  // replay
+            GLS_CUDA(cudaGraphLaunch(conv->graph_exec, s));
+            if (flags & GLS_SYNC) GLS_CUDA(cudaStreamSynchronize(s));
+            return GLS_OK;
+        }
+        if (key.empty()) return set_error(GLS_ERR_INVALID_ARG, "GLS_GRAPH needs caller-owned outputs");
     }
-    // join (also on error, so the caller's stream orders after whatever was queued)
-    for (int k = 0; k < nslots; k++) {
-        GLS_CUDA(cudaEventRecord(conv->join_ev[k], conv->slot_stream[k]));
-        GLS_CUDA(cudaStreamWaitEvent(s, conv->join_ev[k], 0));
+    gls_status result = enqueue_batch(conv, frames, n_frames, flags & ~(GLS_SYNC | GLS_GRAPH), s);
+    if (result == GLS_OK && graph) {
+        // record the same launch sequence (allocations and one-time set-up
+        // are done by the run above) for replays of this batch
+        GLS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+        const gls_status cap = enqueue_batch(conv, frames, n_frames, flags & ~(GLS_SYNC | GLS_GRAPH), s);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(s, &g);
+        if (cap != GLS_OK) {
+            if (g) cudaGraphDestroy(g);
+            return cap;
+        }
+        if (e != cudaSuccess) return set_error(GLS_ERR_CUDA, "batch capture: %s", cudaGetErrorString(e));
+        if (conv->graph_exec) cudaGraphExecDestroy(conv->graph_exec);
+        conv->graph_exec = nullptr;
+        const cudaError_t ie = cudaGraphInstantiate(&conv->graph_exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) {
+            conv->graph_exec = nullptr;
+            return set_error(GLS_ERR_CUDA, "batch graph instantiation: %s", cudaGetErrorString(ie));
+        }
+        conv->graph_key = key;
     }
     if (result != GLS_OK) return result;
     if (flags & (GLS_SYNC | GLS_HOST_IO)) GLS_CUDA(cudaStreamSynchronize(s));

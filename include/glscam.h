@@ -114,7 +114,9 @@ enum {
     GLS_FP16_STORAGE = 1u << 2,  /* FP16 planes + fused kernels + device PCA (the batched path) */
     GLS_HOST_IO = 1u << 3,       /* raw input and caller output buffers are host memory */
     GLS_SYNC = 1u << 4,          /* block until the stream has finished (the reference is synchronous) */
-    GLS_HOST_PCA = 1u << 5       /* per-level PCA eigen-solve on the host, as the reference does */
+    GLS_HOST_PCA = 1u << 5,      /* per-level PCA eigen-solve on the host, as the reference does */
+    GLS_GRAPH = 1u << 6          /* gls_demosaic_batch: record the batch as one CUDA graph and replay it while
+                                    the batch (pointers, sizes, strides, parameter bytes) stays the same */
 };
 
 /* Planes a converter exposes after gls_demosaic, for stage checks. */
@@ -164,7 +166,13 @@ typedef struct gls_frame_desc {
 } gls_frame_desc;
 
 /* Batched RawConverter::demosaic over frames of uneven sizes (no reference
- * counterpart: the reference converts one frame per call). */
+ * counterpart: the reference converts one frame per call). Frames are
+ * spread over the converter's slot streams, largest first onto the
+ * least-loaded slot. With GLS_GRAPH (device buffers, caller-owned outputs,
+ * device PCA, a non-default stream, at least 2 frames) the first call runs
+ * the batch and records its launch sequence as a CUDA graph; later calls
+ * with the same frames, buffers and parameter values replay that graph in
+ * one launch. */
 gls_status gls_demosaic_batch(gls_converter* conv, gls_frame_desc* frames, int32_t n_frames,
                               uint32_t flags, void* stream);
 
