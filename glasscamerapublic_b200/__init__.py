@@ -141,6 +141,7 @@ _SIGNATURES = {
     "gls_converter_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
     "gls_converter_stats": (C.c_int, [C.c_void_p, C.POINTER(KernelStat), C.c_int32, C.POINTER(C.c_int32)]),
     "gls_converter_reset_stats": (C.c_int, [C.c_void_p]),
+    "gls_block_match_tiles": (C.c_int, [C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)]),
     "gls_calibration_fill": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(DemosaicParams)]),
     "gls_gaussian_bilinear_taps": (C.c_int, [C.c_float, C.POINTER(C.c_float), C.c_int32, C.POINTER(C.c_int32)]),
     "gls_demosaic_denoise_vjp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_size_t,
@@ -199,6 +200,14 @@ def check(code: int) -> None:
 
 def exported_symbols() -> list[str]:
     return list(_SIGNATURES)
+
+
+def block_match_tiles() -> list:
+    """The FP16 block matcher's autotuned tile heights: [(w, h, height)]."""
+    buf = (C.c_int32 * 192)()
+    n = C.c_int32(0)
+    check(lib().gls_block_match_tiles(buf, 64, C.byref(n)))
+    return [(buf[3 * i], buf[3 * i + 1], buf[3 * i + 2]) for i in range(min(n.value, 64))]
 
 
 from .api import CameraCalibration, iPhone14WideCalibration, RawConverter, PyramidProcessor  # noqa: E402

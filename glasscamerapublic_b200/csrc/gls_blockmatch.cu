@@ -15,6 +15,10 @@
 // shared-memory operations per tap.
 #include <cmath>
 
+#include <cstdlib>
+#include <map>
+#include <mutex>
+
 #include "gls_common.cuh"
 #include "gls_kernels.h"
 
@@ -189,7 +193,15 @@ __global__ void __launch_bounds__(256) k_block_match_plain(Plane<S, 4> img, Plan
 //     is sw / sqrt(2 log2 e) times it;
 //   * both exponentials are ex2.approx (the reference uses half-precision
 //     exp under fast math here).
-constexpr int BX_NP = 4, BX_TX = 32, BX_TY = 8, BX_W = BX_TX + 20, BX_H = BX_NP * BX_TY + 20;
+constexpr int BX_NP = 4, BX_TX = 32, BX_W = BX_TX + 20;
+// tile height variants (TY threads down, 4 pixels each): 32 x 32 or 32 x 16
+// pixels; the autotuner picks one per level size (launch_block_match)
+template <int TY>
+struct BxTile {
+    static constexpr int H = BX_NP * TY + 20;  // window rows staged
+    static constexpr int LH = H + 4;           // luma rows staged
+    static constexpr int THREADS = BX_TX * TY;
+};
 
 // ---------------------------------------------------------------- FFMA2 form
 // The four pixels of a thread are taken as two pairs, (p0, p1) and
@@ -222,9 +234,10 @@ __device__ __forceinline__ u64 add2(u64 a, u64 b) {
     return d;
 }
 
+template <int TY>
 struct BmPairSmem {
-    uint4 pca[BX_H * BX_W];   // q - c, 8 halves
-    float4 ycc[BX_H * BX_W];  // Y, Cb, Cr, |q - c|^2
+    uint4 pca[BxTile<TY>::H * BX_W];   // q - c, 8 halves
+    float4 ycc[BxTile<TY>::H * BX_W];  // Y, Cb, Cr, |q - c|^2
     float4 sp[22 * 21];       // (sw(j)/sqrt(lk), sw(j-1)/sqrt(lk), -log2 sw(j), -log2 sw(j-1)), j = table row
 };
 
@@ -234,8 +247,8 @@ struct BmPair {  // two pixels, each member of a pair register = one pixel
     u64 c1, c2, no1, no2; // chroma: e = c * v - o  (no = -o)
 };
 
-template <bool A, bool B>
-__device__ __forceinline__ void bmp2_row(const BmPairSmem& sm, int base, int r, const BmPair& pa, const BmPair& pb,
+template <bool A, bool B, class Sm>
+__device__ __forceinline__ void bmp2_row(const Sm& sm, int base, int r, const BmPair& pa, const BmPair& pb,
                                          u64 (&acc)[2][5]) {
 #pragma unroll 7
     for (int i = 0; i < 21; i++) {
@@ -281,41 +294,45 @@ __device__ __forceinline__ void bmp2_row(const BmPairSmem& sm, int base, int r, 
 // tensor-core MMAs (mma.sync m16n8k16, FP32 accumulate). 52 x 52 = 2704
 // positions = 169 chunks of 16 rows; K = 25 padded to 32 (two k-steps);
 // N = the 8 components. The luma tile (window region + 2) is staged once.
-constexpr int BX_LW = BX_W + 4, BX_LH = BX_H + 4;  // luma tile, origin (x0 - 12, y0 - 12)
+constexpr int BX_LW = BX_W + 4;  // luma tile width, origin (x0 - 12, y0 - 12)
 
 __device__ __forceinline__ uint32_t h2u(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
 
-__global__ void __launch_bounds__(256, 2) k_block_match_pair(Plane<__half, 4> img, Plane<__half, 2> grad,
-                                                             const float* __restrict__ basis, Plane<__half, 4> out,
-                                                             BlockMatchArgs a) {
+template <int TY>
+__global__ void __launch_bounds__(BxTile<TY>::THREADS, TY == 8 ? 2 : 3)
+    k_block_match_pair(Plane<__half, 4> img, Plane<__half, 2> grad, const float* __restrict__ basis,
+                       Plane<__half, 4> out, BlockMatchArgs a) {
+    using T = BxTile<TY>;
+    constexpr int BX_H = T::H, BX_LH = T::LH, NT = T::THREADS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    BmPairSmem& sm = *reinterpret_cast<BmPairSmem*>(smem_raw);
-    __half* luma = reinterpret_cast<__half*>(smem_raw + sizeof(BmPairSmem));  // BX_LH x BX_LW
+    BmPairSmem<TY>& sm = *reinterpret_cast<BmPairSmem<TY>*>(smem_raw);
+    __half* luma = reinterpret_cast<__half*>(smem_raw + sizeof(BmPairSmem<TY>));  // BX_LH x BX_LW
     __shared__ float cen[8];
     __shared__ float bsm[25][8];
-    const int x0 = blockIdx.x * BX_TX, y0 = blockIdx.y * (BX_NP * BX_TY);
+    const int x0 = blockIdx.x * BX_TX, y0 = blockIdx.y * (BX_NP * TY);
     const int tid = threadIdx.y * BX_TX + threadIdx.x;
     const float kLog2e = 1.4426950408889634f, lk = 2.f * kLog2e, isq = rsqrtf(lk);
-    for (int k = tid; k < 22 * 21; k += 256) {
+    for (int k = tid; k < 22 * 21; k += NT) {
         const int j = k / 21, i = k % 21 - 10;
         // window row j of the pair's first pixel, j - 1 of its second
         const float w0 = j <= 20 ? spatial_weight(i, j - 10) : 0.f;
         const float w1 = j >= 1 ? spatial_weight(i, j - 11) : 0.f;
         sm.sp[k] = make_float4(w0 * isq, w1 * isq, -log2f(w0), -log2f(w1));
     }
-    if (tid < 200) bsm[tid / 8][tid % 8] = basis[tid];
-    for (int k = tid; k < BX_LW * BX_LH; k += 256) {
+    for (int k = tid; k < 200; k += NT) bsm[k / 8][k % 8] = basis[k];
+    for (int k = tid; k < BX_LW * BX_LH; k += NT) {
         const int ty = k / BX_LW, tx = k % BX_LW;
         luma[k] = *img.pxc(x0 - 12 + tx, y0 - 12 + ty);
     }
-    for (int k = tid; k < BX_W * BX_H; k += 256) {
+    for (int k = tid; k < BX_W * BX_H; k += NT) {
         const int ty = k / BX_W, tx = k % BX_W;
         const f4 p = ld4<__half>(img.pxc(x0 - 10 + tx, y0 - 10 + ty));
         sm.ycc[k] = make_float4(p.x, p.y, p.z, 0.f);
     }
     __syncthreads();
-    if (tid < 8) {  // centring vector: the tile-centre pixel's coefficients (FP32)
-        const int cx = BX_TX / 2 + 12, cy = BX_NP * BX_TY / 2 + 12;  // luma-tile coordinates
+    if (tid < 8) {  // centring vector: the coefficients (FP32) of the centre pixel of the
+                    // enclosing 32 x 32 tile, so that both tile heights centre and round alike
+        const int cx = BX_TX / 2 + 12, cy = 16 + 12 - (y0 % 32);  // luma-tile coordinates
         float c = 0.f;
         for (int k = 0; k < 25; k++) c += bsm[k][tid] * __half2float(luma[(cy + k / 5 - 2) * BX_LW + cx + k % 5 - 2]);
         cen[tid] = c;
@@ -332,7 +349,7 @@ __global__ void __launch_bounds__(256, 2) k_block_match_pair(Plane<__half, 4> im
     }
     __syncthreads();
     uint32_t* pca32 = reinterpret_cast<uint32_t*>(sm.pca);  // [position][4] half2
-    for (int ch = warp; ch < (BX_W * BX_H) / 16; ch += 8) {
+    for (int ch = warp; ch < (BX_W * BX_H) / 16; ch += TY) {
         const int m0 = ch * 16 + g, m1 = m0 + 8;  // the two rows of this thread
         // patch centre in the luma tile: the clamped image position of the
         // window position, as a clamped read of a projected plane would see
@@ -439,19 +456,89 @@ __global__ void __launch_bounds__(256, 2) k_block_match_pair(Plane<__half, 4> im
     }
 }
 
+
+template <int TY>
+static void launch_pair(Plane<__half, 4> img, Plane<__half, 2> grad, const float* basis, Plane<__half, 4> out,
+                        const BlockMatchArgs& a, cudaStream_t s) {
+    const size_t smem = sizeof(BmPairSmem<TY>) + sizeof(__half) * BX_LW * BxTile<TY>::LH;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_block_match_pair<TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        attr = true;
+    }
+    dim3 b(BX_TX, TY);
+    dim3 g((img.w + BX_TX - 1) / BX_TX, (img.h + BX_NP * TY - 1) / (BX_NP * TY));
+    k_block_match_pair<TY><<<g, b, smem, s>>>(img, grad, basis, out, a);
+}
+
+// Tile-height autotuner of the FP16 block matcher. Both heights compute
+// identical results (the same per-pixel arithmetic and the same centring),
+// so the choice only changes speed: 32 x 32 tiles amortise the staged halo
+// better, 32 x 16 tiles fill the GPU on small pyramid levels. The first call
+// for a level size times both on the caller's stream (leaving the result in
+// `out`) and keeps the faster; later calls reuse the choice, and so do calls
+// made while the stream is being captured into a graph (default 32 x 32 for
+// a size not timed yet). GLS_BM_TILE=8 or 4 in the environment fixes the
+// height.
+static std::mutex g_tile_mu;
+static std::map<std::pair<int, int>, int> g_tile_choice;
+
+int bm_tile_list(int* whty, int max) {
+    std::lock_guard<std::mutex> lk(g_tile_mu);
+    int n = 0;
+    for (const auto& kv : g_tile_choice) {
+        if (n < max) {
+            whty[3 * n] = kv.first.first;
+            whty[3 * n + 1] = kv.first.second;
+            whty[3 * n + 2] = kv.second;
+        }
+        n++;
+    }
+    return n;
+}
+
+template <class Run>
+static int bm_tile_height(int w, int h, Run&& run_variant, cudaStream_t s) {
+    static const int forced = [] {
+        const char* e = std::getenv("GLS_BM_TILE");
+        return e ? std::atoi(e) : 0;
+    }();
+    if (forced == 4 || forced == 8) return forced;
+    {
+        std::lock_guard<std::mutex> lk(g_tile_mu);
+        auto it = g_tile_choice.find({w, h});
+        if (it != g_tile_choice.end()) return it->second;
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return 8;
+    cudaEvent_t e[3];
+    for (auto& ev : e) cudaEventCreate(&ev);
+    cudaEventRecord(e[0], s);
+    run_variant(8);
+    cudaEventRecord(e[1], s);
+    run_variant(4);
+    cudaEventRecord(e[2], s);
+    float t8 = 0.f, t4 = 0.f;
+    int choice = 8;
+    if (cudaEventSynchronize(e[2]) == cudaSuccess && cudaEventElapsedTime(&t8, e[0], e[1]) == cudaSuccess &&
+        cudaEventElapsedTime(&t4, e[1], e[2]) == cudaSuccess)
+        choice = t4 < t8 ? 4 : 8;
+    for (auto& ev : e) cudaEventDestroy(ev);
+    std::lock_guard<std::mutex> lk(g_tile_mu);
+    g_tile_choice[{w, h}] = choice;
+    return 0;  // `out` already holds the result
+}
+
 template <class S>
 void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, const float* basis, Plane<S, 4> out,
                         const BlockMatchArgs& a, cudaStream_t s) {
     if constexpr (is_half<S>::value) {
-        const size_t smem = sizeof(BmPairSmem) + sizeof(__half) * BX_LW * BX_LH;
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(k_block_match_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-            attr = true;
-        }
-        dim3 b(BX_TX, BX_TY);
-        dim3 g((img.w + BX_TX - 1) / BX_TX, (img.h + BX_NP * BX_TY - 1) / (BX_NP * BX_TY));
-        k_block_match_pair<<<g, b, smem, s>>>(img, grad, basis, out, a);
+        const int ty = bm_tile_height(img.w, img.h, [&](int t) {
+            if (t == 8) launch_pair<8>(img, grad, basis, out, a, s);
+            else launch_pair<4>(img, grad, basis, out, a, s);
+        }, s);
+        if (ty == 8) launch_pair<8>(img, grad, basis, out, a, s);
+        else if (ty == 4) launch_pair<4>(img, grad, basis, out, a, s);
     } else {
         static bool attr = false;
         if (!attr) {

@@ -1069,4 +1069,14 @@ gls_status gls_demosaic_denoise_vjp(gls_converter* conv, const uint16_t* raw, in
     return adjoint_run(conv, params, tp, target->channels, loss, grad, s);
 }
 
+
+gls_status gls_block_match_tiles(int32_t* entries, int32_t max_entries, int32_t* n) {
+    clear_error();
+    if (!n || (max_entries > 0 && !entries)) return set_error(GLS_ERR_INVALID_ARG, "NULL argument");
+    std::vector<int> buf(3 * size_t(std::max(max_entries, 0)));
+    const int c = bm_tile_list(buf.data(), std::max(max_entries, 0));
+    for (int i = 0; i < std::min(c, max_entries) * 3; i++) entries[i] = buf[i];
+    *n = c;
+    return GLS_OK;
+}
 }  // extern "C"

@@ -103,6 +103,10 @@ template <class S>
 void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, const float* basis, Plane<S, 4> out,
                         const BlockMatchArgs& a, cudaStream_t s);
 
+// the FP16 block matcher's tile-height autotuner decisions: (w, h, height)
+// triples of the level sizes seen so far; returns their count
+int bm_tile_list(int* whty, int max);
+
 // ---- adjoint of the pyramid (gls_adjoint.cu); FP32 planes, tightly packed
 struct AdjointLevelArgs {
     int w, h;

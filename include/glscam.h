@@ -229,6 +229,15 @@ gls_status gls_converter_set_profiling(gls_converter* conv, int32_t enable);
 gls_status gls_converter_stats(gls_converter* conv, gls_kernel_stat* stats, int32_t max_stats, int32_t* n_stats);
 gls_status gls_converter_reset_stats(gls_converter* conv);
 
+/* Decisions of the FP16 block matcher's tile autotuner (no reference
+ * counterpart): for each pyramid level size met so far in this process,
+ * (width, height, tile height in threads: 8 = 32x32-pixel tiles, 4 = 32x16).
+ * The first frame of a size times both heights and keeps the faster; both
+ * compute identical results. Writes at most max_entries triples to
+ * entries; *n receives the count. GLS_BM_TILE=8 or 4 in the environment
+ * fixes the height. */
+gls_status gls_block_match_tiles(int32_t* entries, int32_t max_entries, int32_t* n);
+
 /* ---- CameraCalibration<levels> (CameraCalibration.hpp:24-39) ----
  * Fills the noise model and the denoise schedule of a built-in camera for
  * an ISO, as nlfFromIso() + getDenoiseParameters() do. Returns GLS_ERR_RANGE

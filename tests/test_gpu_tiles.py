@@ -1,0 +1,69 @@
+"""The FP16 block matcher's tile-height autotuner: 32 x 32 and 32 x 16 pixel
+tiles compute the same bits (same per-pixel arithmetic, same centring
+vector), so forcing either height through GLS_BM_TILE, or letting the
+autotuner choose, gives identical frames. Each setting runs in its own
+process because the height is read once per process."""
+import json
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = Path(__file__).resolve().parents[1]
+
+_SCRIPT = r"""
+import json, sys
+import numpy as np, torch
+import glasscamerapublic_b200 as g
+from glasscamerapublic_b200 import RawConverter, scene
+sizes = [(640, 480), (336, 250), (1000, 744)]
+c = RawConverter(0)
+st = torch.cuda.Stream()
+raws, params, outs = [], [], []
+for k, (w, h) in enumerate(sizes):
+    wl = scene.Workload(f"t{k}", w, h, levels=5, gain=1.2 + 0.4 * k, read=3.0 + k, iso=800 * (k + 1), seed=70 + k)
+    raw, _ = scene.make_raw(wl)
+    raws.append(torch.from_numpy(raw.view(np.int16)).cuda())
+    params.append(scene.make_params(wl))
+    outs.append(torch.empty((h, w, 4), dtype=torch.float16, device="cuda"))
+for rep in range(2):  # the second call reuses the chosen heights
+    c.demosaic_batch(raws, params, outs, stream=st)
+    st.synchronize()
+    res = [o.cpu().numpy().view(np.uint16) for o in outs]
+    np.savez(sys.argv[1] + f"_{rep}.npz", *res)
+json.dump(g.block_match_tiles(), open(sys.argv[1] + ".json", "w"))
+c.close()
+"""
+
+
+def _run(tmp_path, tag, tile):
+    env = dict(os.environ)
+    env.pop("GLS_BM_TILE", None)
+    if tile:
+        env["GLS_BM_TILE"] = str(tile)
+    base = str(tmp_path / tag)
+    subprocess.run([sys.executable, "-c", _SCRIPT, base], cwd=ROOT, env=env, check=True, timeout=300)
+    frames = []
+    for rep in range(2):
+        with np.load(base + f"_{rep}.npz") as z:
+            frames.append([z[k] for k in sorted(z.files, key=lambda s: int(s.split("_")[1]))])
+    return frames, json.load(open(base + ".json"))
+
+
+def test_tile_heights_are_bit_identical(tmp_path):
+    f8, _ = _run(tmp_path, "h8", 8)
+    f4, _ = _run(tmp_path, "h4", 4)
+    fa, tiles = _run(tmp_path, "auto", None)
+    for rep in range(2):
+        for a, b, c in zip(f8[rep], f4[rep], fa[rep]):
+            assert np.array_equal(a, b)
+            assert np.array_equal(a, c)
+    # the autotuner timed every FP16 pyramid level size it met
+    assert tiles and all(t[2] in (4, 8) for t in tiles)
+    sizes = {(t[0], t[1]) for t in tiles}
+    assert (640, 480) in sizes and (320, 240) in sizes
