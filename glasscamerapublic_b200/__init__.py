@@ -35,6 +35,7 @@ FP16_STORAGE = 1 << 2
 HOST_IO = 1 << 3
 SYNC = 1 << 4
 GRAPH = 1 << 6
+SURF_CORRECTED = 1 << 7
 HOST_PCA = 1 << 5
 
 PLANE_SCALED_RAW = 0

@@ -96,6 +96,7 @@ struct DetectArgs {
     const float* sum;
     int sum_pitch;  // floats
     float threshold;
+    int per_axis;  // corrected interpolation (else the reference's scale-offset broadcast)
     gls_keypoint* cand;
     int* cand_count;
 };
@@ -256,10 +257,14 @@ __global__ void __launch_bounds__(256) k_hessian_nms(DetectArgs a) {
         const float A0[3] = {dxx, dxy, dxs}, A1[3] = {dxy, dyy, dys}, A2[3] = {dxs, dys, dss};
         float X[3] = {0.0f, 0.0f, 0.0f};
         const float dt = det3(A0, A1, A2);
-        if (dt != 0.0f) {
-            X[0] = fdiv(det3(B, A1, A2), dt);
-            X[1] = fdiv(det3(A0, B, A2), dt);
+        if (dt != 0.0f) {  // solve3x3 (SURF.metal:189-205)
             X[2] = fdiv(det3(A0, A1, B), dt);
+            if (a.per_axis) {
+                X[0] = fdiv(det3(B, A1, A2), dt);
+                X[1] = fdiv(det3(A0, B, A2), dt);
+            } else {  // `(float3)(a, b, c) / det` is float3(c) / det: the scale offset in every lane
+                X[0] = X[1] = X[2];
+            }
         }
         const bool all_zero = X[0] == 0.0f && X[1] == 0.0f && X[2] == 0.0f;
         if (all_zero || !(fabsf(X[0]) <= 1.0f && fabsf(X[1]) <= 1.0f && fabsf(X[2]) <= 1.0f)) continue;
@@ -353,6 +358,7 @@ struct DescArgs {
     gls_keypoint* kps;
     const int* count;
     float* desc;
+    int all;  // describe every keypoint (else the reference's ranges, SURF.cpp:681-693)
 };
 
 constexpr int kDescThreads = 128;
@@ -365,7 +371,16 @@ constexpr int kMaxWinIdx = 42;  // rows / columns of the window resizeVV reads
 // patch, 20 x 20 gradients and the 4 x 4 x 4 descriptor.
 __global__ void __launch_bounds__(kDescThreads) k_describe(DescArgs a) {
     const int k = blockIdx.x;
-    if (k >= *a.count) return;
+    const int n = *a.count;
+    if (k >= n) return;
+    // SURFInvoker::run cuts K > 32 keypoints into ceil(K/8) ranges of
+    // ceil(K/8): the first min(K, ceil(K/8)^2) are described, the others keep
+    // angle -1 and a zero descriptor
+    const int r8 = (n + 7) / 8;
+    if (!a.all && n > 32 && k >= r8 * r8) {
+        for (int i = threadIdx.x; i < 64; i += blockDim.x) a.desc[size_t(k) * 64 + i] = 0.0f;
+        return;
+    }
     __shared__ float X[169], Y[169], ANG[169];
     __shared__ int pos[169];
     __shared__ float bx_s[72], by_s[72], mod_s[72];
@@ -1623,6 +1638,7 @@ gls_status gls_surf_detect_and_compute(gls_surf* s, const gls_image_view* img, i
     da.sum = S;
     da.sum_pitch = W + 1;
     da.threshold = s->threshold;
+    da.per_axis = (flags & GLS_SURF_CORRECTED) ? 1 : 0;
     da.cand = reinterpret_cast<gls_keypoint*>(s->cand.p);
     da.cand_count = reinterpret_cast<int*>(s->cand_count.p);
     int blocks = 0;
@@ -1659,6 +1675,7 @@ gls_status gls_surf_detect_and_compute(gls_surf* s, const gls_image_view* img, i
     ga.kps = reinterpret_cast<gls_keypoint*>(sl.kps.p);
     ga.count = reinterpret_cast<const int*>(sl.count.p);
     ga.desc = reinterpret_cast<float*>(sl.desc.p);
+    ga.all = (flags & GLS_SURF_CORRECTED) ? 1 : 0;
     if (keep > 0) {
         k_describe<<<keep, kDescThreads, 0, st>>>(ga);
         GLS_TRY(launch_check(s, "k_describe"));

@@ -13,7 +13,7 @@ import ctypes as C
 
 import numpy as np
 
-from . import F16, F32, HOST_IO, KEYPOINT_DTYPE, MATCH_DTYPE, SYNC, ImageView, check, lib
+from . import F16, F32, HOST_IO, KEYPOINT_DTYPE, MATCH_DTYPE, SURF_CORRECTED, SYNC, ImageView, check, lib
 from .api import _is_torch, _ptr, _row_stride, _stream_handle
 
 SURF_SLOTS = 32
@@ -32,10 +32,17 @@ def _view(a, channels: int) -> ImageView:
 class SURF:
     """SURF::makeInstance(ctx, width, height, max_features, nOctaves,
     nOctaveLayers, hessianThreshold) (SURF.hpp:45-47). Results of
-    detectAndCompute stay on the GPU in one of SURF_SLOTS feature slots."""
+    detectAndCompute stay on the GPU in one of SURF_SLOTS feature slots.
+
+    The detector is the reference's, two defects included (the maxima
+    interpolation moves x, y and size by the scale offset, SURF.metal:200;
+    a set of 33..56 keypoints is only partly described, SURF.cpp:681-693).
+    corrected=True solves the interpolation per axis and describes every
+    keypoint (GLS_SURF_CORRECTED)."""
 
     def __init__(self, width: int, height: int, max_features: int = -1, nOctaves: int = 4, nOctaveLayers: int = 2,
-                 hessianThreshold: float = 0.02, device: int = 0):
+                 hessianThreshold: float = 0.02, device: int = 0, corrected: bool = False):
+        self._detect_flags = SURF_CORRECTED if corrected else 0
         h = C.c_void_p()
         check(lib().gls_surf_create(device, width, height, max_features, nOctaves, nOctaveLayers,
                                     float(hessianThreshold), C.byref(h)))
@@ -68,7 +75,7 @@ class SURF:
         """Detection + description of img (F32 H x W, numpy or CUDA tensor)
         into a slot, asynchronously for device input."""
         v = _view(img, 1)
-        flags = HOST_IO if isinstance(img, np.ndarray) else 0
+        flags = (HOST_IO if isinstance(img, np.ndarray) else 0) | self._detect_flags
         if sync:
             flags |= SYNC
         check(lib().gls_surf_detect_and_compute(self._h, C.byref(v), slot, flags, _stream_handle(stream)))

@@ -115,8 +115,9 @@ enum {
     GLS_HOST_IO = 1u << 3,       /* raw input and caller output buffers are host memory */
     GLS_SYNC = 1u << 4,          /* block until the stream has finished (the reference is synchronous) */
     GLS_HOST_PCA = 1u << 5,      /* per-level PCA eigen-solve on the host, as the reference does */
-    GLS_GRAPH = 1u << 6          /* gls_demosaic_batch: record the batch as one CUDA graph and replay it while
+    GLS_GRAPH = 1u << 6,         /* gls_demosaic_batch: record the batch as one CUDA graph and replay it while
                                     the batch (pointers, sizes, strides, parameter bytes) stays the same */
+    GLS_SURF_CORRECTED = 1u << 7 /* gls_surf_detect_and_compute: the corrected detector (see there) */
 };
 
 /* Planes a converter exposes after gls_demosaic, for stage checks. */
@@ -323,7 +324,14 @@ gls_status gls_surf_destroy(gls_surf* s);
  * max_features cut, orientation and 64-D descriptor, into feature slot
  * `slot`. img: F32, 1 channel, width x height, device memory or host
  * memory with GLS_HOST_IO. Asynchronous on `stream` unless GLS_SYNC or
- * GLS_HOST_IO. */
+ * GLS_HOST_IO.
+ * By default the reference's detector, two defects included: the maxima
+ * interpolation adds the scale offset to x, y and size alike (SURF.metal:200
+ * returns `(float3)(a, b, c) / det`, a C++ comma expression), and of K > 32
+ * keypoints only the first min(K, ceil(K/8)^2) are oriented and described
+ * (SURF.cpp:681-693; the others keep angle -1 and a zero descriptor).
+ * GLS_SURF_CORRECTED solves the interpolation per axis and describes every
+ * keypoint. */
 gls_status gls_surf_detect_and_compute(gls_surf* s, const gls_image_view* img, int32_t slot, uint32_t flags,
                                        void* stream);
 

@@ -184,9 +184,16 @@ class SURF {
         : max_features_(max_features) {
         check(gls_surf_create(device, width, height, max_features, nOctaves, nOctaveLayers, hessianThreshold, &s_));
     }
-    SURF(SURF&& o) noexcept : s_(o.s_), max_features_(o.max_features_), next_(o.next_) { o.s_ = nullptr; }
+    SURF(SURF&& o) noexcept : s_(o.s_), max_features_(o.max_features_), next_(o.next_), detect_flags_(o.detect_flags_) {
+        o.s_ = nullptr;
+    }
     SURF(const SURF&) = delete;
     ~SURF() { gls_surf_destroy(s_); }
+
+    // The reference's detector by default; true selects the corrected one
+    // (per-axis maxima interpolation, every keypoint described:
+    // GLS_SURF_CORRECTED).
+    void setCorrectedDetector(bool on) { detect_flags_ = on ? uint32_t(GLS_SURF_CORRECTED) : 0u; }
 
     // detectAndCompute (SURF.hpp:57-58): img is a width x height float
     // image (device memory, or host memory with host_input); keypoints and
@@ -197,7 +204,9 @@ class SURF {
         const int slot = next_;
         next_ = (next_ + 1) % GLS_SURF_SLOTS;
         ImageView v{const_cast<float*>(img), width, height, 1, GLS_F32, stride_bytes};
-        check(gls_surf_detect_and_compute(s_, &v, slot, host_input ? uint32_t(GLS_HOST_IO) : uint32_t(GLS_SYNC), stream));
+        check(gls_surf_detect_and_compute(s_, &v, slot,
+                                          (host_input ? uint32_t(GLS_HOST_IO) : uint32_t(GLS_SYNC)) | detect_flags_,
+                                          stream));
         const int cap = max_features_ >= 0 ? max_features_ : GLS_SURF_MAX_KEYPOINTS;
         keypoints->resize(size_t(cap));
         if (descriptors) descriptors->resize(size_t(cap) * 64);
@@ -259,6 +268,7 @@ class SURF {
     gls_surf* s_ = nullptr;
     int max_features_;
     int next_ = 0;
+    uint32_t detect_flags_ = 0;
 };
 
 // FindHomography (Homography.hpp:26-27) on host point pairs; the detector is

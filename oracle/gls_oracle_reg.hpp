@@ -249,6 +249,13 @@ struct SurfConfig {
     int n_octaves = 4, n_octave_layers = 2;
     float hessian_threshold = 0.02f;
     int max_features = 1500;
+    // false: the reference's detector. Its interpolation step
+    // (SURF.metal:200) returns `(float3)(a, b, c) / det`, which C++ (and
+    // Metal, a C++14 dialect) reads as a cast of the comma expression:
+    // float3(c) / det, the scale offset in all three lanes; and it describes
+    // only some keypoints of a small set (described_keypoints). true: the
+    // corrected detector, per-axis Cramer solve and every keypoint described.
+    bool per_axis_interp = false;
 };
 
 // fastHessianDetector (SURF.cpp:1229-1286) with calcDetAndTrace and
@@ -335,9 +342,13 @@ inline std::vector<KeyPoint> detect(const FImg& sum, int width, int height, cons
                     float X[3] = {0, 0, 0};
                     const float det = det3(A0, A1, A2);
                     if (det != 0.0f) {
-                        X[0] = fdiv(det3(B, A1, A2), det);
-                        X[1] = fdiv(det3(A0, B, A2), det);
                         X[2] = fdiv(det3(A0, A1, B), det);
+                        if (cfg.per_axis_interp) {
+                            X[0] = fdiv(det3(B, A1, A2), det);
+                            X[1] = fdiv(det3(A0, B, A2), det);
+                        } else {
+                            X[0] = X[1] = X[2];
+                        }
                     }
                     const bool all_zero = X[0] == 0.0f && X[1] == 0.0f && X[2] == 0.0f;
                     if (!all_zero && std::fabs(X[0]) <= 1.0f && std::fabs(X[1]) <= 1.0f && std::fabs(X[2]) <= 1.0f) {
@@ -546,6 +557,17 @@ inline void describe(const FImg& img, const FImg& sum, const DescriptorTables& T
     for (int k = 0; k < 64; k++) desc[k] = fmul(desc[k], scale);
 }
 
+// SURFInvoker::run (SURF.cpp:681-693): with more than 32 keypoints the
+// reference cuts them into ceil(K / 8) ranges of ceil(K / 8) keypoints, so
+// only the first min(K, ceil(K / 8)^2) are oriented and described; the
+// others keep angle -1 and an all-zero descriptor (K = 33..56 loses some).
+// With per_axis_interp (the corrected detector) every keypoint is.
+inline int described_keypoints(int k, bool all) {
+    if (all || k <= 32) return k;
+    const int r = (k + 7) / 8;
+    return std::min(k, r * r);
+}
+
 // detectAndCompute (SURF.cpp:1380-1450) with one section: integral,
 // detection, the max_features cut, orientation and descriptors.
 struct Features {
@@ -560,7 +582,8 @@ inline Features detect_and_compute(const FImg& img, const SurfConfig& cfg) {
     if (cfg.max_features >= 0 && int(f.kps.size()) > cfg.max_features) f.kps.resize(cfg.max_features);
     f.desc.assign(f.kps.size() * 64, 0.0f);
     const DescriptorTables T = descriptor_tables();
-    parallel_rows(int(f.kps.size()), [&](int k) { describe(img, sum, T, f.kps[k], &f.desc[size_t(k) * 64]); });
+    const int nd = described_keypoints(int(f.kps.size()), cfg.per_axis_interp);
+    parallel_rows(nd, [&](int k) { describe(img, sum, T, f.kps[k], &f.desc[size_t(k) * 64]); });
     return f;
 }
 

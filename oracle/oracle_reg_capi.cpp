@@ -36,7 +36,7 @@ int orc_reg_integral(const float* in, int w, int h, float* sum) {
 // detectAndCompute; returns the number of keypoints written (<= capacity)
 // and the total before the max_features cut in *n_found
 int orc_reg_detect(const float* in, int w, int h, int n_octaves, int n_layers, float threshold, int max_features,
-                   gls_keypoint* kps, float* desc, int capacity, int* n_found) {
+                   gls_keypoint* kps, float* desc, int capacity, int* n_found, int per_axis_interp) {
     FImg img(w, h);
     std::copy(in, in + size_t(w) * h, img.d.begin());
     SurfConfig cfg;
@@ -44,13 +44,15 @@ int orc_reg_detect(const float* in, int w, int h, int n_octaves, int n_layers, f
     cfg.n_octave_layers = n_layers;
     cfg.hessian_threshold = threshold;
     cfg.max_features = -1;
+    cfg.per_axis_interp = per_axis_interp != 0;
     const FImg sum = integral(img);
     std::vector<KeyPoint> all = detect(sum, w, h, cfg);
     if (n_found) *n_found = int(all.size());
     if (max_features >= 0 && int(all.size()) > max_features) all.resize(max_features);
     const DescriptorTables T = descriptor_tables();
     std::vector<float> d(all.size() * 64);
-    orc::parallel_rows(int(all.size()), [&](int k) { describe(img, sum, T, all[k], &d[size_t(k) * 64]); });
+    const int nd = described_keypoints(int(all.size()), cfg.per_axis_interp);
+    orc::parallel_rows(nd, [&](int k) { describe(img, sum, T, all[k], &d[size_t(k) * 64]); });
     const int n = std::min(int(all.size()), capacity);
     std::memcpy(kps, all.data(), size_t(n) * sizeof(KeyPoint));
     if (desc) std::copy(d.begin(), d.begin() + size_t(n) * 64, desc);

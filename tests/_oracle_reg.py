@@ -25,7 +25,8 @@ def lib() -> C.CDLL:
         L.orc_reg_raw_channel.argtypes = [vp, C.c_int, C.c_int, C.c_size_t, C.c_int, C.c_int, C.c_float, C.c_float,
                                           C.c_float, fp]
         L.orc_reg_integral.argtypes = [fp, C.c_int, C.c_int, fp]
-        L.orc_reg_detect.argtypes = [fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, vp, fp, C.c_int, ip]
+        L.orc_reg_detect.argtypes = [fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, vp, fp, C.c_int, ip,
+                                     C.c_int]
         L.orc_reg_describe.argtypes = [fp, C.c_int, C.c_int, vp, C.c_int, fp]
         L.orc_reg_match.argtypes = [fp, C.c_int, fp, C.c_int, vp]
         L.orc_reg_ls_homography.argtypes = [fp, fp, C.c_int, fp]
@@ -73,14 +74,14 @@ def integral(img):
     return out
 
 
-def detect(img, n_octaves=4, n_layers=2, threshold=0.02, max_features=1500, capacity=70000):
+def detect(img, n_octaves=4, n_layers=2, threshold=0.02, max_features=1500, capacity=70000, per_axis=False):
     img = _f32(img)
     h, w = img.shape
     kps = np.zeros(capacity, KEYPOINT_DTYPE)
     desc = np.zeros((capacity, 64), np.float32)
     found = C.c_int(0)
     n = lib().orc_reg_detect(_fp(img), w, h, n_octaves, n_layers, threshold, max_features, kps.ctypes.data,
-                             _fp(desc), capacity, C.byref(found))
+                             _fp(desc), capacity, C.byref(found), 1 if per_axis else 0)
     return kps[:n].copy(), desc[:n].copy(), found.value
 
 

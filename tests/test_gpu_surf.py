@@ -100,6 +100,37 @@ def test_detect_and_compute_bit_exact(max_features, seed):
         s.close()
 
 
+def test_reference_detector_leaves_the_undescribed_tail():
+    # 45 keypoints: the reference's SURFInvoker::run describes the first 36
+    raw, img = _gray(seed=3)
+    h, w = img.shape
+    s = SURF(w, h, max_features=-1)
+    try:
+        kps, desc = s.detectAndCompute(img, slot=0)
+        assert len(kps) == 45
+        assert np.all(kps["angle"][36:] == -1) and not np.any(desc[36:])
+        assert np.all(kps["angle"][:36] != -1)
+    finally:
+        s.close()
+
+
+@pytest.mark.parametrize("seed", [3, 4])
+def test_corrected_detector_bit_exact(seed):
+    raw, img = _gray(seed=seed)
+    h, w = img.shape
+    s = SURF(w, h, max_features=-1, corrected=True)
+    try:
+        kps, desc = s.detectAndCompute(img, slot=0)
+        rk, rd, _ = R.detect(img, max_features=-1, per_axis=True)
+        assert len(kps) == len(rk) > 0
+        for f in rk.dtype.names:
+            assert np.array_equal(kps[f], rk[f]), f
+        assert np.array_equal(desc, rd)
+        assert np.all(kps["angle"] != -1)
+    finally:
+        s.close()
+
+
 def test_detect_device_input_matches_host_input():
     import torch
     raw, img = _gray(seed=6)
