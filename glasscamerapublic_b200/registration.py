@@ -71,6 +71,15 @@ class SURF:
     def handle(self) -> C.c_void_p:
         return self._h
 
+    @property
+    def corrected(self) -> bool:
+        """Whether detections use the corrected detector (GLS_SURF_CORRECTED)."""
+        return bool(self._detect_flags & SURF_CORRECTED)
+
+    @corrected.setter
+    def corrected(self, on: bool):
+        self._detect_flags = SURF_CORRECTED if on else 0
+
     def detect_slot(self, img, slot: int, stream=None, sync: bool = False) -> int:
         """Detection + description of img (F32 H x W, numpy or CUDA tensor)
         into a slot, asynchronously for device input."""

@@ -230,12 +230,16 @@ def test_register_image_identity_is_copy():
     assert torch.equal(out, img)
 
 
-def test_burst_registration_recovers_warps():
+@pytest.mark.parametrize("corrected,bound", [(False, 2.5), (True, 1.0)])
+def test_burst_registration_recovers_warps(corrected, bound):
     # RawChannels (G, G2) -> SURF -> match -> RANSAC per channel, running
-    # average, ScaleHomography: the main() driver of pyramidFusion.cpp:276-346
+    # average, ScaleHomography: the main() driver of pyramidFusion.cpp:276-346.
+    # The reference's detector moves keypoints by the scale offset along x
+    # and y as well (SURF.metal:200), which costs it sub-pixel accuracy; the
+    # corrected detector registers these frames to well under a pixel.
     wl = scene.Workload("burst", 2048, 1536, gain=1.5, read=4.0, iso=800, seed=3001)
     raws, _, Hs = scene.make_burst(wl, 3)
-    s = SURF(1024, 768, max_features=1500)
+    s = SURF(1024, 768, max_features=1500, corrected=corrected)
     try:
         ref = s.raw_channels(raws[0], 2, 512.0, 4095.0)
         s.detect_slot(ref[1], 0)
@@ -250,7 +254,7 @@ def test_burst_registration_recovers_warps():
                 Hacc = (Hc + Hacc * np.float32(c)) / np.float32(c + 1)
             Hf = ScaleHomography(Hacc, 2)
             err = scene.corner_error(Hf, Hs[i], wl.width, wl.height)
-            assert err < 1.0, (i, err)
+            assert err < bound, (i, err)
     finally:
         s.close()
 
@@ -259,7 +263,7 @@ def test_register_frames_batch_equals_single_jobs():
     # the batched burst registration gives the per-job results bit for bit
     wl = scene.Workload("burst", 1024, 768, gain=1.5, read=4.0, iso=800, seed=3002)
     raws, _, Hs = scene.make_burst(wl, 4)
-    s = SURF(512, 384, max_features=1500)
+    s = SURF(512, 384, max_features=1500, corrected=True)
     try:
         planes = []
         for f, r in enumerate(raws):
