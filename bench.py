@@ -338,7 +338,7 @@ def mixed_leg(args, rank, local, conv, stream):
     import torch
     import torch.nn.functional as F
 
-    from glasscamerapublic_b200 import scene
+    from glasscamerapublic_b200 import block_match_tiles, scene
 
     dev = f"cuda:{local}"
     wls = scene.mixed_batch(4)
@@ -403,7 +403,9 @@ def mixed_leg(args, rank, local, conv, stream):
         "ms_per_batch_graph": ms_graph,
         "ms_per_batch_stream_launched": ms_stream,
         "gpu_launches_per_batch": per_batch,
-        "note": "one CUDA graph replay per batch; frames spread largest-first over 3 slot streams",
+        "block_match_tile_heights": [list(t) for t in block_match_tiles()],
+        "note": "one CUDA graph replay per batch; frames spread largest-first over 3 slot streams; "
+                "block_match_tile_heights: autotuned (width, height, thread rows: 8 = 32x32 px tiles, 4 = 32x16)",
     }
 
 
