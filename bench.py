@@ -148,7 +148,49 @@ def cpu_baseline(wl, params_fn, seconds: float):
     fps_sample = n / dt
     scale = (sw * sh) / (wl.width * wl.height)
     return {"value": fps_sample * scale, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{n} x {sw}x{sh} frame(s), 5 levels, {what}, {dt:.1f}s; frames/s scaled by area x{scale:.4f}"}
+            "sample": f"{n} x {sw}x{sh} frame(s), 5 levels, {what}, {dt:.1f}s; frames/s scaled by area x{scale:.4f}",
+            "registration": cpu_registration_baseline(threads)}
+
+
+def cpu_registration_baseline(threads: int):
+    """The burst workload's registration of one frame on the host cores:
+    SURF detect + describe on its G and G2 planes (2016x1512, 1500
+    features), matching against the reference frame's features, and
+    FindHomography (2000 RANSAC iterations + least squares) per channel,
+    as pyramidFusion.cpp:318-346 does per frame. It runs the reference's own
+    registration code compiled for the CPU (oracle/_ref/libglsref_reg.so,
+    kind "reference") where it was built, else the oracle (kind "port").
+    RawChannels is done before the clock starts."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import _oracle as O
+    import _oracle_reg as OR
+    import _ref_reg as F
+    from glasscamerapublic_b200 import scene
+    wl = scene.WORKLOADS["cfg3_burst_4032x3024"]
+    raws, _, _ = scene.make_burst(wl, 2)
+    planes = [[OR.raw_channel(r, wl.pattern, c, float(wl.black), float(wl.white)) for c in (1, 3)] for r in raws]
+    if F.available():
+        kind, what = "reference", "reference SURF.metal / SURF.cpp / Homography.cpp compiled for the CPU"
+        F.lib().ref_reg_set_threads(threads)
+        det, mat = F.detect, F.match
+        fh = lambda p1, p2: F.find_homography(p1, p2, 1.0, 2000)
+    else:
+        kind, what = "port", "registration oracle"
+        O.lib().orc_set_threads(threads)
+        det, mat = OR.detect, OR.match
+        fh = lambda p1, p2: OR.find_homography(p1, p2, 1.0, 2000)[:2]
+    ref = [det(pl) for pl in planes[0]]
+    t0 = time.perf_counter()
+    for c in range(2):
+        k2, d2, _ = det(planes[1][c])
+        k1, d1, _ = ref[c]
+        m = mat(d1, d2)
+        p1 = np.stack([k1["x"][m["query_idx"]], k1["y"][m["query_idx"]]], 1)
+        p2 = np.stack([k2["x"][m["train_idx"]], k2["y"][m["train_idx"]]], 1)
+        fh(p1, p2)
+    ms = 1e3 * (time.perf_counter() - t0)
+    return {"ms_per_frame": ms, "cores": threads, "kind": kind,
+            "sample": f"one burst frame: 2 x (detect 2016x1512 + match + RANSAC 2000), {what}"}
 
 
 def burst_leg(args, rank, local, conv, stream):

@@ -121,6 +121,22 @@ void run_groups(int grid, int group, F&& f) {
     for (auto& t : th) t.join();
 }
 
+// A 2-D dispatch of a kernel without threadgroup memory, rows spread over
+// the host's cores. f(x, y).
+int g_threads = 0;
+template <class F>
+void run_rows(int w, int h, F&& f) {
+    if (w <= 0 || h <= 0) return;
+    const int nt = std::max(1, std::min(h, g_threads > 0 ? g_threads : int(std::thread::hardware_concurrency())));
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; t++)
+        th.emplace_back([&, t] {
+            for (int y = t; y < h; y += nt)
+                for (int x = 0; x < w; x++) f(x, y);
+        });
+    for (auto& t : th) t.join();
+}
+
 struct RefSurf {
     int width, height, max_features, n_octaves = 4, n_octave_layers = 2;
     float threshold = 0.02f;
@@ -178,11 +194,11 @@ struct RefSurf {
             const gls::DetAndTraceHaarPattern hp(sum[0]->st.width, sum[0]->st.height, sizes[i], steps[i]);
             const gls::gpuSurfHF hf(hp.Dx, hp.Dy, hp.Dxy);
             static_assert(sizeof(hf) == 256, "gpuSurfHF layout");
-            for (int y = 0; y < hp.margin_crop.height; y++)
-                for (int x = 0; x < hp.margin_crop.width; x++)
-                    refwrap::calc_det_and_trace(&sum[0]->st, &dets[i]->st, &traces[i]->st, steps[i], hp.Dx[0].w,
-                                                hp.Dxy[0].w, hp.margin_crop.x, hp.margin_crop.y, &hf, unsigned(x),
-                                                unsigned(y));
+            run_rows(hp.margin_crop.width, hp.margin_crop.height, [&](int x, int y) {
+                refwrap::calc_det_and_trace(&sum[0]->st, &dets[i]->st, &traces[i]->st, steps[i], hp.Dx[0].w,
+                                            hp.Dxy[0].w, hp.margin_crop.x, hp.margin_crop.y, &hf, unsigned(x),
+                                            unsigned(y));
+            });
         }
         auto maxima = std::make_unique<refwrap::Maxima>();
         maxima->count = 0;
@@ -192,12 +208,14 @@ struct RefSurf {
             const int step = steps[layer];
             const int lh = height / step, lw = width / step;
             const int margin = (sizes[layer + 1] / 2) / step + 1;
-            for (int y = 0; y < lh - 2 * margin; y++)
-                for (int x = 0; x < lw - 2 * margin; x++)
-                    refwrap::find_maxima_in_layer(&dets[layer - 1]->st, &dets[layer]->st, &dets[layer + 1]->st,
-                                                  &traces[layer]->st, sizes[layer - 1], sizes[layer],
-                                                  sizes[layer + 1], maxima.get(), margin, octave, threshold, step,
-                                                  unsigned(x), unsigned(y));
+            // appended through the kernel's atomic counter in any order, then
+            // sorted by KeypointGreater, a total order on distinct maxima
+            run_rows(lw - 2 * margin, lh - 2 * margin, [&](int x, int y) {
+                refwrap::find_maxima_in_layer(&dets[layer - 1]->st, &dets[layer]->st, &dets[layer + 1]->st,
+                                              &traces[layer]->st, sizes[layer - 1], sizes[layer], sizes[layer + 1],
+                                              maxima.get(), margin, octave, threshold, step, unsigned(x),
+                                              unsigned(y));
+            });
         }
         std::vector<KeyPoint> kps;
         const int n = std::min(maxima->count, refwrap::kMaximaCapacity);
@@ -254,6 +272,9 @@ gls::image<float> wrap(const float* img, int w, int h) {
 extern "C" {
 
 void ref_reg_set_own_math(int on) { gls::g_own_math = on; }
+
+// host threads for the per-pixel kernels (0 = all cores)
+void ref_reg_set_threads(int n) { g_threads = n; }
 
 // summed-area table, (h + 1) x (w + 1), of the integral kernels; entries
 // the kernels never write are NaN
@@ -348,8 +369,9 @@ void ref_reg_fuse(const float* fused, const float* input, int w, int h, const fl
     Plane f(w, h, 4), in(w, h, 4), o(w, h, 4);
     std::memcpy(f.px.data(), fused, sizeof(float) * 4 * size_t(w) * h);
     std::memcpy(in.px.data(), input, sizeof(float) * 4 * size_t(w) * h);
-    for (int y = 0; y < h; y++)
-        for (int x = 0; x < w; x++) refwrap::register_and_fuse(&f.st, &in.st, &o.st, H, count, unsigned(x), unsigned(y));
+    run_rows(w, h, [&](int x, int y) {
+        refwrap::register_and_fuse(&f.st, &in.st, &o.st, H, count, unsigned(x), unsigned(y));
+    });
     std::memcpy(out, o.px.data(), sizeof(float) * 4 * size_t(w) * h);
 }
 

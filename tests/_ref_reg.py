@@ -29,6 +29,7 @@ def lib() -> C.CDLL:
         ip = C.POINTER(C.c_int)
         vp = C.c_void_p
         L.ref_reg_set_own_math.argtypes = [C.c_int]
+        L.ref_reg_set_threads.argtypes = [C.c_int]
         L.ref_reg_integral.argtypes = [fp, C.c_int, C.c_int, fp]
         L.ref_reg_detect.argtypes = [fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, vp, fp, C.c_int, ip]
         L.ref_reg_match.argtypes = [fp, C.c_int, fp, C.c_int, vp]
