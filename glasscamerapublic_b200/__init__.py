@@ -43,6 +43,7 @@ PLANE_GRADIENT = 1
 PLANE_DEMOSAIC = 2
 PLANE_DESPECKLED = 3
 PLANE_OUTPUT = 4
+PLANE_ADJ_DESPECKLED = 5
 PLANE_DENOISED_L0 = 8
 SURF_PLANE_INTEGRAL = 0
 ADJ_NPARAMS = 32

@@ -4,8 +4,8 @@ the 32 calibration scalars can be tuned by gradient descent and checked
 against finite differences and a reference autograd gradient.
 
 Parameter vector layout (GLS_ADJ_*): luma[5], chroma[5], A_Y[5], B_Y[5],
-A_C[5], B_C[5] of the pyramid levels, then raw green a, b (not
-differentiated: NaN).
+A_C[5], B_C[5] of the pyramid levels, then the raw green a and b (the
+means of raw_nlf a[1], a[3] and of b[1], b[3], which move together).
 """
 from __future__ import annotations
 
@@ -33,8 +33,9 @@ def params_to_theta(p: DemosaicParams) -> np.ndarray:
 
 
 def theta_to_params(theta, base: DemosaicParams) -> DemosaicParams:
-    """A copy of base with the pyramid parameters set from theta (Cb and Cr
-    NLF move together, keeping their calibrated offset)."""
+    """A copy of base with the parameters set from theta. Cb and Cr NLF move
+    together, keeping their calibrated offset; so do the raw G and G2
+    variance coefficients."""
     p = DemosaicParams.from_buffer_copy(base)
     th = np.asarray(theta, np.float64)
     for l in range(base.levels):
@@ -48,6 +49,11 @@ def theta_to_params(theta, base: DemosaicParams) -> DemosaicParams:
         p.pyramid_nlf[l].a[2] = base.pyramid_nlf[l].a[2] + da
         p.pyramid_nlf[l].b[1] = base.pyramid_nlf[l].b[1] + db
         p.pyramid_nlf[l].b[2] = base.pyramid_nlf[l].b[2] + db
+    t0 = params_to_theta(base)
+    for k, arr in ((30, "a"), (31, "b")):
+        d = th[k] - t0[k]
+        for c in (1, 3):
+            getattr(p.raw_nlf, arr)[c] = getattr(base.raw_nlf, arr)[c] + d
     return p
 
 
@@ -79,7 +85,7 @@ def denoise_loss_function():
         def forward(ctx, theta, converter, raw, base_params, target):
             p = theta_to_params(theta.detach().cpu().numpy(), base_params)
             loss, g = loss_and_grad(converter, raw, p, target)
-            gt = torch.from_numpy(np.nan_to_num(g.astype(np.float64), nan=0.0)).to(theta.dtype)
+            gt = torch.from_numpy(g.astype(np.float64)).to(theta.dtype)
             ctx.save_for_backward(gt)
             return theta.new_tensor(loss)
 

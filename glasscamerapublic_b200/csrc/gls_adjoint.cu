@@ -11,9 +11,11 @@
 // The PCA basis is held fixed (its dependence on theta is not differentiated).
 //
 // Reverse sweep, fine to coarse: out = M den_0; den_l = BM_l(layer_l);
-// layer_l = SN_l(img_l, img_{l+1}, den_{l+1}) for l < L-1. Only the path
-// through den_{l+1} carries theta, so the input pyramid img_l needs no
-// adjoint.
+// layer_l = SN_l(img_l, img_{l+1}, den_{l+1}) for l < L-1, and
+// layer_{L-1} = img_{L-1}. The pyramid parameters reach the loss through
+// den_{l+1}; the raw green NLF reaches it through the input pyramid
+// img_{l+1} = down(img_l), img_0 = the despeckled front-end output, so the
+// sweep also accumulates dL/d img_l and pushes it down to img_0.
 //   * k_adj_head          dL/d den_0 = M^T 2 (out - target) / N, and the loss
 //   * k_bm_bwd_center     block matching, the pixel as the window centre:
 //                         from the forward's outputs and kernel norms,
@@ -25,7 +27,13 @@
 //   * k_pca_bwd           transpose of the 5x5 x 25x8 projection
 //   * k_sn_bwd            subtractNoiseImage: dL/d(up-sampled den_{l+1}) and
 //                         dL/dtheta through the sharpening gate
-//   * k_up_bwd            transpose of the bilinear up-sampling
+//   * k_up_bwd            transpose of the bilinear up-sampling (for the
+//                         coarse denoised image, and with k_up_bwd_img for
+//                         the coarse noisy image)
+//   * k_down_bwd          transpose of the pyramid down-sampling: with the
+//                         subtract-noise input terms, dL/d(level-0 image),
+//                         which the raw front end's tangents
+//                         (gls_front_jvp.cu) turn into dL/d(raw green NLF)
 // Every reduction is per block and summed in block order: the gradient does
 // not depend on scheduling.
 #include <cfloat>
@@ -441,6 +449,13 @@ __global__ void __launch_bounds__(256) k_sn_bwd(AdjointSnArgs a) {
         a.g_up[pi * 3 + 0] = gpd[0];
         a.g_up[pi * 3 + 1] = gpd[1];
         a.g_up[pi * 3 + 2] = gpd[2];
+        if (a.g_in) {  // d(out)/d(in) = alpha, d(out)/d(up-sampled coarse) = -alpha * weight
+            for (int c = 0; c < 3; c++) {
+                const float wc = c == 0 ? a.luma_weight : 1.f;
+                a.g_in[pi * 3 + c] += alpha * go[c];
+                a.g_p1[pi * 3 + c] = -alpha * wc * go[c];
+            }
+        }
     }
     for (int o = 16; o > 0; o >>= 1) {
         gna += __shfl_down_sync(0xffffffffu, gna, o);
@@ -460,7 +475,7 @@ __global__ void __launch_bounds__(256) k_sn_bwd(AdjointSnArgs a) {
 
 // bilinear up-sampling (the reconstruct step's coarse reads) transposed:
 // each coarse pixel gathers the weights with which fine pixels sampled it.
-__global__ void __launch_bounds__(256) k_up_bwd(AdjointSnArgs a) {
+__device__ __forceinline__ void up_transpose(const AdjointSnArgs& a, const float* src, float* dst, bool accumulate) {
     const int X = blockIdx.x * blockDim.x + threadIdx.x, Y = blockIdx.y * blockDim.y + threadIdx.y;
     if (X >= a.cw || Y >= a.ch) return;
     float acc[3] = {0, 0, 0};
@@ -479,17 +494,66 @@ __global__ void __launch_bounds__(256) k_up_bwd(AdjointSnArgs a) {
             const float wx =
                 (clampi(xi, 0, a.cw - 1) == X ? 1.f - ax : 0.f) + (clampi(xi + 1, 0, a.cw - 1) == X ? ax : 0.f);
             if (wx == 0.f) continue;
-            const float* g = a.g_up + (size_t(y) * a.w + x) * 3;
+            const float* g = src + (size_t(y) * a.w + x) * 3;
             const float wgt = wx * wy;
             acc[0] += wgt * g[0];
             acc[1] += wgt * g[1];
             acc[2] += wgt * g[2];
         }
     }
-    float* o = a.g_coarse_den + (size_t(Y) * a.cw + X) * 3;
-    o[0] = acc[0];
-    o[1] = acc[1];
-    o[2] = acc[2];
+    float* o = dst + (size_t(Y) * a.cw + X) * 3;
+    for (int c = 0; c < 3; c++) o[c] = accumulate ? o[c] + acc[c] : acc[c];
+}
+
+__global__ void __launch_bounds__(256) k_up_bwd(AdjointSnArgs a) { up_transpose(a, a.g_up, a.g_coarse_den, false); }
+__global__ void __launch_bounds__(256) k_up_bwd_img(AdjointSnArgs a) { up_transpose(a, a.g_p1, a.g_coarse_img, true); }
+
+// k_downsample transposed: out(x, y) = 1/4 sum over a, b in {0, 1} of the
+// bilinear sample at (x rx - 0.5 + a rx, y ry - 0.5 + b ry), clamp-to-edge,
+// a separable weight; each fine pixel gathers from the coarse pixels whose
+// samples touch it.
+__device__ __forceinline__ float down_weight(int X, int x, float r, int n) {
+    float wsum = 0.f;
+    for (int t = 0; t < 2; t++) {
+        const float u = __fsub_rn(__fmul_rn(float(x + t), r), 0.5f);
+        const float fu = floorf(u);
+        const int xi = int(fu);
+        const float ax = u - fu;
+        wsum += (clampi(xi, 0, n - 1) == X ? 1.f - ax : 0.f) + (clampi(xi + 1, 0, n - 1) == X ? ax : 0.f);
+    }
+    return wsum;
+}
+
+__global__ void __launch_bounds__(256) k_down_bwd(const float* __restrict__ gc, int cw, int ch, float* __restrict__ gf,
+                                                 int w, int h, float rx, float ry) {
+    const int X = blockIdx.x * blockDim.x + threadIdx.x, Y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (X >= w || Y >= h) return;
+    const int x0 = max(int(floorf(float(X) / rx)) - 3, 0), x1 = min(int(floorf(float(X) / rx)) + 3, cw - 1);
+    const int y0 = max(int(floorf(float(Y) / ry)) - 3, 0), y1 = min(int(floorf(float(Y) / ry)) + 3, ch - 1);
+    float acc[3] = {0, 0, 0};
+    for (int y = y0; y <= y1; y++) {
+        const float wy = down_weight(Y, y, ry, h);
+        if (wy == 0.f) continue;
+        for (int x = x0; x <= x1; x++) {
+            const float wx = down_weight(X, x, rx, w);
+            if (wx == 0.f) continue;
+            const float wgt = 0.25f * wx * wy;
+            const float* g = gc + (size_t(y) * cw + x) * 3;
+            acc[0] += wgt * g[0];
+            acc[1] += wgt * g[1];
+            acc[2] += wgt * g[2];
+        }
+    }
+    float* o = gf + (size_t(Y) * w + X) * 3;
+    o[0] += acc[0];
+    o[1] += acc[1];
+    o[2] += acc[2];
+}
+
+__global__ void __launch_bounds__(256) k_add_layer_grad(const float* __restrict__ gl, float* __restrict__ gi, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int c = 0; c < 3; c++) gi[size_t(i) * 3 + c] += gl[size_t(i) * 4 + c];
 }
 
 size_t adjoint_center_smem() { return sizeof(CenterSmem); }
@@ -520,6 +584,17 @@ void launch_sn_bwd(const AdjointSnArgs& a, cudaStream_t s) {
     const dim3 b(32, 8), g((a.w + 31) / 32, (a.h + 7) / 8), gc((a.cw + 31) / 32, (a.ch + 7) / 8);
     k_sn_bwd<<<g, b, 0, s>>>(a);
     k_up_bwd<<<gc, b, 0, s>>>(a);
+    if (a.g_in) k_up_bwd_img<<<gc, b, 0, s>>>(a);
+}
+
+void launch_add_layer_grad(const float* g_layer, float* g_img, int w, int h, cudaStream_t s) {
+    const int n = w * h;
+    k_add_layer_grad<<<(n + 255) / 256, 256, 0, s>>>(g_layer, g_img, n);
+}
+
+void launch_down_bwd(const float* g_coarse, int cw, int ch, float* g_fine, int w, int h, cudaStream_t s) {
+    const dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
+    k_down_bwd<<<g, b, 0, s>>>(g_coarse, cw, ch, g_fine, w, h, float(w) / float(cw), float(h) / float(ch));
 }
 
 int adjoint_blocks(int w, int h) { return ((w + AT_X - 1) / AT_X) * ((h + AT_Y - 1) / AT_Y); }

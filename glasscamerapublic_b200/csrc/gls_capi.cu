@@ -186,6 +186,8 @@ struct gls_converter {
     cudaGraphExec_t graph_exec = nullptr;
     // adjoint scratch (gls_demosaic_denoise_vjp)
     DevBuf adj_gden[2], adj_rec, adj_glayer, adj_gpca, adj_gup, adj_part, adj_loss, adj_target;
+    DevBuf adj_gimg, adj_gp1, adj_jvp, adj_jvp_part;  // dL/d(input pyramid), front-end tangents
+    int adj_gimg_w = 0, adj_gimg_h = 0;                // size of the last dL/d(despeckled image)
 };
 
 namespace gls {
@@ -378,6 +380,34 @@ static gls_status make_target(Pipeline<S>& P, gls_image_view* out, int w, int h,
     return GLS_OK;
 }
 
+// crossDenoiseRawRGBAImage arguments (raw_converter.cpp:195-202)
+static RawDenoiseArgs raw_denoise_args(const gls_demosaic_params* p, bool fast) {
+    RawDenoiseArgs ra;
+    ra.pattern = p->bayer_pattern;
+    for (int c = 0; c < 4; c++) ra.var[c] = p->raw_nlf.b[c];
+    ra.strength = p->raw_denoise_strength;
+    ra.fast = fast ? 1 : 0;
+    return ra;
+}
+
+// demosaic arguments: getRawVariance (demosaic.hpp:186-193), green the mean
+// of G and G2; cam -> YCbCr when the image goes on to the denoiser
+static DemosaicArgs demosaic_args(const gls_demosaic_params* p, bool transform) {
+    DemosaicArgs da;
+    da.pattern = p->bayer_pattern;
+    da.rv0 = p->raw_nlf.a[0];
+    da.rv1 = p->raw_nlf.b[0];
+    da.gv0 = (p->raw_nlf.a[1] + p->raw_nlf.a[3]) / 2;
+    da.gv1 = (p->raw_nlf.b[1] + p->raw_nlf.b[3]) / 2;
+    da.bv0 = p->raw_nlf.a[2];
+    da.bv1 = p->raw_nlf.b[2];
+    da.transform = transform ? 1 : 0;
+    float c2y[9], y2c[9];
+    cam_ycbcr(p->rgb_cam, p->xyz_rgb, c2y, y2c);
+    std::memcpy(da.m, c2y, sizeof(c2y));
+    return da;
+}
+
 template <class S>
 static gls_status demosaic_run(gls_converter* cv, const uint16_t* raw, int w, int h, size_t stride_bytes,
                                const gls_demosaic_params* p, uint32_t flags, gls_image_view* out, cudaStream_t s,
@@ -437,12 +467,9 @@ static gls_status demosaic_run(gls_converter* cv, const uint16_t* raw, int w, in
         ba.fx[t] = taps[3 * t + 1] - fdx;
         ba.fy[t] = taps[3 * t + 2] - fdy;
     }
-    // getRawVariance, demosaic.hpp:186-193
-    const float rv0 = p->raw_nlf.a[0], rv1 = p->raw_nlf.b[0];
-    const float gv0 = (p->raw_nlf.a[1] + p->raw_nlf.a[3]) / 2, gv1 = (p->raw_nlf.b[1] + p->raw_nlf.b[3]) / 2;
-    const float bv0 = p->raw_nlf.a[2], bv1 = p->raw_nlf.b[2];
-    ba.var0 = gv0;
-    ba.var1 = gv1;
+    // the green raw variance (getRawVariance, demosaic.hpp:186-193)
+    ba.var0 = (p->raw_nlf.a[1] + p->raw_nlf.a[3]) / 2;
+    ba.var1 = (p->raw_nlf.b[1] + p->raw_nlf.b[3]) / 2;
     ba.inv_sqrt45 = 1.0f / sqrtf(4.5f);
     {
         KScope k(cv->prof, KC_SOBEL_BLUR, s);
@@ -451,11 +478,7 @@ static gls_status demosaic_run(gls_converter* cv, const uint16_t* raw, int w, in
 
     // high-noise raw branch, raw_converter.cpp:195-202
     if (denoise && p->high_noise_image) {
-        RawDenoiseArgs ra;
-        ra.pattern = p->bayer_pattern;
-        for (int c = 0; c < 4; c++) ra.var[c] = p->raw_nlf.b[c];
-        ra.strength = p->raw_denoise_strength;
-        ra.fast = is_half<S>::value ? 1 : 0;
+        const RawDenoiseArgs ra = raw_denoise_args(p, is_half<S>::value);
         KScope k(cv->prof, KC_RAW_DENOISE, s, 2);
         launch_raw_denoise<S>(scaled, grad, plane<S, 4>(P.quad, w / 2, h / 2), ra, s);
     }
@@ -463,11 +486,7 @@ static gls_status demosaic_run(gls_converter* cv, const uint16_t* raw, int w, in
     // demosaic + blendHighlights (+ cam -> YCbCr), raw_converter.cpp:204-214
     float c2y[9], y2c[9];
     cam_ycbcr(p->rgb_cam, p->xyz_rgb, c2y, y2c);
-    DemosaicArgs da;
-    da.pattern = p->bayer_pattern;
-    da.rv0 = rv0; da.rv1 = rv1; da.gv0 = gv0; da.gv1 = gv1; da.bv0 = bv0; da.bv1 = bv1;
-    da.transform = denoise ? 1 : 0;
-    std::memcpy(da.m, c2y, sizeof(c2y));
+    const DemosaicArgs da = demosaic_args(p, denoise);
     Plane<S, 4> A = plane<S, 4>(P.A, w, h);
     {
         KScope k(cv->prof, KC_DEMOSAIC, s);
@@ -561,6 +580,16 @@ static gls_status adjoint_run(gls_converter* cv, const gls_demosaic_params* p, c
     GLS_TRY(cv->adj_glayer.ensure(n * 4 * sizeof(float)));
     GLS_TRY(cv->adj_gpca.ensure(n * 8 * sizeof(float)));
     GLS_TRY(cv->adj_gup.ensure(n * 3 * sizeof(float)));
+    // dL/d img_l for every level (3 ch), and the front-end tangent scratch
+    std::vector<size_t> gimg_off(L + 1, 0);
+    for (int i = 0; i < L; i++) gimg_off[i + 1] = gimg_off[i] + size_t(W >> i) * (H >> i) * 3;
+    GLS_TRY(cv->adj_gimg.ensure(gimg_off[L] * sizeof(float)));
+    GLS_TRY(cv->adj_gp1.ensure(n * 3 * sizeof(float)));
+    GLS_TRY(cv->adj_jvp.ensure(front_jvp_scratch_bytes(W, H)));
+    const int jvp_blocks = front_jvp_blocks(W, H);
+    GLS_TRY(cv->adj_jvp_part.ensure(size_t(jvp_blocks) * 2 * sizeof(float)));
+    float* gimg = static_cast<float*>(cv->adj_gimg.p);
+    GLS_CUDA(cudaMemsetAsync(gimg, 0, gimg_off[L] * sizeof(float), s));
     std::vector<size_t> bm_off(L), sn_off(L);
     size_t parts = 0;
     for (int i = 0; i < L; i++) {
@@ -637,14 +666,41 @@ static gls_status adjoint_run(gls_converter* cv, const gls_demosaic_params* p, c
             sa.sharpening = dp.sharpening;
             sa.nlf_a = p->pyramid_nlf[i].a[0] * dp.luma;
             sa.nlf_b = p->pyramid_nlf[i].b[0] * dp.luma;
+            sa.g_in = gimg + gimg_off[i];
+            sa.g_p1 = static_cast<float*>(cv->adj_gp1.p);
+            sa.g_coarse_img = gimg + gimg_off[i + 1];
             launch_sn_bwd(sa, s);
             std::swap(gcur, gnext);
+        } else {  // the coarsest level denoises its image itself
+            launch_add_layer_grad(la.g_layer, gimg + gimg_off[i], wi, hi, s);
         }
     }
+    // img_{l+1} = down(img_l): push dL/d img down to the despeckled image
+    for (int i = L - 2; i >= 0; i--)
+        launch_down_bwd(gimg + gimg_off[i + 1], W >> (i + 1), H >> (i + 1), gimg + gimg_off[i], W >> i, H >> i, s);
+    // the raw front end's tangents along theta30 / theta31, dotted with it
+    FrontJvpArgs fj;
+    fj.w = W;
+    fj.h = H;
+    fj.scaled = static_cast<const float*>(P.scaled.p);
+    fj.quad = static_cast<const float*>(P.quad.p);
+    fj.grad = static_cast<const float*>(P.grad.p);
+    fj.high_noise = p->high_noise_image ? 1 : 0;
+    fj.raw = raw_denoise_args(p, false);
+    fj.dm = demosaic_args(p, true);
+    fj.despeckle_va = p->pyramid_nlf[0].a[0];
+    fj.despeckle_vb = p->pyramid_nlf[0].b[0];
+    fj.g_ds = gimg;
+    fj.scratch = cv->adj_jvp.p;
+    fj.part = static_cast<float*>(cv->adj_jvp_part.p);
+    launch_front_jvp(fj, s);
+    cv->adj_gimg_w = W;
+    cv->adj_gimg_h = H;
     GLS_CUDA(cudaGetLastError());
-    std::vector<float> hp(parts);
+    std::vector<float> hp(parts), hj(size_t(jvp_blocks) * 2);
     std::vector<double> hl(head_blocks);
     if (parts) GLS_CUDA(cudaMemcpyAsync(hp.data(), part, parts * sizeof(float), cudaMemcpyDeviceToHost, s));
+    GLS_CUDA(cudaMemcpyAsync(hj.data(), cv->adj_jvp_part.p, hj.size() * sizeof(float), cudaMemcpyDeviceToHost, s));
     GLS_CUDA(cudaMemcpyAsync(hl.data(), cv->adj_loss.p, hl.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
     GLS_CUDA(cudaStreamSynchronize(s));
     double g[GLS_ADJ_NPARAMS] = {};
@@ -675,9 +731,11 @@ static gls_status adjoint_run(gls_converter* cv, const gls_demosaic_params* p, c
     double lsum = 0;
     for (double v : hl) lsum += v;
     if (loss) *loss = lsum / (3.0 * double(n));
+    for (int b = 0; b < jvp_blocks; b++) {
+        g[GLS_ADJ_RAW_GREEN_A] += hj[size_t(b) * 2];
+        g[GLS_ADJ_RAW_GREEN_B] += hj[size_t(b) * 2 + 1];
+    }
     for (int k = 0; k < GLS_ADJ_NPARAMS; k++) grad[k] = float(g[k]);
-    grad[GLS_ADJ_RAW_GREEN_A] = NAN;  // not differentiated (the front end is held fixed)
-    grad[GLS_ADJ_RAW_GREEN_B] = NAN;
     return GLS_OK;
 }
 
@@ -791,7 +849,8 @@ gls_status gls_converter_destroy(gls_converter* conv) {
     if (conv->fork_ev) cudaEventDestroy(conv->fork_ev);
     if (conv->graph_exec) cudaGraphExecDestroy(conv->graph_exec);
     for (DevBuf* b : {&conv->adj_gden[0], &conv->adj_gden[1], &conv->adj_rec, &conv->adj_glayer, &conv->adj_gpca,
-                      &conv->adj_gup, &conv->adj_part, &conv->adj_loss, &conv->adj_target})
+                      &conv->adj_gup, &conv->adj_part, &conv->adj_loss, &conv->adj_target, &conv->adj_gimg,
+                      &conv->adj_gp1, &conv->adj_jvp, &conv->adj_jvp_part})
         b->release();
     delete conv;
     return GLS_OK;
@@ -941,6 +1000,11 @@ gls_status gls_converter_plane(gls_converter* conv, int32_t which, gls_image_vie
             return set_error(GLS_ERR_INVALID_ARG, "the denoised output lives in the caller's view");
         case GLS_PLANE_DESPECKLED:
             *view = {pick(conv->p16.B, conv->p32.B), w, hh, 4, view->dtype, size_t(w) * 4 * es};
+            return GLS_OK;
+        case GLS_PLANE_ADJ_DESPECKLED:
+            if (!conv->adj_gimg_w) return set_error(GLS_ERR_INVALID_ARG, "no gls_demosaic_denoise_vjp has run");
+            *view = {conv->adj_gimg.p, conv->adj_gimg_w, conv->adj_gimg_h, 3, GLS_F32,
+                     size_t(conv->adj_gimg_w) * 3 * sizeof(float)};
             return GLS_OK;
         default:
             if (which >= GLS_PLANE_DENOISED_L0 && which < GLS_PLANE_DENOISED_L0 + conv->last_levels) {

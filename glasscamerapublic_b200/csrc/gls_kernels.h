@@ -136,9 +136,37 @@ struct AdjointSnArgs {
     float* g_coarse_den;  // 3 ch out at the coarse level
     float* part;          // per-block dL/d nlf_a, dL/d nlf_b
     float luma_weight, sharpening, nlf_a, nlf_b;
+    // optional (null: skipped): dL/d of the level's noisy input image, 3 ch
+    float* g_in;          // += at the fine level
+    float* g_p1;          // 3 ch fine scratch: dL/d(up-sampled coarse noisy image)
+    float* g_coarse_img;  // += at the coarse level
 };
 void launch_adj_head(const float* den0, const float* target, int tstride, int w, int h, const AdjointHeadArgs& a,
                      float* g_den, double* loss_part, cudaStream_t s);
+// g_img (3 ch) += the first 3 channels of g_layer (4 ch): the coarsest
+// level's block matching reads the level image itself
+void launch_add_layer_grad(const float* g_layer, float* g_img, int w, int h, cudaStream_t s);
+// g_fine (3 ch, w x h) += transpose of the pyramid down-sampling
+// (k_downsample) applied to g_coarse (3 ch, cw x ch)
+void launch_down_bwd(const float* g_coarse, int cw, int ch, float* g_fine, int w, int h, cudaStream_t s);
+
+// ---- forward-mode tangents of the raw front end (gls_front_jvp.cu)
+struct FrontJvpArgs {
+    int w, h;
+    const float* scaled;  // Bayer plane after the raw branch (forward, FP32)
+    const float* quad;    // despeckled quads of the raw branch (forward)
+    const float* grad;    // 2 ch gradient plane (forward)
+    int high_noise;       // the raw branch ran
+    RawDenoiseArgs raw;
+    DemosaicArgs dm;      // transform = cam -> YCbCr
+    float despeckle_va, despeckle_vb;
+    const float* g_ds;    // 3 ch: dL/d(despeckled YCbCr), from the reverse sweep
+    void* scratch;        // front_jvp_scratch_bytes(w, h)
+    float* part;          // per block: dL/dtheta30, dL/dtheta31
+};
+size_t front_jvp_scratch_bytes(int w, int h);
+int front_jvp_blocks(int w, int h);
+void launch_front_jvp(const FrontJvpArgs& f, cudaStream_t s);
 void launch_bm_bwd(const AdjointLevelArgs& a, cudaStream_t s);
 void launch_sn_bwd(const AdjointSnArgs& a, cudaStream_t s);
 int adjoint_blocks(int w, int h);

@@ -127,6 +127,7 @@ enum {
     GLS_PLANE_DEMOSAIC = 2,      /* 4 ch camera RGB after blendHighlights */
     GLS_PLANE_DESPECKLED = 3,    /* 4 ch YCbCr input of the pyramid (after despeckle) */
     GLS_PLANE_OUTPUT = 4,        /* 4 ch final camera RGB */
+    GLS_PLANE_ADJ_DESPECKLED = 5, /* 3 ch FP32: dL/d(despeckled YCbCr) of the last gls_demosaic_denoise_vjp */
     GLS_PLANE_DENOISED_L0 = 8    /* + level: 4 ch denoised YCbCr of a pyramid level */
 };
 
@@ -262,14 +263,21 @@ gls_status gls_gaussian_bilinear_taps(float radius, float* taps, int32_t max_tap
  *   [GLS_ADJ_NLF_BY + l]   pyramid_nlf[l].b[0]
  *   [GLS_ADJ_NLF_AC + l]   pyramid_nlf[l].a[1] = a[2] (Cb and Cr tied)
  *   [GLS_ADJ_NLF_BC + l]   pyramid_nlf[l].b[1] = b[2]
- *   [GLS_ADJ_RAW_GREEN_A], [GLS_ADJ_RAW_GREEN_B]  raw_nlf green a, b
+ *   [GLS_ADJ_RAW_GREEN_A]  raw_nlf.a[1] and a[3] moved together (their mean,
+ *                          the demosaic's green variance offset)
+ *   [GLS_ADJ_RAW_GREEN_B]  raw_nlf.b[1] and b[3] moved together (the green
+ *                          variance slope of the demosaic and of the
+ *                          high-noise cross denoise)
  * for l < levels (entries of absent levels are 0). The forward runs first
- * (as gls_demosaic with GLS_DENOISE on FP32 planes); the reverse sweep is
- * hand-written CUDA over its retained planes, with each level's PCA basis
- * held fixed. The raw-green entries are NaN: the front end (demosaic,
- * despeckle) is not differentiated. target: GLS_F32 RGB or RGBA,
- * width x height, device memory (host with GLS_HOST_IO, which also makes
- * raw host memory). Synchronises the stream. */
+ * (as gls_demosaic with GLS_DENOISE on FP32 planes); the reverse sweep of
+ * the pyramid is hand-written CUDA over its retained planes, with each
+ * level's PCA basis held fixed, down to dL/d(despeckled image)
+ * (GLS_PLANE_ADJ_DESPECKLED afterwards); the raw front end (cross denoise,
+ * demosaic, despeckle) contributes by forward-mode tangents along the two
+ * raw-green parameters. The gradient plane's dependence on them (a blur
+ * radius switch) is piecewise constant and contributes nothing.
+ * target: GLS_F32 RGB or RGBA, width x height, device memory (host with
+ * GLS_HOST_IO, which also makes raw host memory). Synchronises the stream. */
 #define GLS_ADJ_NPARAMS 32
 enum {
     GLS_ADJ_LUMA = 0,

@@ -162,14 +162,19 @@ def pyramid_rgb(ds, grad, theta, params, bases, y2c):
     return den[0][..., :3] @ y2c.T
 
 
-def loss_and_grad(ds, grad, params, bases, y2c, target):
-    """MSE loss and its gradient with respect to the 32 parameters (NaN for
-    the two raw-green entries, which this expression does not cover)."""
+def loss_and_grad(ds, grad, params, bases, y2c, target, with_ds: bool = False):
+    """MSE loss and its gradient with respect to the first 30 parameters
+    (NaN for the two raw-green entries, which act before ds); with with_ds,
+    also dL/d(ds) (h, w, 3)."""
     theta = theta_from_params(params, params.levels).requires_grad_(True)
-    rgb = pyramid_rgb(torch.as_tensor(ds, dtype=torch.float64), torch.as_tensor(grad, dtype=torch.float64), theta,
-                      params, torch.as_tensor(bases, dtype=torch.float64), torch.as_tensor(y2c, dtype=torch.float64),)
+    dst = torch.as_tensor(ds, dtype=torch.float64).clone().requires_grad_(with_ds)
+    rgb = pyramid_rgb(dst, torch.as_tensor(grad, dtype=torch.float64), theta, params,
+                      torch.as_tensor(bases, dtype=torch.float64), torch.as_tensor(y2c, dtype=torch.float64))
     loss = ((rgb - torch.as_tensor(target, dtype=torch.float64)[..., :3]) ** 2).mean()
     loss.backward()
     g = theta.grad.detach().clone()
     g[30:] = float("nan")
-    return float(loss.detach()), g.numpy(), rgb.detach().numpy()
+    res = (float(loss.detach()), g.numpy(), rgb.detach().numpy())
+    if with_ds:
+        res = res + (dst.grad.detach()[..., :3].numpy(),)
+    return res
