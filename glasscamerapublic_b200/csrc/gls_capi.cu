@@ -41,6 +41,7 @@ template <class S>
 struct Pipeline {
     int W = 0, H = 0, L = 0;
     DevBuf raw, scaled, grad, quad, A, B, pca, acc, basis, status;
+    DevBuf scaled0;  // the Bayer plane before the raw branch, kept only for the adjoint
     DevBuf img[GLS_MAX_LEVELS], gradp[GLS_MAX_LEVELS], sub[GLS_MAX_LEVELS], den[GLS_MAX_LEVELS];
     DevBuf nc[GLS_MAX_LEVELS];  // chroma norms, kept only for the adjoint
     DevBuf out_f32, out_f16, stage_in, stage_grad;
@@ -74,8 +75,8 @@ struct Pipeline {
         return GLS_OK;
     }
     void release() {
-        for (DevBuf* b : {&raw, &scaled, &grad, &quad, &A, &B, &pca, &acc, &basis, &status, &out_f32, &out_f16,
-                          &stage_in, &stage_grad})
+        for (DevBuf* b : {&raw, &scaled, &scaled0, &grad, &quad, &A, &B, &pca, &acc, &basis, &status, &out_f32,
+                          &out_f16, &stage_in, &stage_grad})
             b->release();
         for (int i = 0; i < GLS_MAX_LEVELS; i++) {
             img[i].release();
@@ -478,6 +479,10 @@ static gls_status demosaic_run(gls_converter* cv, const uint16_t* raw, int w, in
 
     // high-noise raw branch, raw_converter.cpp:195-202
     if (denoise && p->high_noise_image) {
+        if (!is_half<S>::value && cv->keep_nc) {  // the adjoint's front-end tangents read it
+            GLS_TRY(P.scaled0.ensure(size_t(w) * h * sizeof(S)));
+            GLS_CUDA(cudaMemcpyAsync(P.scaled0.p, P.scaled.p, size_t(w) * h * sizeof(S), cudaMemcpyDeviceToDevice, s));
+        }
         const RawDenoiseArgs ra = raw_denoise_args(p, is_half<S>::value);
         KScope k(cv->prof, KC_RAW_DENOISE, s, 2);
         launch_raw_denoise<S>(scaled, grad, plane<S, 4>(P.quad, w / 2, h / 2), ra, s);
@@ -683,6 +688,7 @@ static gls_status adjoint_run(gls_converter* cv, const gls_demosaic_params* p, c
     fj.w = W;
     fj.h = H;
     fj.scaled = static_cast<const float*>(P.scaled.p);
+    fj.scaled0 = static_cast<const float*>(P.scaled0.p);
     fj.quad = static_cast<const float*>(P.quad.p);
     fj.grad = static_cast<const float*>(P.grad.p);
     fj.high_noise = p->high_noise_image ? 1 : 0;

@@ -5,7 +5,8 @@
 //           gv0 of the demosaic (getRawVariance, demosaic.hpp:186-193);
 //   theta31 moves raw_nlf.b[1] and b[3] together: the green variance slope
 //           gv1 of the demosaic and the G / G2 variances of the high-noise
-//           cross denoise (crossDenoiseRawRGBAImage, demosaic.metal:999-1023).
+//           raw branch (despeckleRawRGBAImage and crossDenoiseRawRGBAImage,
+//           demosaic.metal:999-1092).
 // The gradient plane depends on them only through the blur-radius switch of
 // sampledConvolutionSobel (piecewise constant), so its tangent is zero.
 //
@@ -63,10 +64,12 @@ constexpr float kPiJ = 3.14159265358979323846f;
 
 struct JvpPlanes {
     int w, h;
-    const float* scaled;  // Bayer plane after the raw branch (forward)
-    const float* quad;    // despeckled quads (forward, high-noise branch)
-    const float* grad;    // 2 ch
-    float2* rtan;         // d(Bayer)/dtheta
+    const float* scaled;   // Bayer plane after the raw branch (forward)
+    const float* scaled0;  // Bayer plane before it (forward, high-noise branch)
+    const float* quad;     // despeckled quads (forward, high-noise branch)
+    const float* grad;     // 2 ch
+    float4* qtan;          // d(quad)/dtheta31 (theta30 does not reach the raw branch)
+    float2* rtan;          // d(Bayer)/dtheta
     Dv* green;            // W x H
     Dv* tmp;              // W x H x 3
     Dv* ycc;              // W x H x 3, the demosaic output (YCbCr)
@@ -74,25 +77,68 @@ struct JvpPlanes {
 
 __device__ __forceinline__ int cl(int v, int n) { return min(max(v, 0), n - 1); }
 
-// crossDenoiseRawRGBAImage with dual G / G2 variances, written to the Bayer
-// positions the forward writes (rawRGBAToBayer)
+// despeckleRawRGBAImage (demosaic.metal:1025-1092): the order statistics of
+// the 3 x 3 same-channel neighbourhood do not depend on theta; the clamp
+// thresholds do, through sigma = sqrt(var[c] * s)
+__global__ void __launch_bounds__(256) k_jvp_raw_despeckle(JvpPlanes P, RawDenoiseArgs a) {
+    const int qw = P.w / 2, qh = P.h / 2;
+    const int qx = blockIdx.x * blockDim.x + threadIdx.x, qy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (qx >= qw || qy >= qh) return;
+    const float2 g = reinterpret_cast<const float2*>(P.grad)[size_t(2 * qy) * P.w + 2 * qx];
+    const float gradient = sqrtf(g.x * g.x + g.y * g.y);
+    float tan[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const int ox = kBayer[a.pattern][c][0], oy = kBayer[a.pattern][c][1];
+        float fmx = 0, smx = 0, fmn = 65504.f, smn = 65504.f;
+        for (int i = -1; i <= 1; i++)
+            for (int j = -1; j <= 1; j++) {
+                const int sx = cl(qx + i, qw), sy = cl(qy + j, qh);
+                const float v = P.scaled0[size_t(2 * sy + oy) * P.w + 2 * sx + ox];
+                smx = v >= fmx ? fmx : fmaxf(v, smx);
+                fmx = fmaxf(v, fmx);
+                smn = v <= fmn ? fmn : fminf(v, smn);
+                fmn = fminf(v, fmn);
+            }
+        const float sv = P.scaled0[size_t(2 * qy + oy) * P.w + 2 * qx + ox];
+        const Dv var = {a.var[c], 0.f, (c == 1 || c == 3) ? 1.f : 0.f};
+        const Dv sigma = dsqrt_(var * sv);
+        const Dv tex = 1.f - 0.5f * dsmooth_(dc(1.f), dc(2.f), dc(gradient) / sigma);
+        const Dv mn = dmix_(dc(fmn), dc(smn), tex * (1.f - dsmooth_(2.f * sigma, 8.f * sigma, dc(smn - fmn))));
+        const Dv mx = dmix_(dc(fmx), dc(smx), tex * (1.f - dsmooth_(sigma, 4.f * sigma, dc(fmx - smx))));
+        tan[c] = dclamp_(dc(sv), mn, mx).b;
+    }
+    P.qtan[size_t(qy) * qw + qx] = make_float4(tan[0], tan[1], tan[2], tan[3]);
+}
+
+// crossDenoiseRawRGBAImage with dual G / G2 variances and dual quads,
+// written to the Bayer positions the forward writes (rawRGBAToBayer)
 __global__ void __launch_bounds__(256) k_jvp_cross_denoise(JvpPlanes P, RawDenoiseArgs a) {
     const int qw = P.w / 2, qh = P.h / 2;
     const int qx = blockIdx.x * blockDim.x + threadIdx.x, qy = blockIdx.y * blockDim.y + threadIdx.y;
     if (qx >= qw || qy >= qh) return;
-    const float4 p = reinterpret_cast<const float4*>(P.quad)[size_t(qy) * qw + qx];
-    const float pc[4] = {p.x, p.y, p.z, p.w};
+    auto quad = [&](int x, int y, Dv q[4]) {
+        const size_t i = size_t(y) * qw + x;
+        const float4 v = reinterpret_cast<const float4*>(P.quad)[i];
+        const float4 t = P.qtan[i];
+        q[0] = {v.x, 0.f, t.x};
+        q[1] = {v.y, 0.f, t.y};
+        q[2] = {v.z, 0.f, t.z};
+        q[3] = {v.w, 0.f, t.w};
+    };
+    Dv pc[4];
+    quad(qx, qy, pc);
     Dv inv[4];
 #pragma unroll
     for (int c = 0; c < 4; c++) {
         const Dv var = {a.var[c], 0.f, (c == 1 || c == 3) ? 1.f : 0.f};
-        inv[c] = dc(1.f) / (a.strength * dsqrt_(var * (pc[c] + 0.0001f)));
+        inv[c] = dc(1.f) / (a.strength * dsqrt_(var * (pc[c] + dc(0.0001f))));
     }
     Dv sum[4] = {dc(0.f), dc(0.f), dc(0.f), dc(0.f)}, sw = dc(0.f);
     for (int j = -2; j <= 2; j++)
         for (int i = -2; i <= 2; i++) {
-            const float4 s = reinterpret_cast<const float4*>(P.quad)[size_t(cl(qy + j, qh)) * qw + cl(qx + i, qw)];
-            const float sc[4] = {s.x, s.y, s.z, s.w};
+            Dv sc[4];
+            quad(cl(qx + i, qw), cl(qy + j, qh), sc);
             Dv d2 = dc(0.f);
 #pragma unroll
             for (int c = 0; c < 4; c++) {
@@ -356,9 +402,13 @@ __global__ void __launch_bounds__(256) k_jvp_despeckle_dot(JvpPlanes P, float va
 
 }  // namespace
 
+// scratch: quad tangents (float4, 16-byte aligned first), Bayer tangents
+// (float2), then the dual green, red/blue temporary and YCbCr planes
+static size_t quad_tan_bytes(int w, int h) { return size_t(w / 2) * size_t(h / 2) * sizeof(float4); }
+
 size_t front_jvp_scratch_bytes(int w, int h) {
     const size_t n = size_t(w) * h;
-    return n * sizeof(float2) + n * sizeof(Dv) * 7;
+    return quad_tan_bytes(w, h) + n * sizeof(float2) + n * sizeof(Dv) * 7;
 }
 
 int front_jvp_blocks(int w, int h) { return ((w + 31) / 32) * ((h + 7) / 8); }
@@ -370,19 +420,20 @@ void launch_front_jvp(const FrontJvpArgs& f, cudaStream_t s) {
     P.w = f.w;
     P.h = f.h;
     P.scaled = f.scaled;
+    P.scaled0 = f.scaled0;
     P.quad = f.quad;
     P.grad = f.grad;
-    P.rtan = reinterpret_cast<float2*>(sc);
-    P.green = reinterpret_cast<Dv*>(sc + n * sizeof(float2));
+    P.qtan = reinterpret_cast<float4*>(sc);
+    P.rtan = reinterpret_cast<float2*>(sc + quad_tan_bytes(f.w, f.h));
+    P.green = reinterpret_cast<Dv*>(sc + quad_tan_bytes(f.w, f.h) + n * sizeof(float2));
     P.tmp = P.green + n;
     P.ycc = P.tmp + 3 * n;
     const dim3 b(32, 8), g((f.w + 31) / 32, (f.h + 7) / 8);
-    if (f.high_noise) {
+    cudaMemsetAsync(P.rtan, 0, n * sizeof(float2), s);
+    if (f.high_noise) {  // the raw branch: despeckle, then cross denoise into the Bayer plane
         const dim3 gq((f.w / 2 + 31) / 32, (f.h / 2 + 7) / 8);
-        cudaMemsetAsync(P.rtan, 0, n * sizeof(float2), s);
+        k_jvp_raw_despeckle<<<gq, b, 0, s>>>(P, f.raw);
         k_jvp_cross_denoise<<<gq, b, 0, s>>>(P, f.raw);
-    } else {
-        cudaMemsetAsync(P.rtan, 0, n * sizeof(float2), s);
     }
     k_jvp_green<<<g, b, 0, s>>>(P, f.dm);
     k_jvp_red_blue<<<g, b, 0, s>>>(P, f.dm);

@@ -153,8 +153,9 @@ void launch_down_bwd(const float* g_coarse, int cw, int ch, float* g_fine, int w
 // ---- forward-mode tangents of the raw front end (gls_front_jvp.cu)
 struct FrontJvpArgs {
     int w, h;
-    const float* scaled;  // Bayer plane after the raw branch (forward, FP32)
-    const float* quad;    // despeckled quads of the raw branch (forward)
+    const float* scaled;   // Bayer plane after the raw branch (forward, FP32)
+    const float* scaled0;  // Bayer plane before the raw branch (forward, with high_noise)
+    const float* quad;     // despeckled quads of the raw branch (forward)
     const float* grad;    // 2 ch gradient plane (forward)
     int high_noise;       // the raw branch ran
     RawDenoiseArgs raw;
