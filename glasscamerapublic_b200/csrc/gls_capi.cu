@@ -914,8 +914,15 @@ gls_status gls_demosaic_batch(gls_converter* conv, gls_frame_desc* frames, int32
     }
     if (!conv->fork_ev) {
         GLS_CUDA(cudaEventCreateWithFlags(&conv->fork_ev, cudaEventDisableTiming));
+        // slot k one priority step below slot k - 1: the slots' frames finish
+        // one after another, lower slots filling the gaps, so each frame's
+        // copy-out overlaps the later frames' work instead of all of them
+        // queueing at the end of the batch
+        int least = 0, greatest = 0;
+        GLS_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
         for (int k = 0; k < kSlots; k++) {
-            GLS_CUDA(cudaStreamCreateWithFlags(&conv->slot_stream[k], cudaStreamNonBlocking));
+            const int prio = std::min(least, greatest + k);
+            GLS_CUDA(cudaStreamCreateWithPriority(&conv->slot_stream[k], cudaStreamNonBlocking, prio));
             GLS_CUDA(cudaEventCreateWithFlags(&conv->join_ev[k], cudaEventDisableTiming));
         }
     }
