@@ -176,6 +176,10 @@ struct gls_converter {
     Pipeline<float>& p32 = p32s[0];
     Pipeline<__half>& p16 = p16s[0];
     cudaStream_t slot_stream[kSlots] = {};
+    // host I/O of a batch: per slot, copy streams and the events that order
+    // them against the slot's kernels (staging buffers released / filled)
+    cudaStream_t cin_stream[kSlots] = {}, cout_stream[kSlots] = {};
+    cudaEvent_t raw_free[kSlots] = {}, raw_ready[kSlots] = {}, out_ready[kSlots] = {}, out_free[kSlots] = {};
     cudaEvent_t fork_ev = nullptr, join_ev[kSlots] = {};
     int last_storage = -1;  // GLS_F32 / GLS_F16 of the last single-frame call
     int last_levels = 0;
@@ -333,9 +337,19 @@ static gls_status pyramid_run(gls_converter* cv, Pipeline<S>& P, Plane<S, 4> img
     return GLS_OK;
 }
 
+// A batch slot's host copies on their own streams: the next frame's raw
+// upload waits only until the previous frame's scale_raw has read the raw
+// staging buffer, and its output transform only until the previous
+// frame's download has emptied the output staging buffer.
+struct SlotCopies {
+    cudaStream_t in, out;
+    cudaEvent_t raw_free, raw_ready, out_ready, out_free;
+};
+
 template <class S, class O>
 static gls_status finish_output(gls_converter* cv, Plane<S, 4> src, bool transform, const float* m, OutTarget<O>& t,
-                                cudaStream_t s) {
+                                cudaStream_t s, const SlotCopies* cp = nullptr) {
+    if (cp && t.copy_to_host) GLS_CUDA(cudaStreamWaitEvent(s, cp->out_free, 0));
     KScope k(cv->prof, KC_OUTPUT, s);
     if (transform) {
         Mat3Args ma;
@@ -347,8 +361,15 @@ static gls_status finish_output(gls_converter* cv, Plane<S, 4> src, bool transfo
     GLS_CUDA(cudaGetLastError());
     if (t.copy_to_host) {
         const size_t row = size_t(t.plane.w) * 4 * sizeof(O);
+        cudaStream_t cs = s;
+        if (cp) {
+            GLS_CUDA(cudaEventRecord(cp->out_ready, s));
+            GLS_CUDA(cudaStreamWaitEvent(cp->out, cp->out_ready, 0));
+            cs = cp->out;
+        }
         GLS_CUDA(cudaMemcpy2DAsync(t.host, t.host_stride, t.plane.p, t.plane.pitch * sizeof(O), row, t.plane.h,
-                                   cudaMemcpyDeviceToHost, s));
+                                   cudaMemcpyDeviceToHost, cs));
+        if (cp) GLS_CUDA(cudaEventRecord(cp->out_free, cp->out));
     }
     return GLS_OK;
 }
@@ -412,7 +433,7 @@ static DemosaicArgs demosaic_args(const gls_demosaic_params* p, bool transform) 
 template <class S>
 static gls_status demosaic_run(gls_converter* cv, const uint16_t* raw, int w, int h, size_t stride_bytes,
                                const gls_demosaic_params* p, uint32_t flags, gls_image_view* out, cudaStream_t s,
-                               int slot = 0) {
+                               int slot = 0, const SlotCopies* cp = nullptr) {
     Pipeline<S>& P =
         *reinterpret_cast<Pipeline<S>*>(is_half<S>::value ? (void*)&cv->p16s[slot] : (void*)&cv->p32s[slot]);
     const bool host_io = flags & GLS_HOST_IO;
@@ -423,8 +444,13 @@ static gls_status demosaic_run(gls_converter* cv, const uint16_t* raw, int w, in
     const uint16_t* rawp = raw;
     size_t raw_pitch = stride_bytes / 2;
     if (host_io) {
+        if (cp) GLS_CUDA(cudaStreamWaitEvent(cp->in, cp->raw_free, 0));
         GLS_CUDA(cudaMemcpy2DAsync(P.raw.p, size_t(w) * 2, raw, stride_bytes, size_t(w) * 2, h,
-                                   cudaMemcpyHostToDevice, s));
+                                   cudaMemcpyHostToDevice, cp ? cp->in : s));
+        if (cp) {
+            GLS_CUDA(cudaEventRecord(cp->raw_ready, cp->in));
+            GLS_CUDA(cudaStreamWaitEvent(s, cp->raw_ready, 0));
+        }
         rawp = static_cast<const uint16_t*>(P.raw.p);
         raw_pitch = size_t(w);
     } else if ((uintptr_t(raw) & 3) || (stride_bytes & 3)) {
@@ -451,6 +477,7 @@ static gls_status demosaic_run(gls_converter* cv, const uint16_t* raw, int w, in
         KScope k(cv->prof, KC_SCALE, s);
         launch_scale_raw<S>(rawp, raw_pitch, scaled, sa, s);
     }
+    if (cp && host_io) GLS_CUDA(cudaEventRecord(cp->raw_free, s));  // the raw staging buffer is read
 
     // rawImageSobel + sampledConvolutionSobel, raw_converter.cpp:185-193
     BlurArgs ba;
@@ -514,19 +541,21 @@ static gls_status demosaic_run(gls_converter* cv, const uint16_t* raw, int w, in
     if (out->dtype == GLS_F16) {
         OutTarget<__half> t;
         GLS_TRY(make_target<S, __half>(P, out, w, h, host_io, t));
-        GLS_TRY(finish_output<S, __half>(cv, final_src, denoise, y2c, t, s));
+        GLS_TRY(finish_output<S, __half>(cv, final_src, denoise, y2c, t, s, cp));
     } else {
         out->dtype = GLS_F32;
         OutTarget<float> t;
         GLS_TRY(make_target<S, float>(P, out, w, h, host_io, t));
-        GLS_TRY(finish_output<S, float>(cv, final_src, denoise, y2c, t, s));
+        GLS_TRY(finish_output<S, float>(cv, final_src, denoise, y2c, t, s, cp));
     }
     if (slot == 0) {
         cv->last_storage = is_half<S>::value ? GLS_F16 : GLS_F32;
         cv->last_w = w;
         cv->last_h = h;
         cv->last_denoise = denoise;
-        if (host_io || (flags & GLS_SYNC)) GLS_CUDA(cudaStreamSynchronize(s));
+        // a single frame returns with its result (the reference is
+        // synchronous); a batch synchronises once, after its join
+        if (!cp && (host_io || (flags & GLS_SYNC))) GLS_CUDA(cudaStreamSynchronize(s));
     }
     return GLS_OK;
 }
@@ -790,21 +819,34 @@ static gls_status enqueue_batch(gls_converter* conv, gls_frame_desc* frames, int
         slot_of[i] = k;
         load[k] += size_t(frames[i].width) * frames[i].height;
     }
+    const bool host_io = flags & GLS_HOST_IO;
+    std::vector<SlotCopies> cps(nslots);
     GLS_CUDA(cudaEventRecord(conv->fork_ev, s));
-    for (int k = 0; k < nslots; k++) GLS_CUDA(cudaStreamWaitEvent(conv->slot_stream[k], conv->fork_ev, 0));
+    for (int k = 0; k < nslots; k++) {
+        GLS_CUDA(cudaStreamWaitEvent(conv->slot_stream[k], conv->fork_ev, 0));
+        cps[k] = {conv->cin_stream[k], conv->cout_stream[k], conv->raw_free[k], conv->raw_ready[k],
+                  conv->out_ready[k], conv->out_free[k]};
+        if (host_io) {  // both staging buffers start free, after the caller's work
+            GLS_CUDA(cudaEventRecord(conv->raw_free[k], conv->slot_stream[k]));
+            GLS_CUDA(cudaEventRecord(conv->out_free[k], conv->slot_stream[k]));
+        }
+    }
     gls_status result = GLS_OK;
     for (int oi = 0; oi < n && result == GLS_OK; oi++) {
         const int i = order[oi];
         gls_frame_desc& f = frames[i];
         const int k = slot_of[i];
+        const SlotCopies* cp = host_io ? &cps[k] : nullptr;
         result = (flags & GLS_FP16_STORAGE)
                      ? demosaic_run<__half>(conv, f.raw, f.width, f.height, f.raw_stride_bytes, f.params, flags,
-                                            &f.out, conv->slot_stream[k], k)
+                                            &f.out, conv->slot_stream[k], k, cp)
                      : demosaic_run<float>(conv, f.raw, f.width, f.height, f.raw_stride_bytes, f.params, flags,
-                                           &f.out, conv->slot_stream[k], k);
+                                           &f.out, conv->slot_stream[k], k, cp);
     }
-    // join (also on error, so the caller's stream orders after whatever was queued)
+    // join (also on error, so the caller's stream orders after whatever was
+    // queued), downloads included
     for (int k = 0; k < nslots; k++) {
+        if (host_io) GLS_CUDA(cudaStreamWaitEvent(conv->slot_stream[k], conv->out_free[k], 0));
         GLS_CUDA(cudaEventRecord(conv->join_ev[k], conv->slot_stream[k]));
         GLS_CUDA(cudaStreamWaitEvent(s, conv->join_ev[k], 0));
     }
@@ -849,8 +891,11 @@ gls_status gls_converter_destroy(gls_converter* conv) {
     for (int k = 0; k < kSlots; k++) {
         conv->p32s[k].release();
         conv->p16s[k].release();
-        if (conv->slot_stream[k]) cudaStreamDestroy(conv->slot_stream[k]);
-        if (conv->join_ev[k]) cudaEventDestroy(conv->join_ev[k]);
+        for (cudaStream_t st : {conv->slot_stream[k], conv->cin_stream[k], conv->cout_stream[k]})
+            if (st) cudaStreamDestroy(st);
+        for (cudaEvent_t e : {conv->join_ev[k], conv->raw_free[k], conv->raw_ready[k], conv->out_ready[k],
+                              conv->out_free[k]})
+            if (e) cudaEventDestroy(e);
     }
     if (conv->fork_ev) cudaEventDestroy(conv->fork_ev);
     if (conv->graph_exec) cudaGraphExecDestroy(conv->graph_exec);
@@ -923,20 +968,23 @@ gls_status gls_demosaic_batch(gls_converter* conv, gls_frame_desc* frames, int32
         for (int k = 0; k < kSlots; k++) {
             const int prio = std::min(least, greatest + k);
             GLS_CUDA(cudaStreamCreateWithPriority(&conv->slot_stream[k], cudaStreamNonBlocking, prio));
-            GLS_CUDA(cudaEventCreateWithFlags(&conv->join_ev[k], cudaEventDisableTiming));
+            GLS_CUDA(cudaStreamCreateWithFlags(&conv->cin_stream[k], cudaStreamNonBlocking));
+            GLS_CUDA(cudaStreamCreateWithFlags(&conv->cout_stream[k], cudaStreamNonBlocking));
+            for (cudaEvent_t* e : {&conv->join_ev[k], &conv->raw_free[k], &conv->raw_ready[k], &conv->out_ready[k],
+                                   &conv->out_free[k]})
+                GLS_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
         }
     }
     const bool graph = flags & GLS_GRAPH;
     std::vector<uint64_t> key;
     if (graph) {
-        if (flags & (GLS_HOST_IO | GLS_HOST_PCA))
-            return set_error(GLS_ERR_INVALID_ARG, "GLS_GRAPH needs device buffers and the device PCA");
+        if (flags & GLS_HOST_PCA) return set_error(GLS_ERR_INVALID_ARG, "GLS_GRAPH needs the device PCA");
         if (!s) return set_error(GLS_ERR_INVALID_ARG, "GLS_GRAPH needs a stream other than the legacy default stream");
         if (conv->prof.on) return set_error(GLS_ERR_INVALID_ARG, "GLS_GRAPH cannot run with profiling enabled");
         key = batch_key(frames, n_frames, flags);
         if (!key.empty() && conv->graph_exec && key == conv->graph_key) {  // replay
             GLS_CUDA(cudaGraphLaunch(conv->graph_exec, s));
-            if (flags & GLS_SYNC) GLS_CUDA(cudaStreamSynchronize(s));
+            if (flags & (GLS_SYNC | GLS_HOST_IO)) GLS_CUDA(cudaStreamSynchronize(s));
             return GLS_OK;
         }
         if (key.empty()) return set_error(GLS_ERR_INVALID_ARG, "GLS_GRAPH needs caller-owned outputs");
@@ -956,7 +1004,8 @@ gls_status gls_demosaic_batch(gls_converter* conv, gls_frame_desc* frames, int32
         if (e != cudaSuccess) return set_error(GLS_ERR_CUDA, "batch capture: %s", cudaGetErrorString(e));
         if (conv->graph_exec) cudaGraphExecDestroy(conv->graph_exec);
         conv->graph_exec = nullptr;
-        const cudaError_t ie = cudaGraphInstantiate(&conv->graph_exec, g, 0);
+        // kernel nodes keep the slot streams' priorities (captured per node)
+        const cudaError_t ie = cudaGraphInstantiateWithFlags(&conv->graph_exec, g, cudaGraphInstantiateFlagUseNodePriority);
         cudaGraphDestroy(g);
         if (ie != cudaSuccess) {
             conv->graph_exec = nullptr;

@@ -170,11 +170,15 @@ typedef struct gls_frame_desc {
 /* Batched RawConverter::demosaic over frames of uneven sizes (no reference
  * counterpart: the reference converts one frame per call). Frames are
  * spread over the converter's slot streams, largest first onto the
- * least-loaded slot. With GLS_GRAPH (device buffers, caller-owned outputs,
- * device PCA, a non-default stream, at least 2 frames) the first call runs
- * the batch and records its launch sequence as a CUDA graph; later calls
- * with the same frames, buffers and parameter values replay that graph in
- * one launch. */
+ * least-loaded slot; slot k runs one stream priority below slot k - 1, so
+ * frames finish in turn. With GLS_HOST_IO (pinned host memory for full
+ * speed) each slot uploads and downloads on copy streams of its own, which
+ * overlap the other frames' kernels; the call returns when the outputs are
+ * in host memory. With GLS_GRAPH (caller-owned outputs, device PCA, a
+ * non-default stream, at least 2 frames) the first call runs the batch and
+ * records its launch sequence, copies included, as a CUDA graph; later
+ * calls with the same frames, buffers and parameter values replay that
+ * graph in one launch. */
 gls_status gls_demosaic_batch(gls_converter* conv, gls_frame_desc* frames, int32_t n_frames,
                               uint32_t flags, void* stream);
 

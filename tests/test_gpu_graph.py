@@ -60,3 +60,30 @@ def test_graph_replay_reads_new_contents_and_rerecords_on_new_params(converter):
     converter.demosaic_batch(raws, p2, got, stream=st, graph=True)
     st.synchronize()
     assert all(torch.equal(a, b) for a, b in zip(ref, got))
+
+
+def test_host_io_batch_stream_and_graph_match_device_batch(converter):
+    # pinned host buffers: per-slot copy streams; the graph records the
+    # copies too, and its replays read the current contents of the same
+    # host buffers
+    st = torch.cuda.Stream()
+    raws, params = _batch(400)
+    ref = _outs()
+    converter.demosaic_batch(raws, params, ref, stream=st)
+    st.synchronize()
+    hraw = [r.cpu().pin_memory() for r in raws]
+    hout = [torch.empty(o.shape, dtype=o.dtype).pin_memory() for o in ref]
+    converter.demosaic_batch(hraw, params, hout, stream=st)
+    assert all(torch.equal(a.cuda(), b) for a, b in zip(hout, ref))
+    for o in hout:
+        o.zero_()
+    converter.demosaic_batch(hraw, params, hout, stream=st, graph=True)  # runs and records
+    assert all(torch.equal(a.cuda(), b) for a, b in zip(hout, ref))
+    new_raws, _ = _batch(500)
+    for h, n in zip(hraw, new_raws):
+        h.copy_(n.cpu())
+    ref2 = _outs()
+    converter.demosaic_batch(new_raws, params, ref2, stream=st)
+    st.synchronize()
+    converter.demosaic_batch(hraw, params, hout, stream=st, graph=True)  # replays
+    assert all(torch.equal(a.cuda(), b) for a, b in zip(hout, ref2))
