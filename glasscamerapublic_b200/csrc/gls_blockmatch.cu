@@ -185,7 +185,8 @@ __global__ void __launch_bounds__(256) k_block_match_plain(Plane<S, 4> img, Plan
 // rows; a staged neighbour feeds 3.5 taps on average), tile 32 x 32, 256
 // threads. Shared memory per window position: the PCA coefficients minus
 // the tile-centre pixel's, as 8 halves, and (Y, Cb, Cr, |q'|^2) in FP32.
-//   * |p - q|^2 = |p'|^2 + |q'|^2 - 2 p'.q' (an 8-FMA dot product); the
+//   * |p - q|^2 = |p'|^2 + |q'|^2 - 2 p'.q' (an 8-FMA dot product, the
+//     -2 kl luma scale folded into the centre's coefficients); the
 //     centring keeps the cancellation error at FP32 rounding of the local
 //     variation of the coefficients;
 //   * lw is carried scaled by sqrt(2 log2 e), so the chroma exponent is
@@ -242,8 +243,8 @@ struct BmPairSmem {
 };
 
 struct BmPair {  // two pixels, each member of a pair register = one pixel
-    u64 p[8];             // p - c, per component
-    u64 kl, klm2, base;   // luma exponent terms
+    u64 p[8];             // -2 kl (p - c), per component
+    u64 kl, base;         // luma exponent terms
     u64 c1, c2, no1, no2; // chroma: e = c * v - o  (no = -o)
 };
 
@@ -260,10 +261,12 @@ __device__ __forceinline__ void bmp2_row(const Sm& sm, int base, int r, const Bm
                           pk2(a2.x, a2.x), pk2(a2.y, a2.y), pk2(a3.x, a3.x), pk2(a3.y, a3.y)};
         const u64 yy = pk2(y.x, y.x), cb = pk2(y.y, y.y), cr = pk2(y.z, y.z), nn = pk2(y.w, y.w);
         auto pair = [&](const BmPair& P, const float4 s, u64 (&ac)[5]) {
-            u64 dot = mul2(q[0], P.p[0]);
+            // ex = kl |q'|^2 - 2 kl p'.q' + base: the -2 kl scale rides in the
+            // stored coefficients and base starts the dot-product chain
+            u64 dot = fma2(q[0], P.p[0], P.base);
 #pragma unroll
             for (int c = 1; c < 8; c++) dot = fma2(q[c], P.p[c], dot);
-            const u64 ex = fma2(P.klm2, dot, fma2(P.kl, nn, P.base));
+            const u64 ex = fma2(P.kl, nn, dot);
             float e0, e1;
             upk2(ex, e0, e1);
             float l0, l1;
@@ -416,13 +419,11 @@ __global__ void __launch_bounds__(BxTile<TY>::THREADS, TY == 8 ? 2 : 3)
     }
     BmPair PA, PB;
     for (int c = 0; c < 8; c++) {
-        PA.p[c] = pk2(pc[0][c], pc[1][c]);
-        PB.p[c] = pk2(pc[2][c], pc[3][c]);
+        PA.p[c] = pk2(-2.f * kl[0] * pc[0][c], -2.f * kl[1] * pc[1][c]);
+        PB.p[c] = pk2(-2.f * kl[2] * pc[2][c], -2.f * kl[3] * pc[3][c]);
     }
     PA.kl = pk2(kl[0], kl[1]);
     PB.kl = pk2(kl[2], kl[3]);
-    PA.klm2 = pk2(-2.f * kl[0], -2.f * kl[1]);
-    PB.klm2 = pk2(-2.f * kl[2], -2.f * kl[3]);
     PA.base = pk2(base[0], base[1]);
     PB.base = pk2(base[2], base[3]);
     PA.c1 = pk2(c1[0], c1[1]);
