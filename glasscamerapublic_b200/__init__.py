@@ -149,6 +149,9 @@ _SIGNATURES = {
     "gls_demosaic_denoise_vjp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_size_t,
                                            C.POINTER(DemosaicParams), C.POINTER(ImageView), C.c_uint32,
                                            C.POINTER(C.c_double), C.POINTER(C.c_float), C.c_void_p]),
+    "gls_pyramid_denoise_vjp": (C.c_int, [C.c_void_p, C.POINTER(ImageView), C.POINTER(ImageView),
+                                          C.POINTER(DemosaicParams), C.POINTER(ImageView), C.c_uint32,
+                                          C.POINTER(C.c_float), C.POINTER(ImageView), C.c_void_p]),
     "gls_surf_create": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_float,
                                   C.POINTER(C.c_void_p)]),
     "gls_surf_destroy": (C.c_int, [C.c_void_p]),

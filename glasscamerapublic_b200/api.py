@@ -188,3 +188,23 @@ class PyramidProcessor:
         check(lib().gls_pyramid_denoise(self.converter.handle, C.byref(yv), C.byref(gv), C.byref(params), flags,
                                         C.byref(ov), None))
         return out
+
+    def denoise_vjp(self, ycc, gradient, params: DemosaicParams, g_out):
+        """Vector-Jacobian product of the FP32 denoise (gls_pyramid_denoise_vjp):
+        given g_out = dL/d(denoised Y, Cb, Cr) (H, W, 3|4), returns
+        (dL/dtheta [32], dL/d ycc (H, W, 3)), the PCA bases held fixed.
+        Float32 numpy arrays."""
+        ycc = np.ascontiguousarray(ycc, dtype=np.float32)
+        gradient = np.ascontiguousarray(gradient, dtype=np.float32)
+        g_out = np.ascontiguousarray(g_out, dtype=np.float32)
+        h, w = ycc.shape[:2]
+        g_ycc = np.empty((h, w, 3), dtype=np.float32)
+        grad = np.zeros(32, np.float32)
+        yv = _view_for_array(ycc, F32, 4)
+        gv = _view_for_array(gradient, F32, 2)
+        ov = _view_for_array(g_out, F32, g_out.shape[2])
+        iv = _view_for_array(g_ycc, F32, 3)
+        check(lib().gls_pyramid_denoise_vjp(self.converter.handle, C.byref(yv), C.byref(gv), C.byref(params),
+                                            C.byref(ov), HOST_IO, grad.ctypes.data_as(C.POINTER(C.c_float)),
+                                            C.byref(iv), None))
+        return grad, g_ycc

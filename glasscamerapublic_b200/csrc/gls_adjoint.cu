@@ -556,6 +556,40 @@ __global__ void __launch_bounds__(256) k_add_layer_grad(const float* __restrict_
     for (int c = 0; c < 3; c++) gi[size_t(i) * 3 + c] += gl[size_t(i) * 4 + c];
 }
 
+// 3-channel gradient planes to and from caller views of 3 or 4 channels
+__global__ void __launch_bounds__(256) k_pack3(const float* __restrict__ src, size_t pitch, int ch,
+                                              float* __restrict__ dst, int w, int h) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const float* p = src + size_t(y) * pitch + size_t(x) * ch;
+    float* o = dst + (size_t(y) * w + x) * 3;
+    o[0] = p[0];
+    o[1] = p[1];
+    o[2] = p[2];
+}
+
+__global__ void __launch_bounds__(256) k_unpack3(const float* __restrict__ src, float* __restrict__ dst, size_t pitch,
+                                                int ch, int w, int h) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const float* p = src + (size_t(y) * w + x) * 3;
+    float* o = dst + size_t(y) * pitch + size_t(x) * ch;
+    o[0] = p[0];
+    o[1] = p[1];
+    o[2] = p[2];
+    if (ch == 4) o[3] = 0.f;
+}
+
+void launch_pack3(const float* src, size_t pitch_floats, int channels, float* dst, int w, int h, cudaStream_t s) {
+    const dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
+    k_pack3<<<g, b, 0, s>>>(src, pitch_floats, channels, dst, w, h);
+}
+
+void launch_unpack3(const float* src, float* dst, size_t pitch_floats, int channels, int w, int h, cudaStream_t s) {
+    const dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
+    k_unpack3<<<g, b, 0, s>>>(src, dst, pitch_floats, channels, w, h);
+}
+
 size_t adjoint_center_smem() { return sizeof(CenterSmem); }
 size_t adjoint_neighbor_smem() { return sizeof(NeighborSmem); }
 

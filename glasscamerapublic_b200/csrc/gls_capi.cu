@@ -192,6 +192,7 @@ struct gls_converter {
     // adjoint scratch (gls_demosaic_denoise_vjp)
     DevBuf adj_gden[2], adj_rec, adj_glayer, adj_gpca, adj_gup, adj_part, adj_loss, adj_target;
     DevBuf adj_gimg, adj_gp1, adj_jvp, adj_jvp_part;  // dL/d(input pyramid), front-end tangents
+    DevBuf adj_gout;                                   // a caller's cotangent, packed (pyramid VJP)
     int adj_gimg_w = 0, adj_gimg_h = 0;                // size of the last dL/d(despeckled image)
 };
 
@@ -603,8 +604,13 @@ namespace gls {
 // loss head, then per level fine to coarse block matching transposed and,
 // below the coarsest level, the reconstruct step transposed into the next
 // level's denoised image. grad receives GLS_ADJ_NPARAMS values.
+// The reverse sweep over the FP32 forward's retained planes (slot 0).
+// Head: the MSE of the output RGB against `target` (loss and its
+// gradient), or, with target NULL, the given cotangent g_out3 (3 ch,
+// tightly packed) of the denoised YCbCr. front_end: add the raw front
+// end's tangents (parameters 30, 31; else 0).
 static gls_status adjoint_run(gls_converter* cv, const gls_demosaic_params* p, const float* target, int tstride,
-                              double* loss, float* grad, cudaStream_t s) {
+                              const float* g_out3, bool front_end, double* loss, float* grad, cudaStream_t s) {
     Pipeline<float>& P = cv->p32s[0];
     const int W = P.W, H = P.H, L = p->levels;
     const size_t n = size_t(W) * H;
@@ -644,8 +650,11 @@ static gls_status adjoint_run(gls_converter* cv, const gls_demosaic_params* p, c
     ha.inv_n = float(1.0 / (3.0 * double(n)));
     float* gcur = static_cast<float*>(cv->adj_gden[0].p);
     float* gnext = static_cast<float*>(cv->adj_gden[1].p);
-    launch_adj_head(static_cast<const float*>(P.den[0].p), target, tstride, W, H, ha, gcur,
-                    static_cast<double*>(cv->adj_loss.p), s);
+    if (target)
+        launch_adj_head(static_cast<const float*>(P.den[0].p), target, tstride, W, H, ha, gcur,
+                        static_cast<double*>(cv->adj_loss.p), s);
+    else
+        GLS_CUDA(cudaMemcpyAsync(gcur, g_out3, n * 3 * sizeof(float), cudaMemcpyDeviceToDevice, s));
     for (int i = 0; i < L; i++) {
         const int wi = W >> i, hi = H >> i;
         const gls_denoise_params& dp = p->denoise[i];
@@ -713,30 +722,34 @@ static gls_status adjoint_run(gls_converter* cv, const gls_demosaic_params* p, c
     for (int i = L - 2; i >= 0; i--)
         launch_down_bwd(gimg + gimg_off[i + 1], W >> (i + 1), H >> (i + 1), gimg + gimg_off[i], W >> i, H >> i, s);
     // the raw front end's tangents along theta30 / theta31, dotted with it
-    FrontJvpArgs fj;
-    fj.w = W;
-    fj.h = H;
-    fj.scaled = static_cast<const float*>(P.scaled.p);
-    fj.scaled0 = static_cast<const float*>(P.scaled0.p);
-    fj.quad = static_cast<const float*>(P.quad.p);
-    fj.grad = static_cast<const float*>(P.grad.p);
-    fj.high_noise = p->high_noise_image ? 1 : 0;
-    fj.raw = raw_denoise_args(p, false);
-    fj.dm = demosaic_args(p, true);
-    fj.despeckle_va = p->pyramid_nlf[0].a[0];
-    fj.despeckle_vb = p->pyramid_nlf[0].b[0];
-    fj.g_ds = gimg;
-    fj.scratch = cv->adj_jvp.p;
-    fj.part = static_cast<float*>(cv->adj_jvp_part.p);
-    launch_front_jvp(fj, s);
+    if (front_end) {
+        FrontJvpArgs fj;
+        fj.w = W;
+        fj.h = H;
+        fj.scaled = static_cast<const float*>(P.scaled.p);
+        fj.scaled0 = static_cast<const float*>(P.scaled0.p);
+        fj.quad = static_cast<const float*>(P.quad.p);
+        fj.grad = static_cast<const float*>(P.grad.p);
+        fj.high_noise = p->high_noise_image ? 1 : 0;
+        fj.raw = raw_denoise_args(p, false);
+        fj.dm = demosaic_args(p, true);
+        fj.despeckle_va = p->pyramid_nlf[0].a[0];
+        fj.despeckle_vb = p->pyramid_nlf[0].b[0];
+        fj.g_ds = gimg;
+        fj.scratch = cv->adj_jvp.p;
+        fj.part = static_cast<float*>(cv->adj_jvp_part.p);
+        launch_front_jvp(fj, s);
+    }
     cv->adj_gimg_w = W;
     cv->adj_gimg_h = H;
     GLS_CUDA(cudaGetLastError());
-    std::vector<float> hp(parts), hj(size_t(jvp_blocks) * 2);
-    std::vector<double> hl(head_blocks);
+    std::vector<float> hp(parts), hj(front_end ? size_t(jvp_blocks) * 2 : 0);
+    std::vector<double> hl(target ? head_blocks : 0);
     if (parts) GLS_CUDA(cudaMemcpyAsync(hp.data(), part, parts * sizeof(float), cudaMemcpyDeviceToHost, s));
-    GLS_CUDA(cudaMemcpyAsync(hj.data(), cv->adj_jvp_part.p, hj.size() * sizeof(float), cudaMemcpyDeviceToHost, s));
-    GLS_CUDA(cudaMemcpyAsync(hl.data(), cv->adj_loss.p, hl.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (!hj.empty())
+        GLS_CUDA(cudaMemcpyAsync(hj.data(), cv->adj_jvp_part.p, hj.size() * sizeof(float), cudaMemcpyDeviceToHost, s));
+    if (!hl.empty())
+        GLS_CUDA(cudaMemcpyAsync(hl.data(), cv->adj_loss.p, hl.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
     GLS_CUDA(cudaStreamSynchronize(s));
     double g[GLS_ADJ_NPARAMS] = {};
     for (int i = 0; i < L; i++) {
@@ -766,9 +779,9 @@ static gls_status adjoint_run(gls_converter* cv, const gls_demosaic_params* p, c
     double lsum = 0;
     for (double v : hl) lsum += v;
     if (loss) *loss = lsum / (3.0 * double(n));
-    for (int b = 0; b < jvp_blocks; b++) {
-        g[GLS_ADJ_RAW_GREEN_A] += hj[size_t(b) * 2];
-        g[GLS_ADJ_RAW_GREEN_B] += hj[size_t(b) * 2 + 1];
+    for (size_t b = 0; b < hj.size() / 2; b++) {
+        g[GLS_ADJ_RAW_GREEN_A] += hj[b * 2];
+        g[GLS_ADJ_RAW_GREEN_B] += hj[b * 2 + 1];
     }
     for (int k = 0; k < GLS_ADJ_NPARAMS; k++) grad[k] = float(g[k]);
     return GLS_OK;
@@ -901,7 +914,7 @@ gls_status gls_converter_destroy(gls_converter* conv) {
     if (conv->graph_exec) cudaGraphExecDestroy(conv->graph_exec);
     for (DevBuf* b : {&conv->adj_gden[0], &conv->adj_gden[1], &conv->adj_rec, &conv->adj_glayer, &conv->adj_gpca,
                       &conv->adj_gup, &conv->adj_part, &conv->adj_loss, &conv->adj_target, &conv->adj_gimg,
-                      &conv->adj_gp1, &conv->adj_jvp, &conv->adj_jvp_part})
+                      &conv->adj_gp1, &conv->adj_jvp, &conv->adj_jvp_part, &conv->adj_gout})
         b->release();
     delete conv;
     return GLS_OK;
@@ -1192,7 +1205,74 @@ gls_status gls_demosaic_denoise_vjp(gls_converter* conv, const uint16_t* raw, in
                                    (flags & GLS_HOST_IO) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
         tp = static_cast<const float*>(conv->adj_target.p);
     }
-    return adjoint_run(conv, params, tp, target->channels, loss, grad, s);
+    return adjoint_run(conv, params, tp, target->channels, nullptr, true, loss, grad, s);
+}
+
+gls_status gls_pyramid_denoise_vjp(gls_converter* conv, const gls_image_view* ycc, const gls_image_view* gradient,
+                                   const gls_demosaic_params* params, const gls_image_view* g_out, uint32_t flags,
+                                   float* grad, gls_image_view* g_ycc, void* stream) {
+    clear_error();
+    if (!conv || !ycc || !gradient || !params || !g_out || !g_out->data || !grad)
+        return set_error(GLS_ERR_INVALID_ARG, "NULL argument");
+    if (params->levels < 1 || params->levels > GLS_MAX_LEVELS) return set_error(GLS_ERR_INVALID_ARG, "bad levels");
+    const int w = ycc->width, h = ycc->height;
+    if (gradient->width != w || gradient->height != h) return set_error(GLS_ERR_INVALID_ARG, "gradient and image sizes differ");
+    if (w < 1 || h < 1 || (w >> (params->levels - 1)) < 1 || (h >> (params->levels - 1)) < 1)
+        return set_error(GLS_ERR_INVALID_ARG, "image too small for the pyramid");
+    auto check3 = [&](const gls_image_view* v, const char* what) -> gls_status {
+        if (v->width != w || v->height != h || v->dtype != GLS_F32 || (v->channels != 3 && v->channels != 4))
+            return set_error(GLS_ERR_INVALID_ARG, "%s must be a %dx%d GLS_F32 view of 3 or 4 channels", what, w, h);
+        const size_t row = size_t(w) * v->channels * 4;
+        const size_t st = v->stride_bytes ? v->stride_bytes : row;
+        if (st < row || st % 4) return set_error(GLS_ERR_INVALID_ARG, "bad %s stride", what);
+        return GLS_OK;
+    };
+    GLS_TRY(check3(g_out, "g_out"));
+    if (g_ycc) {
+        if (!g_ycc->data) return set_error(GLS_ERR_INVALID_ARG, "g_ycc has no data");
+        GLS_TRY(check3(g_ycc, "g_ycc"));
+    }
+    GLS_CUDA(cudaSetDevice(conv->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const bool host_io = flags & GLS_HOST_IO;
+    gls_image_view out{};  // converter-owned FP32 output
+    out.dtype = GLS_F32;
+    conv->keep_nc = true;
+    const gls_status fst = pyramid_only<float>(conv, ycc, gradient, params, GLS_DENOISE | (flags & GLS_HOST_IO), &out, s);
+    conv->keep_nc = false;
+    GLS_TRY(fst);
+    const size_t n = size_t(w) * h;
+    GLS_TRY(conv->adj_gout.ensure(n * 3 * sizeof(float)));
+    float* g3 = static_cast<float*>(conv->adj_gout.p);
+    {  // the cotangent into a packed 3-channel plane
+        const size_t row = size_t(w) * g_out->channels * 4;
+        const size_t st = g_out->stride_bytes ? g_out->stride_bytes : row;
+        const float* src = static_cast<const float*>(g_out->data);
+        size_t pitch = st / 4;
+        if (host_io) {
+            GLS_TRY(conv->adj_target.ensure(size_t(h) * row));
+            GLS_CUDA(cudaMemcpy2DAsync(conv->adj_target.p, row, g_out->data, st, row, h, cudaMemcpyHostToDevice, s));
+            src = static_cast<const float*>(conv->adj_target.p);
+            pitch = row / 4;
+        }
+        launch_pack3(src, pitch, g_out->channels, g3, w, h, s);
+    }
+    GLS_TRY(adjoint_run(conv, params, nullptr, 0, g3, false, nullptr, grad, s));
+    if (g_ycc) {
+        const size_t row = size_t(w) * g_ycc->channels * 4;
+        const size_t st = g_ycc->stride_bytes ? g_ycc->stride_bytes : row;
+        const float* gi = static_cast<const float*>(conv->adj_gimg.p);  // level 0 first
+        if (host_io) {
+            GLS_TRY(conv->adj_target.ensure(size_t(h) * row));
+            launch_unpack3(gi, static_cast<float*>(conv->adj_target.p), row / 4, g_ycc->channels, w, h, s);
+            GLS_CUDA(cudaMemcpy2DAsync(g_ycc->data, st, conv->adj_target.p, row, row, h, cudaMemcpyDeviceToHost, s));
+        } else {
+            launch_unpack3(gi, static_cast<float*>(g_ycc->data), st / 4, g_ycc->channels, w, h, s);
+        }
+        GLS_CUDA(cudaGetLastError());
+    }
+    GLS_CUDA(cudaStreamSynchronize(s));
+    return GLS_OK;
 }
 
 

@@ -150,6 +150,11 @@ void launch_add_layer_grad(const float* g_layer, float* g_img, int w, int h, cud
 // (k_downsample) applied to g_coarse (3 ch, cw x ch)
 void launch_down_bwd(const float* g_coarse, int cw, int ch, float* g_fine, int w, int h, cudaStream_t s);
 
+// 3-channel planes (tightly packed) from / to views of 3 or 4 channels
+// (pitch in floats; a fourth channel is written as 0)
+void launch_pack3(const float* src, size_t pitch_floats, int channels, float* dst, int w, int h, cudaStream_t s);
+void launch_unpack3(const float* src, float* dst, size_t pitch_floats, int channels, int w, int h, cudaStream_t s);
+
 // ---- forward-mode tangents of the raw front end (gls_front_jvp.cu)
 struct FrontJvpArgs {
     int w, h;

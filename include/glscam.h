@@ -298,6 +298,21 @@ gls_status gls_demosaic_denoise_vjp(gls_converter* conv, const uint16_t* raw, in
                                     const gls_image_view* target, uint32_t flags, double* loss, float* grad,
                                     void* stream);
 
+/* Vector-Jacobian product of PyramidProcessor<levels>::denoise (no
+ * reference counterpart; the denoise-only counterpart of
+ * gls_demosaic_denoise_vjp, as gls_pyramid_denoise is of gls_demosaic).
+ * The FP32 denoise of ycc (4 ch YCbCr) and gradient (2 ch) runs first, as
+ * gls_pyramid_denoise without GLS_FP16_STORAGE. Given g_out = dL/d(denoised
+ * Y, Cb, Cr) (GLS_F32, 3 or 4 channels, a fourth ignored), grad receives
+ * GLS_ADJ_NPARAMS entries, dL/dtheta of the pyramid parameters (the
+ * raw-green entries are 0: they act before this stage), and g_ycc, unless
+ * NULL, dL/d(ycc) (GLS_F32, 3 or 4 channels; a fourth is written 0). Each
+ * level's PCA basis is held fixed. Views are device memory, or host memory
+ * with GLS_HOST_IO. Synchronises the stream. */
+gls_status gls_pyramid_denoise_vjp(gls_converter* conv, const gls_image_view* ycc, const gls_image_view* gradient,
+                                   const gls_demosaic_params* params, const gls_image_view* g_out, uint32_t flags,
+                                   float* grad, gls_image_view* g_ycc, void* stream);
+
 /* ==== Registration and fusion (ImageRegistration/, PyramidFusion/) ==== */
 
 /* KeyPoint (ImageRegistration/feature2d.hpp:25-47), 28 bytes. angle is in

@@ -130,12 +130,27 @@ class RawConverter {
         check(gls_demosaic(conv_, raw, width, height, stride_bytes, params, flags, out, stream));
     }
 
-    // many frames of any sizes in one call (no reference counterpart)
+    // many frames of any sizes in one call (no reference counterpart); graph
+    // records the batch and replays it while frames, buffers and
+    // parameters stay the same
     void demosaic_batch(std::vector<gls_frame_desc>& frames, bool noiseReduction = true, bool fp16 = true,
-                        bool host_io = false, void* stream = nullptr) {
+                        bool host_io = false, void* stream = nullptr, bool graph = false) {
         uint32_t flags = flag_if(noiseReduction, GLS_DENOISE) | flag_if(fp16, GLS_FP16_STORAGE) |
-                         flag_if(host_io, GLS_HOST_IO);
+                         flag_if(host_io, GLS_HOST_IO) | flag_if(graph, GLS_GRAPH);
         check(gls_demosaic_batch(conv_, frames.data(), int32_t(frames.size()), flags, stream));
+    }
+
+    // calibration gradient (no reference counterpart): the MSE of the FP32
+    // path's RGB against target (F32 RGB or RGBA) and its gradient with
+    // respect to the GLS_ADJ_NPARAMS parameters (gls_demosaic_denoise_vjp)
+    double demosaic_denoise_vjp(const uint16_t* raw, int width, int height, size_t stride_bytes,
+                                const DemosaicParameters* params, const ImageView& target,
+                                std::array<float, GLS_ADJ_NPARAMS>* grad, bool host_io = false,
+                                void* stream = nullptr) {
+        double loss = 0;
+        check(gls_demosaic_denoise_vjp(conv_, raw, width, height, stride_bytes, params, &target,
+                                       flag_if(host_io, GLS_HOST_IO), &loss, grad->data(), stream));
+        return loss;
     }
 
     gls_converter* handle() const { return conv_; }
@@ -158,6 +173,18 @@ class PyramidProcessor {
         p.levels = int32_t(levels);
         uint32_t flags = flag_if(fp16, GLS_FP16_STORAGE) | flag_if(host_io, GLS_HOST_IO | GLS_SYNC);
         check(gls_pyramid_denoise(conv_, &ycc, &gradient, &p, flags, out, stream));
+    }
+
+    // the denoise's vector-Jacobian product (gls_pyramid_denoise_vjp):
+    // g_out = dL/d(denoised YCbCr) in; dL/dtheta and, if g_ycc is given,
+    // dL/d(ycc) out
+    void denoise_vjp(const ImageView& ycc, const ImageView& gradient, const DemosaicParameters* params,
+                     const ImageView& g_out, std::array<float, GLS_ADJ_NPARAMS>* grad, ImageView* g_ycc = nullptr,
+                     bool host_io = false, void* stream = nullptr) {
+        DemosaicParameters p = *params;
+        p.levels = int32_t(levels);
+        check(gls_pyramid_denoise_vjp(conv_, &ycc, &gradient, &p, &g_out, flag_if(host_io, GLS_HOST_IO), grad->data(),
+                                      g_ycc, stream));
     }
 
    private:

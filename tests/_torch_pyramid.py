@@ -178,3 +178,17 @@ def loss_and_grad(ds, grad, params, bases, y2c, target, with_ds: bool = False):
     if with_ds:
         res = res + (dst.grad.detach()[..., :3].numpy(),)
     return res
+
+
+def vjp(ds, grad, params, bases, g_out):
+    """dL/dtheta (first 30 entries; NaN for the raw-green ones) and dL/d(ds)
+    (h, w, 3) of L = sum(g_out * denoised YCbCr), by autograd of the float64
+    re-expression (bases held fixed)."""
+    theta = theta_from_params(params, params.levels).requires_grad_(True)
+    dst = torch.as_tensor(ds, dtype=torch.float64).clone().requires_grad_(True)
+    den0 = pyramid_rgb(dst, torch.as_tensor(grad, dtype=torch.float64), theta, params,
+                       torch.as_tensor(bases, dtype=torch.float64), torch.eye(3, dtype=torch.float64))
+    (den0 * torch.as_tensor(g_out, dtype=torch.float64)[..., :3]).sum().backward()
+    g = theta.grad.detach().clone()
+    g[30:] = float("nan")
+    return g.numpy(), dst.grad.detach()[..., :3].numpy()

@@ -133,3 +133,26 @@ def test_adjoint_device_inputs_and_autograd_function(converter):
     loss.backward()
     assert abs(float(loss.detach()) - l0) <= 1e-6 * l0
     assert np.allclose(theta.grad.numpy(), g0.astype(np.float64), rtol=1e-6, atol=0)
+
+
+def test_pyramid_denoise_vjp_matches_autograd(converter):
+    # the denoise-only VJP: a random cotangent of the denoised YCbCr
+    wl = scene.Workload("adj", 160, 112, levels=3, gain=0.8, read=3.0, iso=800, seed=81)
+    raw, _ = scene.make_raw(wl)
+    p = scene.make_params(wl)
+    converter.demosaic(raw, p)  # a realistic despeckled image and gradient
+    ds = converter.plane(g.PLANE_DESPECKLED)
+    grad = converter.plane(g.PLANE_GRADIENT)
+    rng = np.random.default_rng(5)
+    g_out = rng.standard_normal((112, 160, 4)).astype(np.float32) * 1e-3
+    pp = g.PyramidProcessor(converter)
+    gt, g_ycc = pp.denoise_vjp(ds, grad, p, g_out)
+    bases = np.stack([converter.pca_basis(l) for l in range(3)]).astype(np.float64)
+    g_ref, gds_ref = TP.vjp(ds, grad, p, bases, g_out)
+    assert np.all(gt[30:] == 0) and np.all(gt[3:5] == 0)
+    for kind in range(6):
+        sl = slice(5 * kind, 5 * kind + 3)
+        ref = g_ref[sl]
+        tol = 2e-3 * np.abs(ref) + 1e-3 * np.abs(ref).max() + 1e-30
+        assert np.all(np.abs(gt[sl] - ref) <= tol), (kind, gt[sl], ref)
+    assert np.abs(g_ycc - gds_ref).max() <= 1e-3 * np.abs(gds_ref).max()
