@@ -625,9 +625,11 @@ static gls_status adjoint_run(gls_converter* cv, const gls_demosaic_params* p, c
     for (int i = 0; i < L; i++) gimg_off[i + 1] = gimg_off[i] + size_t(W >> i) * (H >> i) * 3;
     GLS_TRY(cv->adj_gimg.ensure(gimg_off[L] * sizeof(float)));
     GLS_TRY(cv->adj_gp1.ensure(n * 3 * sizeof(float)));
-    GLS_TRY(cv->adj_jvp.ensure(front_jvp_scratch_bytes(W, H)));
     const int jvp_blocks = front_jvp_blocks(W, H);
-    GLS_TRY(cv->adj_jvp_part.ensure(size_t(jvp_blocks) * 2 * sizeof(float)));
+    if (front_end) {
+        GLS_TRY(cv->adj_jvp.ensure(front_jvp_scratch_bytes(W, H)));
+        GLS_TRY(cv->adj_jvp_part.ensure(size_t(jvp_blocks) * 2 * sizeof(float)));
+    }
     float* gimg = static_cast<float*>(cv->adj_gimg.p);
     GLS_CUDA(cudaMemsetAsync(gimg, 0, gimg_off[L] * sizeof(float), s));
     std::vector<size_t> bm_off(L), sn_off(L);
