@@ -66,6 +66,26 @@ class RawNLF(C.Structure):
     _fields_ = [("a", C.c_float * 4), ("b", C.c_float * 4)]
 
 
+class RgbConversionParams(C.Structure):
+    _fields_ = [
+        ("contrast", C.c_float),
+        ("saturation", C.c_float),
+        ("tone_curve_slope", C.c_float),
+        ("exposure_bias", C.c_float),
+        ("blacks", C.c_float),
+        ("local_tone_mapping", C.c_int32),
+    ]
+
+
+class LtmParams(C.Structure):
+    _fields_ = [
+        ("eps", C.c_float),
+        ("shadows", C.c_float),
+        ("highlights", C.c_float),
+        ("detail", C.c_float * 3),
+    ]
+
+
 class DemosaicParams(C.Structure):
     _fields_ = [
         ("bayer_pattern", C.c_int32),
@@ -83,6 +103,8 @@ class DemosaicParams(C.Structure):
         ("denoise", DenoiseParams * MAX_LEVELS),
         ("levels", C.c_int32),
         ("iso", C.c_int32),
+        ("rgb_conversion", RgbConversionParams),
+        ("ltm", LtmParams),
     ]
 
 
@@ -144,6 +166,7 @@ _SIGNATURES = {
     "gls_converter_stats": (C.c_int, [C.c_void_p, C.POINTER(KernelStat), C.c_int32, C.POINTER(C.c_int32)]),
     "gls_converter_reset_stats": (C.c_int, [C.c_void_p]),
     "gls_block_match_tiles": (C.c_int, [C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)]),
+    "gls_grain_tables": (C.c_int, [C.c_uint32, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     "gls_calibration_fill": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(DemosaicParams)]),
     "gls_gaussian_bilinear_taps": (C.c_int, [C.c_float, C.POINTER(C.c_float), C.c_int32, C.POINTER(C.c_int32)]),
     "gls_demosaic_denoise_vjp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_size_t,

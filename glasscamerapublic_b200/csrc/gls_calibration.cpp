@@ -176,7 +176,20 @@ gls_status calibration_fill(int camera, int iso, gls_demosaic_params* p) {
     if (iso <= 0) return set_error(GLS_ERR_RANGE, "gls_calibration_fill: ISO must be positive");
     iphone14wide_nlf(iso, p);
     iphone14wide_denoise(iso, p);
-    p->lens_shading_correction = 1.6f;  // buildDemosaicParameters, iPhone14WideCalibration.cpp:121-137
+    // buildDemosaicParameters, iPhone14WideCalibration.cpp:121-137
+    p->lens_shading_correction = 1.6f;
+    p->rgb_conversion.contrast = 1.05f;
+    p->rgb_conversion.saturation = 1.0f;
+    p->rgb_conversion.tone_curve_slope = 3.5f;
+    p->rgb_conversion.exposure_bias = 0.0f;
+    p->rgb_conversion.blacks = 0.0f;
+    p->rgb_conversion.local_tone_mapping = 1;
+    p->ltm.eps = 0.01f;
+    p->ltm.shadows = 1.0f;
+    p->ltm.highlights = 1.0f;
+    p->ltm.detail[0] = 1.0f;
+    p->ltm.detail[1] = 1.5f;
+    p->ltm.detail[2] = 2.0f;
     if (p->levels <= 0) p->levels = 5;
     return GLS_OK;
 }

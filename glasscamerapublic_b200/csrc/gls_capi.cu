@@ -14,6 +14,7 @@
 #include "gls_devbuf.h"
 #include "gls_host.h"
 #include "gls_kernels.h"
+#include "gls_noise.h"
 
 namespace gls {
 
@@ -42,6 +43,7 @@ struct Pipeline {
     int W = 0, H = 0, L = 0;
     DevBuf raw, scaled, grad, quad, A, B, pca, acc, basis, status;
     DevBuf scaled0;  // the Bayer plane before the raw branch, kept only for the adjoint
+    DevBuf post_hist, post_stats, post_perm, post_gtab, post_ab;  // display post-processing scratch
     DevBuf img[GLS_MAX_LEVELS], gradp[GLS_MAX_LEVELS], sub[GLS_MAX_LEVELS], den[GLS_MAX_LEVELS];
     DevBuf nc[GLS_MAX_LEVELS];  // chroma norms, kept only for the adjoint
     DevBuf out_f32, out_f16, stage_in, stage_grad;
@@ -76,7 +78,7 @@ struct Pipeline {
     }
     void release() {
         for (DevBuf* b : {&raw, &scaled, &scaled0, &grad, &quad, &A, &B, &pca, &acc, &basis, &status, &out_f32,
-                          &out_f16, &stage_in, &stage_grad})
+                          &out_f16, &stage_in, &stage_grad, &post_hist, &post_stats, &post_perm, &post_gtab, &post_ab})
             b->release();
         for (int i = 0; i < GLS_MAX_LEVELS; i++) {
             img[i].release();
@@ -253,6 +255,15 @@ struct OutTarget {
     size_t host_stride = 0;
 };
 
+// The display post-processing reads the histogram of denoised level 3 and
+// guides the tone mapping with levels 4, 2 and 0: the reference's 5-level
+// pyramid (raw_converter.cpp:88-110).
+static gls_status check_post(const gls_demosaic_params* p, uint32_t flags) {
+    if (!(flags & GLS_POSTPROCESS) || !(flags & GLS_DENOISE) || !p) return GLS_OK;
+    if (p->levels != 5) return set_error(GLS_ERR_INVALID_ARG, "post-processing needs the 5-level pyramid");
+    return GLS_OK;
+}
+
 template <class S>
 static gls_status pyramid_run(gls_converter* cv, Pipeline<S>& P, Plane<S, 4> img0, Plane<S, 2> grad0,
                               const gls_demosaic_params* p, uint32_t flags, cudaStream_t s) {
@@ -349,10 +360,12 @@ struct SlotCopies {
 
 template <class S, class O>
 static gls_status finish_output(gls_converter* cv, Plane<S, 4> src, bool transform, const float* m, OutTarget<O>& t,
-                                cudaStream_t s, const SlotCopies* cp = nullptr) {
+                                cudaStream_t s, const SlotCopies* cp = nullptr, const PostArgs<S>* post = nullptr) {
     if (cp && t.copy_to_host) GLS_CUDA(cudaStreamWaitEvent(s, cp->out_free, 0));
     KScope k(cv->prof, KC_OUTPUT, s);
-    if (transform) {
+    if (post) {  // the display post-processing writes the output
+        launch_post<S, O>(*post, t.plane, s);
+    } else if (transform) {
         Mat3Args ma;
         std::memcpy(ma.m, m, sizeof(ma.m));
         launch_transform<S, O>(src, t.plane, ma, s);
@@ -538,16 +551,39 @@ static gls_status demosaic_run(gls_converter* cv, const uint16_t* raw, int w, in
         GLS_TRY(pyramid_run<S>(cv, P, B, grad, p, flags, s));
         final_src = plane<S, 4>(P.den[0], w, h);
     }
+    // display post-processing (raw_converter.cpp:80-116, 231-244)
+    PostArgs<S> pa{};
+    const bool post = flags & GLS_POSTPROCESS;
+    if (post) {
+        pa.params = p;
+        std::memcpy(pa.y2c, y2c, sizeof(pa.y2c));
+        pa.denoise = denoise;
+        if (denoise)
+            for (int l = 0; l < 5; l++) pa.den[l] = plane<S, 4>(P.den[l], w >> l, h >> l);
+        pa.rgb = A;
+        pa.grad2 = grad;
+        pa.raw = rawp;
+        GLS_TRY(P.post_hist.ensure(256 * sizeof(uint32_t)));
+        GLS_TRY(P.post_stats.ensure(sizeof(PostStats)));
+        GLS_TRY(P.post_perm.ensure(kNoiseSize * sizeof(int)));
+        GLS_TRY(P.post_gtab.ensure(kNoiseSize * 2 * sizeof(float)));
+        GLS_TRY(P.post_ab.ensure(post_ab_bytes(w, h)));
+        pa.hist = static_cast<uint32_t*>(P.post_hist.p);
+        pa.stats = static_cast<PostStats*>(P.post_stats.p);
+        pa.perm = static_cast<int*>(P.post_perm.p);
+        pa.grad_tab = static_cast<float*>(P.post_gtab.p);
+        pa.ab = static_cast<float2*>(P.post_ab.p);
+    }
     // transformImage(YCbCr -> cam), raw_converter.cpp:219
     if (out->dtype == GLS_F16) {
         OutTarget<__half> t;
         GLS_TRY(make_target<S, __half>(P, out, w, h, host_io, t));
-        GLS_TRY(finish_output<S, __half>(cv, final_src, denoise, y2c, t, s, cp));
+        GLS_TRY(finish_output<S, __half>(cv, final_src, denoise, y2c, t, s, cp, post ? &pa : nullptr));
     } else {
         out->dtype = GLS_F32;
         OutTarget<float> t;
         GLS_TRY(make_target<S, float>(P, out, w, h, host_io, t));
-        GLS_TRY(finish_output<S, float>(cv, final_src, denoise, y2c, t, s, cp));
+        GLS_TRY(finish_output<S, float>(cv, final_src, denoise, y2c, t, s, cp, post ? &pa : nullptr));
     }
     if (slot == 0) {
         cv->last_storage = is_half<S>::value ? GLS_F16 : GLS_F32;
@@ -927,9 +963,8 @@ gls_status gls_demosaic(gls_converter* conv, const uint16_t* raw, int32_t width,
                         gls_image_view* out, void* stream) {
     clear_error();
     if (!conv || !raw || !out) return set_error(GLS_ERR_INVALID_ARG, "converter, raw and out must not be NULL");
-    if (flags & GLS_POSTPROCESS)
-        return set_error(GLS_ERR_UNSUPPORTED, "sRGB post-processing is not part of this path (linear camera RGB only)");
     GLS_TRY(check_params(params, width, height));
+    GLS_TRY(check_post(params, flags));
     if (raw_stride_bytes == 0) raw_stride_bytes = size_t(width) * 2;
     if (raw_stride_bytes < size_t(width) * 2) return set_error(GLS_ERR_INVALID_ARG, "raw stride too small");
     if (out->dtype != GLS_F32 && out->dtype != GLS_F16) return set_error(GLS_ERR_INVALID_ARG, "output dtype must be F32 or F16");
@@ -944,10 +979,9 @@ gls_status gls_demosaic_batch(gls_converter* conv, gls_frame_desc* frames, int32
                               void* stream) {
     clear_error();
     if (!conv || (!frames && n_frames > 0) || n_frames < 0) return set_error(GLS_ERR_INVALID_ARG, "bad batch");
-    if (flags & GLS_POSTPROCESS)
-        return set_error(GLS_ERR_UNSUPPORTED, "sRGB post-processing is not part of this path (linear camera RGB only)");
     for (int i = 0; i < n_frames; i++) {  // validate every frame before any work is queued
         gls_frame_desc& f = frames[i];
+        GLS_TRY(check_post(f.params, flags));
         if (!f.raw) return set_error(GLS_ERR_INVALID_ARG, "frame %d: raw is NULL", i);
         gls_status st = check_params(f.params, f.width, f.height);
         if (st != GLS_OK) return st;
@@ -1285,6 +1319,15 @@ gls_status gls_block_match_tiles(int32_t* entries, int32_t max_entries, int32_t*
     const int c = bm_tile_list(buf.data(), std::max(max_entries, 0));
     for (int i = 0; i < std::min(c, max_entries) * 3; i++) entries[i] = buf[i];
     *n = c;
+    return GLS_OK;
+}
+
+gls_status gls_grain_tables(uint32_t seed, int32_t* perm, float* grad) {
+    clear_error();
+    if (!perm || !grad) return set_error(GLS_ERR_INVALID_ARG, "NULL argument");
+    int pi[kNoiseSize];
+    noise_tables(seed, pi, grad);
+    for (int i = 0; i < kNoiseSize; i++) perm[i] = pi[i];
     return GLS_OK;
 }
 }  // extern "C"

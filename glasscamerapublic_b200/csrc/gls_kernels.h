@@ -7,6 +7,8 @@
 
 #include "gls_common.cuh"
 
+struct gls_demosaic_params;
+
 namespace gls {
 
 constexpr int kMaxTaps = 32;
@@ -106,6 +108,30 @@ void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, cons
 // the FP16 block matcher's tile-height autotuner decisions: (w, h, height)
 // triples of the level sizes seen so far; returns their count
 int bm_tile_list(int* whty, int max);
+
+// ---- display post-processing (gls_post.cu)
+// histogram_data's statistics (demosaic.metal:1360-1369)
+struct PostStats {
+    float black, white, shadows, highlights, mean, median;
+};
+template <class S>
+struct PostArgs {
+    const gls_demosaic_params* params;
+    float y2c[9];           // YCbCr -> camera RGB
+    bool denoise;           // den[] valid (else rgb is the demosaic output)
+    Plane<S, 4> den[5];     // denoised levels, YCbCr
+    Plane<S, 4> rgb;        // camera RGB without noise reduction
+    Plane<S, 2> grad2;      // level-0 gradient plane
+    const uint16_t* raw;    // the raw frame on the device: its first pixel seeds the grain
+    uint32_t* hist;         // 256 bins
+    PostStats* stats;
+    int* perm;              // kNoiseSize
+    float* grad_tab;        // kNoiseSize x 2
+    float2* ab;             // post_ab_bytes: the three bands' filtered (a, b)
+};
+size_t post_ab_bytes(int w, int h);
+template <class S, class O>
+void launch_post(const PostArgs<S>& pa, Plane<O, 4> out, cudaStream_t s);
 
 // ---- adjoint of the pyramid (gls_adjoint.cu); FP32 planes, tightly packed
 struct AdjointLevelArgs {

@@ -74,8 +74,28 @@ typedef struct gls_raw_nlf {
     float b[4];
 } gls_raw_nlf;
 
-/* DemosaicParameters, demosaic.hpp:102-124, flattened to plain data. The
- * local-tone-mapping and sRGB conversion members are not part of this path. */
+/* RGBConversionParameters, demosaic.hpp:43-50 (GLS_POSTPROCESS) */
+typedef struct gls_rgb_conversion_params {
+    float contrast;                  /* 1.05 */
+    float saturation;                /* 1.0 */
+    float tone_curve_slope;          /* 3.5 */
+    float exposure_bias;             /* EV; log2(exposure_multiplier) is added per call */
+    float blacks;                    /* 0 */
+    int32_t local_tone_mapping;      /* the three-band LTM mask */
+} gls_rgb_conversion_params;
+
+/* LTMParameters, demosaic.hpp:95-100 (GLS_POSTPROCESS with local tone
+ * mapping). The mask takes its shadows / highlights exponents from the
+ * image histogram (demosaic.metal:1510), so those two fields are carried
+ * but not read, as in the reference. */
+typedef struct gls_ltm_params {
+    float eps;                       /* guided-filter regulariser, 0.01 */
+    float shadows;
+    float highlights;
+    float detail[3];                 /* low, medium, high frequency band */
+} gls_ltm_params;
+
+/* DemosaicParameters, demosaic.hpp:102-124, flattened to plain data. */
 typedef struct gls_demosaic_params {
     int32_t bayer_pattern;           /* GLS_GRBG .. GLS_BGGR */
     float black_level;               /* DN */
@@ -92,6 +112,8 @@ typedef struct gls_demosaic_params {
     gls_denoise_params denoise[GLS_MAX_LEVELS];
     int32_t levels;                  /* pyramid levels, 1..5 (the reference fixes 5) */
     int32_t iso;
+    gls_rgb_conversion_params rgb_conversion;  /* GLS_POSTPROCESS only */
+    gls_ltm_params ltm;                        /* GLS_POSTPROCESS with local tone mapping */
 } gls_demosaic_params;
 
 /* element types of an image view */
@@ -110,7 +132,7 @@ typedef struct gls_image_view {
 /* flags for gls_demosaic / gls_demosaic_batch / gls_pyramid_denoise */
 enum {
     GLS_DENOISE = 1u << 0,       /* run the pyramid denoise (RawConverter::demosaic noiseReduction) */
-    GLS_POSTPROCESS = 1u << 1,   /* sRGB post-processing: not on this path, rejected */
+    GLS_POSTPROCESS = 1u << 1,   /* display post-processing (histogram, local tone mapping, convertTosRGB) */
     GLS_FP16_STORAGE = 1u << 2,  /* FP16 planes + fused kernels + device PCA (the batched path) */
     GLS_HOST_IO = 1u << 3,       /* raw input and caller output buffers are host memory */
     GLS_SYNC = 1u << 4,          /* block until the stream has finished (the reference is synchronous) */
@@ -234,6 +256,12 @@ typedef struct gls_kernel_stat {
 gls_status gls_converter_set_profiling(gls_converter* conv, int32_t enable);
 gls_status gls_converter_stats(gls_converter* conv, gls_kernel_stat* stats, int32_t max_stats, int32_t* n_stats);
 gls_status gls_converter_reset_stats(gls_converter* conv);
+
+/* The grain tables of the display post-processing (Noise2D::randomSeed +
+ * initGradients, SimplexNoise.hpp:109-143): perm[514] and grad[514][2] for
+ * a seed (the raw frame's first pixel). The same code builds them on the
+ * device during gls_demosaic with GLS_POSTPROCESS. */
+gls_status gls_grain_tables(uint32_t seed, int32_t* perm, float* grad);
 
 /* Decisions of the FP16 block matcher's tile autotuner (no reference
  * counterpart): for each pyramid level size met so far in this process,

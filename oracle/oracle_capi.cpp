@@ -8,6 +8,7 @@
 
 #include "../include/glscam.h"
 #include "gls_oracle.hpp"
+#include "gls_oracle_post.hpp"
 
 using namespace orc;
 
@@ -292,4 +293,52 @@ int orc_jacobi(int n, const double* a, double* evals, double* evecs) {
     return 0;
 }
 
+
+// The display post-processing (gls_oracle_post.hpp) of one frame from its
+// denoised levels (5 levels packed, 4 ch, sizes w >> l x h >> l; NULL
+// without noise reduction), level-0 gradient (2 ch) and linear camera RGB
+// (4 ch); seed = the raw frame's first pixel. stats (optional, 6 floats):
+// black, white, shadows, highlights, mean, median.
+int orc_postprocess(const float* den_levels, const float* grad, const float* rgb, int w, int h,
+                    const gls_demosaic_params* gp, unsigned seed, int f64, float* out, float* stats) {
+    if (!grad || !rgb || !gp || !out || w < 16 || h < 16) return 1;
+    post::PostParams pp;
+    const gls_rgb_conversion_params& rc = gp->rgb_conversion;
+    pp.contrast = rc.contrast;
+    pp.saturation = rc.saturation;
+    pp.slope = rc.tone_curve_slope;
+    pp.bias = rc.exposure_bias + std::log2(gp->exposure_multiplier);
+    pp.blacks = rc.blacks;
+    pp.ltm = rc.local_tone_mapping != 0;
+    pp.eps = gp->ltm.eps;
+    for (int k = 0; k < 3; k++) pp.detail[k] = gp->ltm.detail[k];
+    pp.nlf[0] = gp->pyramid_nlf[0].a[0];
+    pp.nlf[1] = gp->pyramid_nlf[0].b[0];
+    pp.luma_var[0] = 2.0f * ((gp->raw_nlf.a[1] + gp->raw_nlf.a[3]) / 2);
+    pp.luma_var[1] = 2.0f * ((gp->raw_nlf.b[1] + gp->raw_nlf.b[3]) / 2);
+    for (int i = 0; i < 9; i++) pp.rgb_cam[i] = gp->rgb_cam[i];
+    auto run = [&](auto tag) {
+        using T = decltype(tag);
+        std::vector<Plane4<T>> den;
+        if (den_levels) {
+            size_t off = 0;
+            for (int l = 0; l < 5; l++) {
+                den.push_back(copy_in<T, 4>(den_levels + off, w >> l, h >> l));
+                off += size_t(w >> l) * (h >> l) * 4;
+            }
+        }
+        const auto g = copy_in<T, 2>(grad, w, h);
+        const auto c = copy_in<T, 4>(rgb, w, h);
+        post::Stats st;
+        const auto o = post::postprocess<T>(den, g, c, pp, seed, &st);
+        copy_out(o, out);
+        if (stats) {
+            const float v[6] = {st.black, st.white, st.shadows, st.highlights, st.mean, st.median};
+            std::copy(v, v + 6, stats);
+        }
+    };
+    if (f64) run(double());
+    else run(float());
+    return 0;
+}
 }  // extern "C"

@@ -39,6 +39,8 @@ def lib() -> C.CDLL:
         L.orc_jacobi.argtypes = [C.c_int, dp, dp, dp]
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_pyramid_loss.argtypes = [fp, fp, C.c_int, C.c_int, C.POINTER(DemosaicParams), dp, dp, fp, C.c_int, dp]
+        L.orc_postprocess.argtypes = [fp, fp, fp, C.c_int, C.c_int, C.POINTER(DemosaicParams), C.c_uint, C.c_int,
+                                      fp, fp]
         _lib = L
     return _lib
 
@@ -182,3 +184,22 @@ def pyramid_loss(ycc, grad, p: DemosaicParams, bases, y2c, target) -> float:
     assert lib().orc_pyramid_loss(_fp(ycc), _fp(grad), w, h, C.byref(p), _dp(b), _dp(m), _fp(t), t.shape[2],
                                   C.byref(out)) == 0
     return out.value
+
+
+def postprocess(den_levels, grad, rgb, p: DemosaicParams, seed: int, f64: bool = False):
+    """The display post-processing of one frame (oracle/gls_oracle_post.hpp).
+    den_levels: list of 5 (h >> l, w >> l, 4) YCbCr levels, or None without
+    noise reduction; grad (h, w, 2); rgb (h, w, 4) linear camera RGB.
+    Returns (out (h, w, 4), stats [black, white, shadows, highlights, mean,
+    median])."""
+    rgb = np.ascontiguousarray(rgb, np.float32)
+    grad = np.ascontiguousarray(grad, np.float32)
+    h, w = rgb.shape[:2]
+    den = None
+    if den_levels is not None:
+        den = np.concatenate([np.ascontiguousarray(d, np.float32).ravel() for d in den_levels])
+    out = np.zeros((h, w, 4), np.float32)
+    st = np.zeros(6, np.float32)
+    assert lib().orc_postprocess(_fp(den), _fp(grad), _fp(rgb), w, h, C.byref(p), seed, int(f64), _fp(out),
+                                 _fp(st)) == 0
+    return out, st
