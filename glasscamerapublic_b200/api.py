@@ -13,7 +13,7 @@ import ctypes as C
 
 import numpy as np
 
-from . import (DENOISE, F16, F32, FP16_STORAGE, GRAPH, HOST_IO, HOST_PCA, SYNC, CAMERA_IPHONE14_WIDE,
+from . import (DENOISE, F16, F32, FP16_STORAGE, GRAPH, HOST_IO, HOST_PCA, POSTPROCESS, SYNC, CAMERA_IPHONE14_WIDE,
                DemosaicParams, ImageView, FrameDesc, check, lib)
 
 
@@ -102,14 +102,17 @@ class RawConverter:
         return self._h
 
     def demosaic(self, raw, params: DemosaicParams, noiseReduction: bool = True, fp16: bool = False,
-                 out=None, out_fp16: bool = False, stream=None, host_pca: bool = False, sync: bool = True):
-        """RawConverter::demosaic(raw, params, noiseReduction, postProcess=false).
+                 out=None, out_fp16: bool = False, stream=None, host_pca: bool = False, sync: bool = True,
+                 postProcess: bool = False):
+        """RawConverter::demosaic(raw, params, noiseReduction, postProcess).
 
         ``raw``: numpy uint16 (H, W) host array, or a torch CUDA int16/uint16
-        tensor. Returns linear camera RGBA (H, W, 4): a numpy array for host
-        input, or ``out`` (a torch CUDA tensor) for device input.
+        tensor. Returns RGBA (H, W, 4): linear camera RGB, or display sRGB in
+        [0, 1] with ``postProcess`` (raw_converter.cpp:226-242); a numpy array
+        for host input, or ``out`` (a torch CUDA tensor) for device input.
         """
         flags = (DENOISE if noiseReduction else 0) | (FP16_STORAGE if fp16 else 0) | (HOST_PCA if host_pca else 0)
+        flags |= POSTPROCESS if postProcess else 0
         flags |= SYNC if sync else 0
         dt = F16 if out_fp16 else F32
         h, w = raw.shape[0], raw.shape[1]
@@ -128,7 +131,7 @@ class RawConverter:
 
     def demosaic_batch(self, raws, params_list, outs, fp16: bool = True, noiseReduction: bool = True,
                        out_fp16: bool = True, stream=None, sync: bool = False, host_pca: bool = False,
-                       graph: bool = False):
+                       graph: bool = False, postProcess: bool = False):
         """Batched RawConverter::demosaic over frames of uneven sizes.
 
         ``raws``/``outs``: torch CUDA tensors (device I/O), or host buffers
@@ -148,6 +151,7 @@ class RawConverter:
             frames[i].out = ImageView(C.c_void_p(_ptr(o)), w, h, 4, F16 if out_fp16 else F32, _row_stride(o))
         flags = (DENOISE if noiseReduction else 0) | (FP16_STORAGE if fp16 else 0) | (SYNC if sync else 0)
         flags |= (HOST_IO if host else 0) | (HOST_PCA if host_pca else 0) | (GRAPH if graph else 0)
+        flags |= POSTPROCESS if postProcess else 0
         check(lib().gls_demosaic_batch(self._h, frames, n, flags, _stream_handle(stream)))
         return outs
 
