@@ -8,6 +8,7 @@
 //   * lines 754-1291 (collectPatches, pcaProjection, blockMatchingDenoise,
 //                     pyramid down/up-sampling and reconstruct, the
 //                     high-noise quad kernels, despeckle and median);
+//   * lines 1292-1723 (the display post-processing kernels);
 // and this file supplies, between them, the `_half8` helper type and its
 // `length` overloads of lines 721-752: eight halves bit-reinterpreted from
 // and to uint4, element-wise subtraction, and a length over the first n
@@ -15,8 +16,10 @@
 // reference's own declaration: class-type members in an anonymous struct,
 // which Metal allows because its vectors are builtin types.)
 //
-// The host sequence around the kernels restates raw_converter.cpp:148-248
-// and pyramid_processor.cpp:96-172. Two host pieces are the oracle's: the
+// The host sequence around the kernels restates raw_converter.cpp:148-248,
+// pyramid_processor.cpp:96-172 and, for post-processing,
+// raw_converter.cpp:70-115 with demosaic_kernels.hpp:485-671; the grain
+// tables come from the reference's own Noise2D (ref_noise.cpp). Two host pieces are the oracle's: the
 // Gaussian tap folding (demosaic_utils.cpp:934-1006) and the PCA basis
 // (Eigen in the reference; the oracle's FP64 Jacobi here, on the dense
 // patch grid the reference's collectPatches kernel wrote), rounded to half
@@ -49,6 +52,16 @@ half length(_half8 x, int components) {
 }
 
 #include "demosaic_b.inc"
+
+// Lines 1292-1723 (the guided filter and box filter of local tone mapping,
+// histogramImage / histogramStatistics, localToneMappingMaskImage, the
+// Perlin grain and convertTosRGB) size arrays with `constant` scalars
+// (histogramSize, noiseGradSize), so `constant` reads as `const` there.
+#undef constant
+#define constant const
+#include "demosaic_c.inc"
+#undef constant
+#define constant
 
 // ------------------------------------------------------------------ harness
 #undef kernel
@@ -368,6 +381,141 @@ int ref_raw_pipeline(const uint16_t* raw, int w, int h, const gls_demosaic_param
     ref_pyramid_denoise(desp.data(), grad.data(), w, h, p, den.data(), nullptr, nullptr);
     ref_transform(den.data(), w, h, &y2c.m[0][0], out);
     return 0;
+}
+
+int ref_noise_tables(unsigned seed, int* perm, float* grad);
+
+// RawConverter::demosaic's post-processing (raw_converter.cpp:87-112 and
+// 231-241): the histogram of denoised level 3 and its statistics, the
+// guided-filter (a, b) of levels 4, 2 and 0 with their box filter, the
+// tone-mapping mask at full size, and convertTosRGB with the grain seeded by
+// `seed`. den_levels: the 5 denoised levels (YCbCr RGBA float, packed level
+// after level), or NULL for a frame without noise reduction (the fixed
+// statistics of raw_converter.cpp:225-229; the reference computes no mask
+// then, so local tone mapping must be off: returns 2 otherwise).
+// grad: the level-0 gradient (2 floats per pixel); rgb: the linear camera
+// RGB (RGBA float). out: RGBA float; stats: black, white, shadows,
+// highlights, mean, median.
+int ref_postprocess(const float* den_levels, const float* grad, const float* rgb, int w, int h,
+                    const gls_demosaic_params* p, unsigned seed, float* out, float* stats) {
+    const gls_rgb_conversion_params& rc = p->rgb_conversion;
+    if (!den_levels && rc.local_tone_mapping) return 2;
+    histogram_data hd{};
+    Tex mask(w, h, 1);
+    std::vector<Tex*> den;
+    if (den_levels) {
+        size_t off = 0;
+        for (int l = 0; l < 5; l++) {
+            const int wl = w >> l, hl = h >> l;
+            Tex* t = new Tex(wl, hl, 4);
+            std::copy(den_levels + off, den_levels + off + size_t(wl) * hl * 4, t->f.begin());
+            off += size_t(wl) * hl * 4;
+            den.push_back(t);
+        }
+        // raw_converter.cpp:87-90
+        auto t3 = den[3]->t<float>();
+        run_grid(w >> 3, h >> 3, [&](metal::uint2 i) { histogramImage(t3, hd, i); });
+        const metal::uint2 dims(uint(w >> 3), uint(h >> 3));
+        histogramStatistics(hd, dims, metal::uint2(0u, 0u));
+    } else {
+        hd.black_level = 0.1f;
+        hd.white_level = 1.0f;
+        hd.mean = 0.22f;
+        hd.median = 0.22f;
+    }
+    if (den_levels && rc.local_tone_mapping) {
+        // LocalToneMapping::createMask (raw_converter.hpp:61-75), guides =
+        // denoised levels 4, 2, 0 (raw_converter.cpp:105-112)
+        LTMParameters lp;
+        lp.eps = p->ltm.eps;
+        lp.shadows = p->ltm.shadows;
+        lp.highlights = p->ltm.highlights;
+        for (int k = 0; k < 3; k++) lp.detail[k] = p->ltm.detail[k];
+        std::vector<Tex*> abm;
+        for (int k : {4, 2, 0}) {
+            const int wk = w >> k, hk = h >> k;
+            Tex ab(wk, hk, 2);
+            Tex* mean = new Tex(wk, hk, 2);
+            auto tg = den[k]->t<float>();
+            auto tab_w = ab.t<float, access::write>();
+            const float eps = lp.eps;
+            run_grid(wk, hk, [&](metal::uint2 i) { GuidedFilterABImage(tg, tab_w, eps, i); });
+            auto tab = ab.t<float>();
+            auto tm_w = mean->t<float, access::write>();
+            run_grid(wk, hk, [&](metal::uint2 i) { BoxFilterGFImage(tab, tm_w, i); });
+            abm.push_back(mean);
+        }
+        Tex g(w, h, 2);
+        std::copy(grad, grad + size_t(w) * h * 2, g.f.begin());
+        const metal::float2 nlf = f2(p->pyramid_nlf[0].a[0], p->pyramid_nlf[0].b[0]);
+        auto t0 = den[0]->t<float>();
+        auto tg = g.t<float>();
+        auto lf = abm[0]->t<float>(), mf = abm[1]->t<float>(), hf = abm[2]->t<float>();
+        auto tmask_w = mask.t<float, access::write>();
+        run_grid(w, h, [&](metal::uint2 i) {
+            localToneMappingMaskImage(t0, tg, lf, mf, hf, tmask_w, lp, nlf, hd, i);
+        });
+        for (Tex* t : abm) delete t;
+    }
+    // convertTosRGB (demosaic_kernels.hpp:629-671, raw_converter.cpp:231-241)
+    RGBConversionParameters cp;
+    cp.contrast = rc.contrast;
+    cp.saturation = rc.saturation;
+    cp.toneCurveSlope = rc.tone_curve_slope;
+    cp.exposureBias = rc.exposure_bias;
+    cp.exposureBias += std::log2(p->exposure_multiplier);
+    cp.blacks = rc.blacks;
+    cp.localToneMapping = rc.local_tone_mapping != 0;
+    Matrix3x3 tr;
+    for (int r = 0; r < 3; r++) tr.m[r] = metal::float3(p->rgb_cam[3 * r], p->rgb_cam[3 * r + 1], p->rgb_cam[3 * r + 2]);
+    const metal::float2 luma_var = f2(2.0f * ((p->raw_nlf.a[1] + p->raw_nlf.a[3]) / 2),
+                                      2.0f * ((p->raw_nlf.b[1] + p->raw_nlf.b[3]) / 2));
+    metal::array<int, 514> perm;
+    metal::array<metal::float2, 514> g2;
+    {
+        float gt[514 * 2];
+        ref_noise_tables(seed, perm.data(), gt);
+        for (int i = 0; i < 514; i++) g2[i] = f2(gt[2 * i], gt[2 * i + 1]);
+    }
+    Tex lin(w, h, 4), o(w, h, 4);
+    std::copy(rgb, rgb + size_t(w) * h * 4, lin.f.begin());
+    auto tl = lin.t<float>();
+    auto tmask = mask.t<float>();
+    auto to_w = o.t<float, access::write>();
+    run_grid(w, h, [&](metal::uint2 i) { convertTosRGB(tl, tmask, to_w, tr, cp, hd, luma_var, perm, g2, i); });
+    std::copy(o.f.begin(), o.f.end(), out);
+    if (stats) {
+        const float v[6] = {hd.black_level, hd.white_level, hd.shadows, hd.highlights, hd.mean, hd.median};
+        std::copy(v, v + 6, stats);
+    }
+    for (Tex* t : den) delete t;
+    return 0;
+}
+
+// RawConverter::demosaic(postProcess = true) end to end through the
+// reference kernels: ref_raw_pipeline's stages, keeping the five denoised
+// levels, then ref_postprocess seeded with the first raw pixel
+// (raw_converter.cpp:238). Noise reduction needs levels == 5.
+int ref_demosaic_post(const uint16_t* raw, int w, int h, const gls_demosaic_params* p, int denoise, float* out,
+                      float* stats) {
+    const size_t n = size_t(w) * h;
+    std::vector<float> scaled(n), grad(n * 2), rgb(n * 4), ycc(n * 4), desp(n * 4), den(n * 4), cam(n * 4);
+    std::vector<float> levels;
+    ref_scale(raw, w, h, p, scaled.data());
+    ref_sobel_blur(scaled.data(), w, h, p, grad.data());
+    if (denoise && p->high_noise_image) ref_raw_denoise(scaled.data(), grad.data(), w, h, p, scaled.data());
+    ref_demosaic_rgb(scaled.data(), grad.data(), w, h, p, rgb.data());
+    if (!denoise) return ref_postprocess(nullptr, grad.data(), rgb.data(), w, h, p, raw[0], out, stats);
+    if (p->levels != 5) return 3;
+    size_t tot = 0;
+    for (int l = 0; l < 5; l++) tot += size_t(w >> l) * (h >> l) * 4;
+    levels.resize(tot);
+    const orc::Mat3 c2y = orc::cam_ycbcr(p->rgb_cam, p->xyz_rgb), y2c = orc::inverse3(c2y);
+    ref_transform(rgb.data(), w, h, &c2y.m[0][0], ycc.data());
+    ref_despeckle(ycc.data(), w, h, p, desp.data());
+    ref_pyramid_denoise(desp.data(), grad.data(), w, h, p, den.data(), levels.data(), nullptr);
+    ref_transform(den.data(), w, h, &y2c.m[0][0], cam.data());
+    return ref_postprocess(levels.data(), grad.data(), cam.data(), w, h, p, raw[0], out, stats);
 }
 
 void ref_set_threads(int n) { orc::num_threads() = n > 0 ? n : 1; }

@@ -36,6 +36,9 @@ def lib() -> C.CDLL:
         L.ref_pyramid_denoise.argtypes = [fp, fp, C.c_int, C.c_int, P, fp, fp, dp]
         L.ref_raw_pipeline.argtypes = [C.c_void_p, C.c_int, C.c_int, P, C.c_int, fp]
         L.ref_set_threads.argtypes = [C.c_int]
+        L.ref_noise_tables.argtypes = [C.c_uint, C.POINTER(C.c_int32), fp]
+        L.ref_postprocess.argtypes = [fp, fp, fp, C.c_int, C.c_int, P, C.c_uint, fp, fp]
+        L.ref_demosaic_post.argtypes = [C.c_void_p, C.c_int, C.c_int, P, C.c_int, fp, fp]
         _lib = L
     return _lib
 
@@ -113,3 +116,39 @@ def raw_pipeline(raw, p, denoise=True):
     out = np.zeros((h, w, 4), np.float32)
     assert lib().ref_raw_pipeline(raw.ctypes.data, w, h, C.byref(p), int(denoise), _fp(out)) == 0
     return out
+
+
+def noise_tables(seed):
+    """Noise2D::randomSeed + initGradients (SimplexNoise.hpp) of the reference."""
+    perm = np.zeros(514, np.int32)
+    grad = np.zeros((514, 2), np.float32)
+    lib().ref_noise_tables(seed, perm.ctypes.data_as(C.POINTER(C.c_int32)), _fp(grad))
+    return perm, grad
+
+
+def postprocess(den_levels, grad, rgb, p, seed):
+    """The reference's post-processing kernels (demosaic.metal:1292-1723) in
+    the host order of raw_converter.cpp; arguments as _oracle.postprocess."""
+    rgb, grad = _f32(rgb), _f32(grad)
+    h, w = rgb.shape[:2]
+    den = None
+    if den_levels is not None:
+        den = np.concatenate([_f32(d).ravel() for d in den_levels])
+    out = np.zeros((h, w, 4), np.float32)
+    st = np.zeros(6, np.float32)
+    rc = lib().ref_postprocess(None if den is None else _fp(den), _fp(grad), _fp(rgb), w, h, C.byref(p), seed,
+                               _fp(out), _fp(st))
+    assert rc == 0, rc
+    return out, st
+
+
+def demosaic_post(raw, p, denoise=True):
+    """RawConverter::demosaic(raw, p, noiseReduction, postProcess=true) end
+    to end through the reference kernels. Returns (sRGB RGBA, stats)."""
+    raw = np.ascontiguousarray(raw, np.uint16)
+    h, w = raw.shape
+    out = np.zeros((h, w, 4), np.float32)
+    st = np.zeros(6, np.float32)
+    rc = lib().ref_demosaic_post(raw.ctypes.data, w, h, C.byref(p), int(denoise), _fp(out), _fp(st))
+    assert rc == 0, rc
+    return out, st

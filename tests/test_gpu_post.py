@@ -16,6 +16,7 @@ import numpy as np
 import pytest
 
 import _oracle as O
+import _ref as R
 import glasscamerapublic_b200 as g
 from glasscamerapublic_b200 import scene
 
@@ -108,3 +109,27 @@ def test_post_needs_the_five_level_pyramid(converter):
     with pytest.raises(g.GlsError) as e:
         converter.demosaic(raw, p, postProcess=True)
     assert e.value.code == g.GLS_ERR_INVALID_ARG
+
+
+@pytest.mark.skipif(not R.available(), reason="reference kernels not built (make -C oracle ref)")
+def test_post_vs_reference_kernels(converter):
+    # the same planes through the reference's own post-processing kernels
+    raw, p = _frame(256, 256, iso=1600, seed=17)
+    out = converter.demosaic(raw, p, postProcess=True)
+    den, grad = _planes(converter)
+    rgb = converter.demosaic(raw, p).astype(np.float32)
+    ref, _ = R.postprocess(den, grad, rgb, p, int(raw[0, 0]))
+    q, m = _p999(out, ref)
+    assert q <= 1e-4 and m <= 2e-3, (q, m)
+    # and end to end: raw -> display sRGB through the reference kernels
+    ref_e2e, _ = R.demosaic_post(raw, p)
+    orc = O.postprocess(*_oracle_planes(raw, p), p, int(raw[0, 0]))[0]
+    ps_cuda = scene.psnr(out[..., :3], ref_e2e[..., :3])
+    ps_orc = scene.psnr(orc[..., :3], ref_e2e[..., :3])
+    assert ps_cuda >= 55.0 and ps_cuda >= ps_orc - 3.0, (ps_cuda, ps_orc)
+
+
+def _oracle_planes(raw, p):
+    st = O.raw_pipeline(raw, p, denoise=True, f64=False, stages=True)
+    den = O.pyramid_denoise(st["despeckled"], st["gradient"], p, f64=False, levels_out=True)["levels"]
+    return den, st["gradient"], st["out"]
