@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--adjoint-only", action="store_true", help="run only the adjoint leg (for profiler captures)")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-sensor batch leg")
     ap.add_argument("--mixed-only", action="store_true", help="run only the mixed-sensor batch leg")
+    ap.add_argument("--no-post", action="store_true", help="skip the display post-processing leg")
+    ap.add_argument("--post-only", action="store_true", help="run only the post-processing leg")
+    ap.add_argument("--post-frames", type=int, default=N_ROTATE, help="frames per batch of the post-processing leg")
     return ap.parse_args()
 
 
@@ -459,6 +462,82 @@ def mixed_leg(args, rank, local, conv, stream):
     }
 
 
+def post_leg(args, rank, local, conv, stream):
+    """RawConverter::demosaic with postProcess on the headline workload: the
+    six-frame (--post-frames) FP16 batch with GLS_POSTPROCESS (histogram statistics,
+    guided-filter tone mapping, grain, sRGB tone curve) against the same
+    batch without it, and the post-processing kernels' own device time per
+    frame from the per-launch event profile. Roofline: the HBM bytes the
+    post-processing must move per frame (denoised level 0 and the gradient in,
+    RGBA FP16 out; FP16 planes) over its device time."""
+    import torch
+
+    import glasscamerapublic_b200 as g
+    from glasscamerapublic_b200 import scene
+
+    wl = scene.WORKLOADS[args.workload]
+    params = scene.make_params(wl)
+    H, W = wl.height, wl.width
+    B = max(1, args.post_frames)
+    dev = f"cuda:{local}"
+    raws = [torch.from_numpy(scene.make_raw(wl, frame=100 + rank * B + f)[0].view(np.int16)).to(dev)
+            for f in range(B)]
+    outs = [torch.empty((H, W, 4), dtype=torch.float16, device=dev) for _ in range(B)]
+    plist = [params] * B
+    lib = g.lib()
+
+    def stats():
+        st = (g.KernelStat * 32)()
+        n = C.c_int32()
+        g.check(lib.gls_converter_stats(conv.handle, st, 32, C.byref(n)))
+        return {st[i].name.decode(): {"launches": int(st[i].launches), "ms": st[i].ms} for i in range(n.value)}
+
+    def batch_ms(post: bool) -> float:
+        for _ in range(2):
+            conv.demosaic_batch(raws, plist, outs, fp16=True, out_fp16=True, stream=stream, postProcess=post)
+        stream.synchronize()
+        reps = max(3, args.steps // 2)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            conv.demosaic_batch(raws, plist, outs, fp16=True, out_fp16=True, stream=stream, postProcess=post)
+        e1.record(stream)
+        stream.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    with torch.cuda.stream(stream):
+        ms_plain = batch_ms(False)
+        ms_post = batch_ms(True)
+        g.check(lib.gls_converter_reset_stats(conv.handle))
+        g.check(lib.gls_converter_set_profiling(conv.handle, 1))
+        for i in range(B):
+            conv.demosaic(raws[i], params, noiseReduction=True, fp16=True, out=outs[i], out_fp16=True,
+                          stream=stream, sync=False, postProcess=True)
+        stream.synchronize()
+        pk = stats()["post_process"]
+        g.check(lib.gls_converter_set_profiling(conv.handle, 0))
+    post_ms = pk["ms"] / B
+    px = W * H
+    small = sum((W >> l) * (H >> l) for l in (2, 3, 4)) * 8  # levels 2, 3, 4 (FP16 RGBA)
+    bytes_frame = px * (8 + 4 + 8) + small
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    gbs = bytes_frame / (post_ms / 1e3) / 1e9
+    return {
+        "workload": f"{B} x {W}x{H} RGGB 12-bit, demosaic + 5-level denoise + post-processing, FP16 storage",
+        "value": B / (ms_post / 1e3), "unit": "frames/s",
+        "ms_per_batch_post": ms_post, "ms_per_batch_plain": ms_plain,
+        "added_ms_per_frame": (ms_post - ms_plain) / B,
+        "post_kernels_ms_per_frame": post_ms,
+        "post_launches_per_frame": pk["launches"] / B,
+        "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                     "bytes_per_frame": bytes_frame,
+                     "note": "all post-processing kernels of a frame together; bytes: denoised level 0 (8 B/px) "
+                             "and gradient (4 B/px) read, RGBA FP16 (8 B/px) written, levels 2-4; peak "
+                             + ("of measured" if peaks else "of fallback")},
+    }
+
+
 def run_reference(args, rank):
     """The reference arm: the reference's path on the host cores. The Metal
     runtime cannot run here; the reference's own kernel source, compiled
@@ -511,8 +590,9 @@ def main():
     conv = g.RawConverter(local)
     lib = g.lib()
     stream = torch.cuda.Stream()
-    if args.burst_only or args.adjoint_only or args.mixed_only:
-        leg = burst_leg if args.burst_only else adjoint_leg if args.adjoint_only else mixed_leg
+    if args.burst_only or args.adjoint_only or args.mixed_only or args.post_only:
+        leg = (burst_leg if args.burst_only else adjoint_leg if args.adjoint_only else
+               mixed_leg if args.mixed_only else post_leg)
         b = leg(args, rank, local, conv, stream)
         if rank == 0:
             print(json.dumps({leg.__name__: True, **b}), flush=True)
@@ -677,6 +757,11 @@ def main():
         (mx["ms_per_batch_graph"],) = max_over_ranks([mx["ms_per_batch_graph"]], dist if world > 1 else None)
         mx["value"] = world * mx["megapixels_per_batch"] / (mx["ms_per_batch_graph"] / 1e3)
         line["mixed_batch"] = mx
+    if not args.no_post:
+        pp = post_leg(args, rank, local, conv, stream)
+        (pp["ms_per_batch_post"],) = max_over_ranks([pp["ms_per_batch_post"]], dist if world > 1 else None)
+        pp["value"] = world * max(1, args.post_frames) / (pp["ms_per_batch_post"] / 1e3)
+        line["post_process"] = pp
     if not args.no_adjoint:
         a = adjoint_leg(args, rank, local, conv, stream)
         (a["ms_per_batch"],) = max_over_ranks([a["ms_per_batch"]], dist if world > 1 else None)

@@ -98,11 +98,11 @@ namespace gls {
 // kernel classes for launch accounting
 enum KernelClass {
     KC_SCALE, KC_SOBEL_BLUR, KC_RAW_DENOISE, KC_DEMOSAIC, KC_DESPECKLE, KC_DOWNSAMPLE, KC_SUBTRACT,
-    KC_PCA_COV, KC_PCA_EIGEN, KC_PCA_PROJECT, KC_BLOCK_MATCH, KC_OUTPUT, KC_VIEW_IN, KC_COUNT
+    KC_PCA_COV, KC_PCA_EIGEN, KC_PCA_PROJECT, KC_BLOCK_MATCH, KC_OUTPUT, KC_VIEW_IN, KC_POST, KC_COUNT
 };
 static const char* const kKcNames[KC_COUNT] = {
     "scale_raw", "sobel_blur", "raw_quad_denoise", "demosaic", "despeckle", "downsample", "subtract_noise",
-    "pca_cov", "pca_eigen", "pca_project", "block_match", "output_transform", "view_in"};
+    "pca_cov", "pca_eigen", "pca_project", "block_match", "output_transform", "view_in", "post_process"};
 
 struct Prof {
     bool on = false;
@@ -362,15 +362,18 @@ template <class S, class O>
 static gls_status finish_output(gls_converter* cv, Plane<S, 4> src, bool transform, const float* m, OutTarget<O>& t,
                                 cudaStream_t s, const SlotCopies* cp = nullptr, const PostArgs<S>* post = nullptr) {
     if (cp && t.copy_to_host) GLS_CUDA(cudaStreamWaitEvent(s, cp->out_free, 0));
-    KScope k(cv->prof, KC_OUTPUT, s);
     if (post) {  // the display post-processing writes the output
-        launch_post<S, O>(*post, t.plane, s);
-    } else if (transform) {
-        Mat3Args ma;
-        std::memcpy(ma.m, m, sizeof(ma.m));
-        launch_transform<S, O>(src, t.plane, ma, s);
+        KScope k(cv->prof, KC_POST, s, 0);
+        cv->prof.launches[KC_POST] += launch_post<S, O>(*post, t.plane, s);
     } else {
-        launch_convert4<S, O>(src, t.plane, s);
+        KScope k(cv->prof, KC_OUTPUT, s);
+        if (transform) {
+            Mat3Args ma;
+            std::memcpy(ma.m, m, sizeof(ma.m));
+            launch_transform<S, O>(src, t.plane, ma, s);
+        } else {
+            launch_convert4<S, O>(src, t.plane, s);
+        }
     }
     GLS_CUDA(cudaGetLastError());
     if (t.copy_to_host) {
@@ -563,7 +566,7 @@ static gls_status demosaic_run(gls_converter* cv, const uint16_t* raw, int w, in
         pa.rgb = A;
         pa.grad2 = grad;
         pa.raw = rawp;
-        GLS_TRY(P.post_hist.ensure(256 * sizeof(uint32_t)));
+        GLS_TRY(P.post_hist.ensure_zeroed(256 * sizeof(uint32_t), s));
         GLS_TRY(P.post_stats.ensure(sizeof(PostStats)));
         GLS_TRY(P.post_perm.ensure(kNoiseSize * sizeof(int)));
         GLS_TRY(P.post_gtab.ensure(kNoiseSize * 2 * sizeof(float)));

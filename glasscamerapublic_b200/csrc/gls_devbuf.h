@@ -38,6 +38,16 @@ struct DevBuf {
         bytes = b;
         return GLS_OK;
     }
+    // ensure(), and a newly allocated buffer is zeroed on stream s (a
+    // buffer that its users leave zeroed after each use)
+    gls_status ensure_zeroed(size_t b, cudaStream_t s) {
+        if (b <= bytes) return GLS_OK;
+        const gls_status st = ensure(b);
+        if (st != GLS_OK) return st;
+        const cudaError_t e = cudaMemsetAsync(p, 0, b, s);
+        if (e != cudaSuccess) return set_error(GLS_ERR_CUDA, "cudaMemsetAsync: %s", cudaGetErrorString(e));
+        return GLS_OK;
+    }
     void release() {
         if (p) cudaFree(p);
         p = nullptr;

@@ -123,15 +123,16 @@ struct PostArgs {
     Plane<S, 4> rgb;        // camera RGB without noise reduction
     Plane<S, 2> grad2;      // level-0 gradient plane
     const uint16_t* raw;    // the raw frame on the device: its first pixel seeds the grain
-    uint32_t* hist;         // 256 bins
+    uint32_t* hist;         // 256 bins, zero on entry (zeroed when allocated; left zeroed)
     PostStats* stats;
     int* perm;              // kNoiseSize
     float* grad_tab;        // kNoiseSize x 2
     float2* ab;             // post_ab_bytes: the three bands' filtered (a, b)
 };
 size_t post_ab_bytes(int w, int h);
+// returns the number of kernels launched
 template <class S, class O>
-void launch_post(const PostArgs<S>& pa, Plane<O, 4> out, cudaStream_t s);
+int launch_post(const PostArgs<S>& pa, Plane<O, 4> out, cudaStream_t s);
 
 // ---- adjoint of the pyramid (gls_adjoint.cu); FP32 planes, tightly packed
 struct AdjointLevelArgs {

@@ -7,10 +7,12 @@ The oracle is fed the CUDA path's own intermediate planes of the same call
 a run without post-processing), with the grain seeded from the raw frame's
 first pixel, so the comparison isolates the post-processing kernels.
 
-Tolerances (outputs in [0, 1]): FP32 storage, 99.9th percentile of |diff|
-<= 1e-4 and max <= 2e-3; FP16 storage (the oracle fed the FP16 planes),
-99.9th percentile <= 2e-3. The histogram statistics agree to 1e-6, except
-that a pixel whose luma sits within an ulp of a bin edge may move one count.
+Tolerances (outputs in [0, 1]; FP32 and FP16 storage alike, the oracle fed
+the planes the path stored): 99.9th percentile of |diff| <= 5e-6, max
+<= 2e-4. Measured on B200: 99.9th percentiles of 2-5e-7 and maxima of
+1e-6 to 2e-5 (1024 x 768). The kernels' pow is exp2(y log2 x) and their
+sigmoid a logistic of exp2, a few ulps from the oracle's C library calls,
+which the tone-mapping powers amplify near dark pixels.
 """
 import numpy as np
 import pytest
@@ -53,7 +55,7 @@ def test_post_fp32_matches_oracle(converter, ltm):
     p.rgb_conversion.local_tone_mapping = ltm
     out, ref, _ = _post_vs_oracle(converter, raw, p)
     q, m = _p999(out, ref)
-    assert q <= 1e-4 and m <= 2e-3, (q, m)
+    assert q <= 5e-6 and m <= 2e-4, (q, m)
     assert np.all(out[..., 3] == 1)
     assert out[..., :3].min() >= 0 and out[..., :3].max() <= 1
 
@@ -62,7 +64,7 @@ def test_post_without_noise_reduction(converter):
     raw, p = _frame(seed=9)
     out, ref, stats = _post_vs_oracle(converter, raw, p, denoise=False)
     q, m = _p999(out, ref)
-    assert q <= 1e-4 and m <= 2e-3, (q, m)
+    assert q <= 5e-6 and m <= 2e-4, (q, m)
     assert stats[0] == pytest.approx(0.1) and stats[4] == pytest.approx(0.22)
 
 
@@ -71,7 +73,7 @@ def test_post_fp16_storage_matches_oracle(converter, w, h, iso):
     raw, p = _frame(w, h, iso=iso, seed=11)
     out, ref, _ = _post_vs_oracle(converter, raw, p, fp16=True)
     q, m = _p999(out, ref)
-    assert q <= 2e-3, (q, m)
+    assert q <= 5e-6 and m <= 2e-4, (q, m)
 
 
 def test_grain_follows_the_first_raw_pixel(converter):
@@ -84,7 +86,7 @@ def test_grain_follows_the_first_raw_pixel(converter):
     rgb = converter.demosaic(raw2, p).astype(np.float32)
     ref, _ = O.postprocess(den, grad, rgb, p, int(raw2[0, 0]))
     q, m = _p999(b, ref)
-    assert q <= 1e-4 and m <= 2e-3, (q, m)
+    assert q <= 5e-6 and m <= 2e-4, (q, m)
     assert np.abs(a - b)[8:, 8:].max() > 1e-4  # the grain moved
 
 
@@ -120,7 +122,7 @@ def test_post_vs_reference_kernels(converter):
     rgb = converter.demosaic(raw, p).astype(np.float32)
     ref, _ = R.postprocess(den, grad, rgb, p, int(raw[0, 0]))
     q, m = _p999(out, ref)
-    assert q <= 1e-4 and m <= 2e-3, (q, m)
+    assert q <= 5e-6 and m <= 2e-4, (q, m)
     # and end to end: raw -> display sRGB through the reference kernels
     ref_e2e, _ = R.demosaic_post(raw, p)
     orc = O.postprocess(*_oracle_planes(raw, p), p, int(raw[0, 0]))[0]
