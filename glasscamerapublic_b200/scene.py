@@ -93,6 +93,32 @@ def clean_scene(w: int, h: int, seed: int, n_rect: int = 20) -> np.ndarray:
     return np.clip(img, 0.0, 1.0).astype(np.float32)
 
 
+def step_chart(w: int, h: int, seed: int, cells: tuple = (12, 8)) -> np.ndarray:
+    """A neutral step chart, (h, w, 3) float32: a grid of flat grey patches
+    with levels spread over [0.01, 0.85] of white (log-spaced, shuffled),
+    the kind of capture a noise model is measured on."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nx, ny = cells
+    levels = np.geomspace(0.01, 0.85, nx * ny)
+    rng.shuffle(levels)
+    img = np.zeros((h, w, 3), dtype=np.float32)
+    for j in range(ny):
+        for i in range(nx):
+            x0, x1 = i * w // nx, (i + 1) * w // nx
+            y0, y1 = j * h // ny, (j + 1) * h // ny
+            img[y0:y1, x0:x1, :] = levels[j * nx + i]
+    return img
+
+
+def make_chart_raw(wl: "Workload", frame: int = 0):
+    """(raw uint16 (h, w), clean RGB) of a step chart at the workload's
+    sensor noise."""
+    seed = wl.seed + frame
+    clean = step_chart(wl.width, wl.height, seed)
+    raw = add_noise(mosaic(clean, wl.pattern), wl.black, wl.white, wl.gain, wl.read, seed)
+    return raw, clean
+
+
 def mosaic(rgb: np.ndarray, pattern: int = RGGB) -> np.ndarray:
     """Sample a linear RGB image to a Bayer mosaic (float, same units)."""
     h, w = rgb.shape[:2]

@@ -8,6 +8,7 @@
 
 #include "../include/glscam.h"
 #include "gls_oracle.hpp"
+#include "gls_oracle_nlf.hpp"
 #include "gls_oracle_post.hpp"
 
 using namespace orc;
@@ -341,4 +342,70 @@ int orc_postprocess(const float* den_levels, const float* grad, const float* rgb
     else run(float());
     return 0;
 }
+// ---- noise-model measurement (calibrateFromImage), FP32 statistics ----
+
+// basicRawNoiseStatistics: mean, var are (w/2) x (h/2) x 4
+int orc_raw_noise_stats(const float* scaled, int w, int h, int pattern, float* mean, float* var) {
+    if (!scaled || !mean || !var || w < 2 || h < 2 || pattern < 0 || pattern > 3) return 1;
+    const auto s = copy_in<float, 1>(scaled, w, h);
+    Plane4<float> m, v;
+    nlf::raw_stats(s, pattern, m, v);
+    copy_out(m, mean);
+    copy_out(v, var);
+    return 0;
+}
+
+// basicNoiseStatistics: stats is w x h x 4 (mean Y, var Y, var Cb, var Cr)
+int orc_ycc_noise_stats(const float* img, int w, int h, float* stats) {
+    if (!img || !stats || w < 1 || h < 1) return 1;
+    copy_out(nlf::ycc_stats(copy_in<float, 4>(img, w, h)), stats);
+    return 0;
+}
+
+int orc_measure_raw_nlf(const float* mean, const float* var, int raw_w, int raw_h, float exposure_multiplier,
+                        float* a, float* b) {
+    if (!mean || !var || !a || !b || raw_w < 2 || raw_h < 2) return 1;
+    const RawNLF r = nlf::measure_raw(copy_in<float, 4>(mean, raw_w / 2, raw_h / 2),
+                                      copy_in<float, 4>(var, raw_w / 2, raw_h / 2), raw_w, raw_h, exposure_multiplier);
+    std::copy(r.a, r.a + 4, a);
+    std::copy(r.b, r.b + 4, b);
+    return 0;
+}
+
+int orc_measure_ycc_nlf(const float* stats, int w, int h, float exposure_multiplier, float* a, float* b) {
+    if (!stats || !a || !b || w < 1 || h < 1) return 1;
+    const YCbCrNLF r = nlf::measure_ycc(copy_in<float, 4>(stats, w, h), exposure_multiplier);
+    std::copy(r.a, r.a + 3, a);
+    std::copy(r.b, r.b + 3, b);
+    return 0;
+}
+
+// RawConverter::demosaic with calibrateFromImage and noise reduction: out
+// RGBA (w = 0); raw_nlf (8 floats: a[4], b[4]) and pyr_nlf (levels x 6:
+// a[3], b[3]) receive the measured models.
+int orc_raw_pipeline_calibrated(const uint16_t* raw, int w, int h, size_t stride_elems, const gls_demosaic_params* gp,
+                                int f64, float* out_rgba, float* raw_nlf, float* pyr_nlf) {
+    if (!raw || !gp || !out_rgba || w < 2 || h < 2 || gp->levels < 1 || gp->levels > 5) return 1;
+    const Params p = to_params(gp);
+    RawNLF mr{};
+    YCbCrNLF mp[5]{};
+    auto run = [&](auto tag) {
+        using T = decltype(tag);
+        copy_out(nlf::raw_pipeline_calibrated<T>(raw, stride_elems, w, h, p, gp->exposure_multiplier, &mr, mp),
+                 out_rgba);
+    };
+    if (f64) run(double());
+    else run(float());
+    if (raw_nlf) {
+        std::copy(mr.a, mr.a + 4, raw_nlf);
+        std::copy(mr.b, mr.b + 4, raw_nlf + 4);
+    }
+    if (pyr_nlf)
+        for (int l = 0; l < p.levels; l++) {
+            std::copy(mp[l].a, mp[l].a + 3, pyr_nlf + 6 * l);
+            std::copy(mp[l].b, mp[l].b + 3, pyr_nlf + 6 * l + 3);
+        }
+    return 0;
+}
+
 }  // extern "C"

@@ -385,6 +385,35 @@ int ref_raw_pipeline(const uint16_t* raw, int w, int h, const gls_demosaic_param
 
 int ref_noise_tables(unsigned seed, int* perm, float* grad);
 
+// basicRawNoiseStatistics (demosaic.metal:1110-1136) over a scaled raw frame
+// (RawConverter::MeasureRawNLF, raw_converter.cpp:340): 9x9 mean and
+// variance of the four channels at every half-resolution position.
+int ref_raw_noise_stats(const float* scaled, int w, int h, int pattern, float* mean, float* var) {
+    Tex s(w, h, 1), m(w / 2, h / 2, 4), v(w / 2, h / 2, 4);
+    std::copy(scaled, scaled + size_t(w) * h, s.f.begin());
+    auto ts = s.t<float>();
+    auto tm = m.t<float, access::write>();
+    auto tv = v.t<float, access::write>();
+    int bp = pattern;
+    run_grid(w / 2, h / 2, [&](metal::uint2 i) { basicRawNoiseStatistics(ts, bp, tm, tv, i); });
+    std::copy(m.f.begin(), m.f.end(), mean);
+    std::copy(v.f.begin(), v.f.end(), var);
+    return 0;
+}
+
+// basicNoiseStatistics (demosaic.metal:1138-1159) over one YCbCr pyramid
+// level (PyramidProcessor::MeasureYCbCrNLF, pyramid_processor.cpp:180):
+// 5x5 mean of Y and variances of Y, Cb, Cr.
+int ref_ycc_noise_stats(const float* img, int w, int h, float* stats) {
+    Tex in(w, h, 4), st(w, h, 4);
+    std::copy(img, img + size_t(w) * h * 4, in.f.begin());
+    auto ti = in.t<float>();
+    auto ts = st.t<float, access::write>();
+    run_grid(w, h, [&](metal::uint2 i) { basicNoiseStatistics(ti, ts, i); });
+    std::copy(st.f.begin(), st.f.end(), stats);
+    return 0;
+}
+
 // RawConverter::demosaic's post-processing (raw_converter.cpp:87-112 and
 // 231-241): the histogram of denoised level 3 and its statistics, the
 // guided-filter (a, b) of levels 4, 2 and 0 with their box filter, the

@@ -203,3 +203,71 @@ def postprocess(den_levels, grad, rgb, p: DemosaicParams, seed: int, f64: bool =
     assert lib().orc_postprocess(_fp(den), _fp(grad), _fp(rgb), w, h, C.byref(p), seed, int(f64), _fp(out),
                                  _fp(st)) == 0
     return out, st
+
+
+def _nlf_setup(L):
+    fp = C.POINTER(C.c_float)
+    L.orc_raw_noise_stats.argtypes = [fp, C.c_int, C.c_int, C.c_int, fp, fp]
+    L.orc_ycc_noise_stats.argtypes = [fp, C.c_int, C.c_int, fp]
+    L.orc_measure_raw_nlf.argtypes = [fp, fp, C.c_int, C.c_int, C.c_float, fp, fp]
+    L.orc_measure_ycc_nlf.argtypes = [fp, C.c_int, C.c_int, C.c_float, fp, fp]
+    L.orc_raw_pipeline_calibrated.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_size_t, C.POINTER(DemosaicParams),
+                                              C.c_int, fp, fp, fp]
+    L._nlf_ready = True
+
+
+def _nlf_lib():
+    L = lib()
+    if not hasattr(L, "_nlf_ready"):
+        _nlf_setup(L)
+    return L
+
+
+def raw_noise_stats(scaled, pattern):
+    """basicRawNoiseStatistics (FP32): (mean, var), each (h/2, w/2, 4)."""
+    s = np.ascontiguousarray(scaled, np.float32)
+    h, w = s.shape
+    mean = np.zeros((h // 2, w // 2, 4), np.float32)
+    var = np.zeros((h // 2, w // 2, 4), np.float32)
+    assert _nlf_lib().orc_raw_noise_stats(_fp(s), w, h, int(pattern), _fp(mean), _fp(var)) == 0
+    return mean, var
+
+
+def ycc_noise_stats(img):
+    """basicNoiseStatistics (FP32): (h, w, 4) = mean Y, var Y, var Cb, var Cr."""
+    a = np.ascontiguousarray(img, np.float32)
+    h, w = a.shape[:2]
+    st = np.zeros((h, w, 4), np.float32)
+    assert _nlf_lib().orc_ycc_noise_stats(_fp(a), w, h, _fp(st)) == 0
+    return st
+
+
+def measure_raw_nlf(mean, var, raw_w, raw_h, exposure=1.0):
+    a = np.zeros(4, np.float32)
+    b = np.zeros(4, np.float32)
+    assert _nlf_lib().orc_measure_raw_nlf(_fp(np.ascontiguousarray(mean, np.float32)),
+                                          _fp(np.ascontiguousarray(var, np.float32)), raw_w, raw_h, exposure,
+                                          _fp(a), _fp(b)) == 0
+    return a, b
+
+
+def measure_ycc_nlf(stats, exposure=1.0):
+    st = np.ascontiguousarray(stats, np.float32)
+    h, w = st.shape[:2]
+    a = np.zeros(3, np.float32)
+    b = np.zeros(3, np.float32)
+    assert _nlf_lib().orc_measure_ycc_nlf(_fp(st), w, h, exposure, _fp(a), _fp(b)) == 0
+    return a, b
+
+
+def raw_pipeline_calibrated(raw, p, f64=False):
+    """RawConverter::demosaic with calibrateFromImage: (out RGBA, raw NLF
+    (a[4], b[4]), pyramid NLF (levels, 2, 3))."""
+    raw = np.ascontiguousarray(raw, dtype=np.uint16)
+    h, w = raw.shape
+    out = np.zeros((h, w, 4), np.float32)
+    rn = np.zeros(8, np.float32)
+    pn = np.zeros((p.levels, 6), np.float32)
+    assert _nlf_lib().orc_raw_pipeline_calibrated(raw.ctypes.data, w, h, w, C.byref(p), int(f64), _fp(out), _fp(rn),
+                                                  _fp(pn)) == 0
+    return out, (rn[:4], rn[4:]), pn.reshape(p.levels, 2, 3)

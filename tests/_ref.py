@@ -39,6 +39,10 @@ def lib() -> C.CDLL:
         L.ref_noise_tables.argtypes = [C.c_uint, C.POINTER(C.c_int32), fp]
         L.ref_postprocess.argtypes = [fp, fp, fp, C.c_int, C.c_int, P, C.c_uint, fp, fp]
         L.ref_demosaic_post.argtypes = [C.c_void_p, C.c_int, C.c_int, P, C.c_int, fp, fp]
+        L.ref_raw_noise_stats.argtypes = [fp, C.c_int, C.c_int, C.c_int, fp, fp]
+        L.ref_ycc_noise_stats.argtypes = [fp, C.c_int, C.c_int, fp]
+        L.ref_measure_raw_nlf.argtypes = [fp, fp, C.c_int, C.c_int, C.c_float, fp, fp]
+        L.ref_measure_ycc_nlf.argtypes = [fp, C.c_int, C.c_int, C.c_float, fp, fp]
         _lib = L
     return _lib
 
@@ -152,3 +156,40 @@ def demosaic_post(raw, p, denoise=True):
     rc = lib().ref_demosaic_post(raw.ctypes.data, w, h, C.byref(p), int(denoise), _fp(out), _fp(st))
     assert rc == 0, rc
     return out, st
+
+
+def raw_noise_stats(scaled, pattern):
+    """basicRawNoiseStatistics: (mean, var), each (h/2, w/2, 4)."""
+    s = _f32(scaled)
+    h, w = s.shape
+    mean = np.zeros((h // 2, w // 2, 4), np.float32)
+    var = np.zeros((h // 2, w // 2, 4), np.float32)
+    lib().ref_raw_noise_stats(_fp(s), w, h, int(pattern), _fp(mean), _fp(var))
+    return mean, var
+
+
+def ycc_noise_stats(img):
+    """basicNoiseStatistics: (h, w, 4) = mean Y, var Y, var Cb, var Cr."""
+    a = _f32(img)
+    h, w = a.shape[:2]
+    st = np.zeros((h, w, 4), np.float32)
+    lib().ref_ycc_noise_stats(_fp(a), w, h, _fp(st))
+    return st
+
+
+def measure_raw_nlf(mean, var, raw_w, raw_h, exposure=1.0):
+    """RawConverter::MeasureRawNLF over given statistics: (a[4], b[4])."""
+    a = np.zeros(4, np.float32)
+    b = np.zeros(4, np.float32)
+    lib().ref_measure_raw_nlf(_fp(_f32(mean)), _fp(_f32(var)), raw_w, raw_h, exposure, _fp(a), _fp(b))
+    return a, b
+
+
+def measure_ycc_nlf(stats, exposure=1.0):
+    """PyramidProcessor::MeasureYCbCrNLF over given statistics: (a[3], b[3])."""
+    st = _f32(stats)
+    h, w = st.shape[:2]
+    a = np.zeros(3, np.float32)
+    b = np.zeros(3, np.float32)
+    lib().ref_measure_ycc_nlf(_fp(st), w, h, exposure, _fp(a), _fp(b))
+    return a, b
