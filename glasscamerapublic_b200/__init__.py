@@ -44,7 +44,10 @@ PLANE_DEMOSAIC = 2
 PLANE_DESPECKLED = 3
 PLANE_OUTPUT = 4
 PLANE_ADJ_DESPECKLED = 5
+PLANE_NLF_MEAN = 6
+PLANE_NLF_VAR = 7
 PLANE_DENOISED_L0 = 8
+PLANE_NLF_STATS = 13
 SURF_PLANE_INTEGRAL = 0
 ADJ_NPARAMS = 32
 ADJ_LUMA, ADJ_CHROMA, ADJ_NLF_AY, ADJ_NLF_BY, ADJ_NLF_AC, ADJ_NLF_BC = 0, 5, 10, 15, 20, 25
@@ -167,6 +170,12 @@ _SIGNATURES = {
     "gls_converter_reset_stats": (C.c_int, [C.c_void_p]),
     "gls_block_match_tiles": (C.c_int, [C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)]),
     "gls_grain_tables": (C.c_int, [C.c_uint32, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
+    "gls_measure_raw_nlf": (C.c_int, [C.c_void_p, C.POINTER(ImageView), C.c_int32, C.c_float, C.POINTER(RawNLF),
+                                      C.c_void_p]),
+    "gls_measure_ycbcr_nlf": (C.c_int, [C.c_void_p, C.POINTER(ImageView), C.c_float, C.POINTER(YCbCrNLF),
+                                        C.c_void_p]),
+    "gls_converter_noise_model": (C.c_int, [C.c_void_p, C.POINTER(RawNLF), C.POINTER(YCbCrNLF), C.c_int32,
+                                            C.POINTER(C.c_int32)]),
     "gls_calibration_fill": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(DemosaicParams)]),
     "gls_gaussian_bilinear_taps": (C.c_int, [C.c_float, C.POINTER(C.c_float), C.c_int32, C.POINTER(C.c_int32)]),
     "gls_demosaic_denoise_vjp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_size_t,

@@ -14,7 +14,7 @@ import ctypes as C
 import numpy as np
 
 from . import (DENOISE, F16, F32, FP16_STORAGE, GRAPH, HOST_IO, HOST_PCA, POSTPROCESS, SYNC, CAMERA_IPHONE14_WIDE,
-               DemosaicParams, ImageView, FrameDesc, check, lib)
+               DemosaicParams, ImageView, FrameDesc, RawNLF, YCbCrNLF, check, lib)
 
 
 def _stream_handle(stream) -> C.c_void_p:
@@ -80,11 +80,12 @@ def _is_torch(a) -> bool:
 class RawConverter:
     """RawConverter (raw_converter.hpp:80-188) on a CUDA device."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, calibrateFromImage: bool = False):
         h = C.c_void_p()
-        check(lib().gls_converter_create(int(device), None, 0, 0, C.byref(h)))
+        check(lib().gls_converter_create(int(device), None, 0, 1 if calibrateFromImage else 0, C.byref(h)))
         self._h = h
         self.device = device
+        self.calibrateFromImage = calibrateFromImage
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
@@ -164,6 +165,36 @@ class RawConverter:
         dst = ImageView(C.c_void_p(arr.ctypes.data), v.width, v.height, v.channels, v.dtype, arr.strides[0])
         check(lib().gls_copy_view(C.byref(v), C.byref(dst), 0, None))
         return arr
+
+    def MeasureRawNLF(self, scaled, bayerPattern: int, exposure_multiplier: float = 1.0, stream=None):
+        """RawConverter::MeasureRawNLF (raw_converter.cpp:339-490) on a scaled
+        raw frame (a torch CUDA (h, w) float32/float16 tensor): (a[4], b[4])."""
+        v = ImageView(C.c_void_p(_ptr(scaled)), scaled.shape[1], scaled.shape[0], 1,
+                      F16 if str(scaled.dtype) == "torch.float16" else F32, _row_stride(scaled))
+        r = RawNLF()
+        check(lib().gls_measure_raw_nlf(self._h, C.byref(v), int(bayerPattern), float(exposure_multiplier),
+                                        C.byref(r), _stream_handle(stream)))
+        return np.array(r.a[:], np.float32), np.array(r.b[:], np.float32)
+
+    def MeasureYCbCrNLF(self, ycc, exposure_multiplier: float = 1.0, stream=None):
+        """PyramidProcessor::MeasureYCbCrNLF (pyramid_processor.cpp:173-324)
+        on a YCbCr image (a torch CUDA (h, w, 4) tensor): (a[3], b[3])."""
+        v = ImageView(C.c_void_p(_ptr(ycc)), ycc.shape[1], ycc.shape[0], 4,
+                      F16 if str(ycc.dtype) == "torch.float16" else F32, _row_stride(ycc))
+        r = YCbCrNLF()
+        check(lib().gls_measure_ycbcr_nlf(self._h, C.byref(v), float(exposure_multiplier), C.byref(r),
+                                          _stream_handle(stream)))
+        return np.array(r.a[:], np.float32), np.array(r.b[:], np.float32)
+
+    def noise_model(self):
+        """The models the last calibrating call measured: ((a[4], b[4]),
+        [(a[3], b[3]) per pyramid level])."""
+        r = RawNLF()
+        pyr = (YCbCrNLF * 5)()
+        n = C.c_int32()
+        check(lib().gls_converter_noise_model(self._h, C.byref(r), pyr, 5, C.byref(n)))
+        return ((np.array(r.a[:], np.float32), np.array(r.b[:], np.float32)),
+                [(np.array(pyr[i].a[:], np.float32), np.array(pyr[i].b[:], np.float32)) for i in range(n.value)])
 
     def pca_basis(self, level: int) -> np.ndarray:
         b = (C.c_float * 200)()

@@ -98,11 +98,11 @@ namespace gls {
 // kernel classes for launch accounting
 enum KernelClass {
     KC_SCALE, KC_SOBEL_BLUR, KC_RAW_DENOISE, KC_DEMOSAIC, KC_DESPECKLE, KC_DOWNSAMPLE, KC_SUBTRACT,
-    KC_PCA_COV, KC_PCA_EIGEN, KC_PCA_PROJECT, KC_BLOCK_MATCH, KC_OUTPUT, KC_VIEW_IN, KC_POST, KC_COUNT
+    KC_PCA_COV, KC_PCA_EIGEN, KC_PCA_PROJECT, KC_BLOCK_MATCH, KC_OUTPUT, KC_VIEW_IN, KC_POST, KC_NLF, KC_COUNT
 };
 static const char* const kKcNames[KC_COUNT] = {
     "scale_raw", "sobel_blur", "raw_quad_denoise", "demosaic", "despeckle", "downsample", "subtract_noise",
-    "pca_cov", "pca_eigen", "pca_project", "block_match", "output_transform", "view_in", "post_process"};
+    "pca_cov", "pca_eigen", "pca_project", "block_match", "output_transform", "view_in", "post_process", "noise_model"};
 
 struct Prof {
     bool on = false;
@@ -196,6 +196,14 @@ struct gls_converter {
     DevBuf adj_gimg, adj_gp1, adj_jvp, adj_jvp_part;  // dL/d(input pyramid), front-end tangents
     DevBuf adj_gout;                                   // a caller's cotangent, packed (pyramid VJP)
     int adj_gimg_w = 0, adj_gimg_h = 0;                // size of the last dL/d(despeckled image)
+    // noise-model measurement (calibrateFromImage): scratch, the last
+    // statistics planes and the last measured models
+    bool calibrate = false;
+    DevBuf nlf_scratch, nlf_mean, nlf_var, nlf_stats;
+    int nlf_mw = 0, nlf_mh = 0, nlf_sw = 0, nlf_sh = 0;
+    gls_raw_nlf nlf_raw{};
+    gls_ycbcr_nlf nlf_pyr[GLS_MAX_LEVELS]{};
+    int nlf_levels = 0;
 };
 
 namespace gls {
@@ -264,6 +272,59 @@ static gls_status check_post(const gls_demosaic_params* p, uint32_t flags) {
     return GLS_OK;
 }
 
+// RawConverter::MeasureRawNLF / PyramidProcessor::MeasureYCbCrNLF on the
+// device (gls_nlf.cu), the result read back to the host (synchronous, as the
+// reference's host regressions are)
+static gls_status nlf_result(gls_converter* cv, gls_raw_nlf* host, cudaStream_t s) {
+    GLS_CUDA(cudaGetLastError());
+    const auto* dres = reinterpret_cast<const gls_raw_nlf*>(static_cast<char*>(cv->nlf_scratch.p) + nlf_scratch_bytes());
+    GLS_CUDA(cudaMemcpyAsync(host, dres, sizeof(gls_raw_nlf), cudaMemcpyDeviceToHost, s));
+    GLS_CUDA(cudaStreamSynchronize(s));
+    return GLS_OK;
+}
+
+template <class S>
+static gls_status measure_raw_nlf(gls_converter* cv, Plane<S, 1> scaled, int pattern, float exposure,
+                                  gls_raw_nlf* out, cudaStream_t s) {
+    const int mw = scaled.w / 2, mh = scaled.h / 2;
+    if (mw < 1 || mh < 1) return set_error(GLS_ERR_INVALID_ARG, "raw noise measurement needs a frame of at least 2 x 2");
+    GLS_TRY(cv->nlf_scratch.ensure(nlf_scratch_bytes() + sizeof(gls_raw_nlf)));
+    GLS_TRY(cv->nlf_mean.ensure(size_t(mw) * mh * 4 * sizeof(float)));
+    GLS_TRY(cv->nlf_var.ensure(size_t(mw) * mh * 4 * sizeof(float)));
+    auto* dres = reinterpret_cast<gls_raw_nlf*>(static_cast<char*>(cv->nlf_scratch.p) + nlf_scratch_bytes());
+    {
+        KScope k(cv->prof, KC_NLF, s, 0);
+        cv->prof.launches[KC_NLF] += launch_measure_raw_nlf<S>(scaled, pattern, plane<float, 4>(cv->nlf_mean, mw, mh),
+                                                               plane<float, 4>(cv->nlf_var, mw, mh), exposure,
+                                                               cv->nlf_scratch.p, dres, s);
+    }
+    cv->nlf_mw = mw;
+    cv->nlf_mh = mh;
+    return nlf_result(cv, out, s);
+}
+
+template <class S>
+static gls_status measure_ycc_nlf(gls_converter* cv, Plane<S, 4> img, float exposure, gls_ycbcr_nlf* out,
+                                  cudaStream_t s) {
+    GLS_TRY(cv->nlf_scratch.ensure(nlf_scratch_bytes() + sizeof(gls_raw_nlf)));
+    GLS_TRY(cv->nlf_stats.ensure(size_t(img.w) * img.h * 4 * sizeof(float)));
+    auto* dres = reinterpret_cast<gls_raw_nlf*>(static_cast<char*>(cv->nlf_scratch.p) + nlf_scratch_bytes());
+    {
+        KScope k(cv->prof, KC_NLF, s, 0);
+        cv->prof.launches[KC_NLF] += launch_measure_ycc_nlf<S>(img, plane<float, 4>(cv->nlf_stats, img.w, img.h),
+                                                               exposure, cv->nlf_scratch.p, dres, s);
+    }
+    cv->nlf_sw = img.w;
+    cv->nlf_sh = img.h;
+    gls_raw_nlf r{};
+    GLS_TRY(nlf_result(cv, &r, s));
+    for (int c = 0; c < 3; c++) {
+        out->a[c] = r.a[c];
+        out->b[c] = r.b[c];
+    }
+    return GLS_OK;
+}
+
 template <class S>
 static gls_status pyramid_run(gls_converter* cv, Pipeline<S>& P, Plane<S, 4> img0, Plane<S, 2> grad0,
                               const gls_demosaic_params* p, uint32_t flags, cudaStream_t s) {
@@ -279,6 +340,16 @@ static gls_status pyramid_run(gls_converter* cv, Pipeline<S>& P, Plane<S, 4> img
         KScope k(cv->prof, KC_DOWNSAMPLE, s, 2);
         launch_downsample<S, 4>(img[i - 1], img[i], s);
         launch_downsample<S, 2>(grd[i - 1], grd[i], s);
+    }
+    gls_demosaic_params measured;
+    if (cv->calibrate) {  // each level's model, measured before the denoise (pyramid_processor.cpp:113-117)
+        measured = *p;
+        for (int i = 0; i < L; i++) {
+            GLS_TRY(measure_ycc_nlf<S>(cv, img[i], p->exposure_multiplier, &measured.pyramid_nlf[i], s));
+            cv->nlf_pyr[i] = measured.pyramid_nlf[i];
+        }
+        cv->nlf_levels = L;
+        p = &measured;
     }
     double* acc = static_cast<double*>(P.acc.p);
     float* basis = static_cast<float*>(P.basis.p);
@@ -496,6 +567,18 @@ static gls_status demosaic_run(gls_converter* cv, const uint16_t* raw, int w, in
     }
     if (cp && host_io) GLS_CUDA(cudaEventRecord(cp->raw_free, s));  // the raw staging buffer is read
 
+    // calibrateFromImage: the raw model measured on the scaled frame, the
+    // high-noise branch off (raw_converter.cpp:160, 188-189)
+    gls_demosaic_params calibrated;
+    if (cv->calibrate) {
+        calibrated = *p;
+        calibrated.high_noise_image = 0;
+        GLS_TRY(measure_raw_nlf<S>(cv, scaled, p->bayer_pattern, p->exposure_multiplier, &calibrated.raw_nlf, s));
+        cv->nlf_raw = calibrated.raw_nlf;
+        cv->nlf_levels = 0;
+        p = &calibrated;
+    }
+
     // rawImageSobel + sampledConvolutionSobel, raw_converter.cpp:185-193
     BlurArgs ba;
     float taps[3 * kMaxTaps];
@@ -553,6 +636,8 @@ static gls_status demosaic_run(gls_converter* cv, const uint16_t* raw, int w, in
         }
         GLS_TRY(pyramid_run<S>(cv, P, B, grad, p, flags, s));
         final_src = plane<S, 4>(P.den[0], w, h);
+        if (cv->calibrate)  // the post-processing reads the measured level-0 model
+            for (int i = 0; i < p->levels; i++) calibrated.pyramid_nlf[i] = cv->nlf_pyr[i];
     }
     // display post-processing (raw_converter.cpp:80-116, 231-244)
     PostArgs<S> pa{};
@@ -924,8 +1009,6 @@ gls_status gls_converter_create(int32_t device, const uint8_t* icc, size_t icc_l
     *out = nullptr;
     if (icc && icc_len)
         return set_error(GLS_ERR_UNSUPPORTED, "ICC profiles are not part of this path; pass xyz_rgb in the parameters");
-    if (calibrate_from_image)
-        return set_error(GLS_ERR_UNSUPPORTED, "calibrateFromImage (noise measurement) is not part of this path");
     int n = 0;
     cudaError_t e = cudaGetDeviceCount(&n);
     if (e != cudaSuccess || device < 0 || device >= n)
@@ -933,6 +1016,7 @@ gls_status gls_converter_create(int32_t device, const uint8_t* icc, size_t icc_l
     gls_converter* c = new (std::nothrow) gls_converter();
     if (!c) return set_error(GLS_ERR_OOM, "host allocation failed");
     c->device = device;
+    c->calibrate = calibrate_from_image != 0;
     *out = c;
     return GLS_OK;
 }
@@ -955,7 +1039,8 @@ gls_status gls_converter_destroy(gls_converter* conv) {
     if (conv->graph_exec) cudaGraphExecDestroy(conv->graph_exec);
     for (DevBuf* b : {&conv->adj_gden[0], &conv->adj_gden[1], &conv->adj_rec, &conv->adj_glayer, &conv->adj_gpca,
                       &conv->adj_gup, &conv->adj_part, &conv->adj_loss, &conv->adj_target, &conv->adj_gimg,
-                      &conv->adj_gp1, &conv->adj_jvp, &conv->adj_jvp_part, &conv->adj_gout})
+                      &conv->adj_gp1, &conv->adj_jvp, &conv->adj_jvp_part, &conv->adj_gout, &conv->nlf_scratch,
+                      &conv->nlf_mean, &conv->nlf_var, &conv->nlf_stats})
         b->release();
     delete conv;
     return GLS_OK;
@@ -1033,6 +1118,8 @@ gls_status gls_demosaic_batch(gls_converter* conv, gls_frame_desc* frames, int32
         if (flags & GLS_HOST_PCA) return set_error(GLS_ERR_INVALID_ARG, "GLS_GRAPH needs the device PCA");
         if (!s) return set_error(GLS_ERR_INVALID_ARG, "GLS_GRAPH needs a stream other than the legacy default stream");
         if (conv->prof.on) return set_error(GLS_ERR_INVALID_ARG, "GLS_GRAPH cannot run with profiling enabled");
+        if (conv->calibrate)
+            return set_error(GLS_ERR_INVALID_ARG, "GLS_GRAPH cannot record a calibrating converter's host reads");
         key = batch_key(frames, n_frames, flags);
         if (!key.empty() && conv->graph_exec && key == conv->graph_key) {  // replay
             GLS_CUDA(cudaGraphLaunch(conv->graph_exec, s));
@@ -1092,6 +1179,17 @@ gls_status gls_pyramid_denoise(gls_converter* conv, const gls_image_view* ycc, c
 gls_status gls_converter_plane(gls_converter* conv, int32_t which, gls_image_view* view) {
     clear_error();
     if (!conv || !view) return set_error(GLS_ERR_INVALID_ARG, "NULL argument");
+    if (which == GLS_PLANE_NLF_MEAN || which == GLS_PLANE_NLF_VAR) {
+        if (!conv->nlf_mw) return set_error(GLS_ERR_INVALID_ARG, "no raw noise measurement has run");
+        *view = {which == GLS_PLANE_NLF_MEAN ? conv->nlf_mean.p : conv->nlf_var.p, conv->nlf_mw, conv->nlf_mh, 4,
+                 GLS_F32, size_t(conv->nlf_mw) * 4 * sizeof(float)};
+        return GLS_OK;
+    }
+    if (which == GLS_PLANE_NLF_STATS) {
+        if (!conv->nlf_sw) return set_error(GLS_ERR_INVALID_ARG, "no YCbCr noise measurement has run");
+        *view = {conv->nlf_stats.p, conv->nlf_sw, conv->nlf_sh, 4, GLS_F32, size_t(conv->nlf_sw) * 4 * sizeof(float)};
+        return GLS_OK;
+    }
     if (conv->last_storage < 0) return set_error(GLS_ERR_INVALID_ARG, "no frame has been processed");
     const bool h = conv->last_storage == GLS_F16;
     const int w = conv->last_w, hh = conv->last_h;
@@ -1334,3 +1432,60 @@ gls_status gls_grain_tables(uint32_t seed, int32_t* perm, float* grad) {
     return GLS_OK;
 }
 }  // extern "C"
+
+// ---- noise-model measurement (calibrateFromImage)
+
+gls_status gls_measure_raw_nlf(gls_converter* conv, const gls_image_view* scaled_raw, int32_t bayer_pattern,
+                               float exposure_multiplier, gls_raw_nlf* out, void* stream) {
+    clear_error();
+    if (!conv || !scaled_raw || !scaled_raw->data || !out) return set_error(GLS_ERR_INVALID_ARG, "NULL argument");
+    if (bayer_pattern < 0 || bayer_pattern > 3) return set_error(GLS_ERR_INVALID_ARG, "bad Bayer pattern");
+    if (scaled_raw->channels != 1) return set_error(GLS_ERR_INVALID_ARG, "the scaled raw view must have 1 channel");
+    if (scaled_raw->width < 2 || scaled_raw->height < 2) return set_error(GLS_ERR_INVALID_ARG, "frame too small");
+    const size_t es = scaled_raw->dtype == GLS_F32 ? 4 : scaled_raw->dtype == GLS_F16 ? 2 : 0;
+    if (!es) return set_error(GLS_ERR_INVALID_ARG, "scaled raw dtype must be F32 or F16");
+    if (scaled_raw->stride_bytes % es) return set_error(GLS_ERR_INVALID_ARG, "stride is not a whole number of elements");
+    GLS_CUDA(cudaSetDevice(conv->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (es == 4) {
+        Plane<float, 1> pl{static_cast<float*>(scaled_raw->data), scaled_raw->width, scaled_raw->height,
+                           scaled_raw->stride_bytes / 4};
+        return measure_raw_nlf<float>(conv, pl, bayer_pattern, exposure_multiplier, out, s);
+    }
+    Plane<__half, 1> pl{static_cast<__half*>(scaled_raw->data), scaled_raw->width, scaled_raw->height,
+                        scaled_raw->stride_bytes / 2};
+    return measure_raw_nlf<__half>(conv, pl, bayer_pattern, exposure_multiplier, out, s);
+}
+
+gls_status gls_measure_ycbcr_nlf(gls_converter* conv, const gls_image_view* ycc, float exposure_multiplier,
+                                 gls_ycbcr_nlf* out, void* stream) {
+    clear_error();
+    if (!conv || !ycc || !ycc->data || !out) return set_error(GLS_ERR_INVALID_ARG, "NULL argument");
+    if (ycc->channels != 4) return set_error(GLS_ERR_INVALID_ARG, "the YCbCr view must have 4 channels");
+    if (ycc->width < 1 || ycc->height < 1) return set_error(GLS_ERR_INVALID_ARG, "empty image");
+    const size_t es = ycc->dtype == GLS_F32 ? 4 : ycc->dtype == GLS_F16 ? 2 : 0;
+    if (!es) return set_error(GLS_ERR_INVALID_ARG, "YCbCr dtype must be F32 or F16");
+    if (ycc->stride_bytes % (4 * es)) return set_error(GLS_ERR_INVALID_ARG, "stride is not a whole number of pixels");
+    if (uintptr_t(ycc->data) % (4 * es)) return set_error(GLS_ERR_INVALID_ARG, "YCbCr data must be pixel-aligned");
+    GLS_CUDA(cudaSetDevice(conv->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (es == 4) {
+        Plane<float, 4> pl{static_cast<float*>(ycc->data), ycc->width, ycc->height, ycc->stride_bytes / 4};
+        return measure_ycc_nlf<float>(conv, pl, exposure_multiplier, out, s);
+    }
+    Plane<__half, 4> pl{static_cast<__half*>(ycc->data), ycc->width, ycc->height, ycc->stride_bytes / 2};
+    return measure_ycc_nlf<__half>(conv, pl, exposure_multiplier, out, s);
+}
+
+gls_status gls_converter_noise_model(gls_converter* conv, gls_raw_nlf* raw, gls_ycbcr_nlf* pyramid,
+                                     int32_t max_levels, int32_t* n_levels) {
+    clear_error();
+    if (!conv) return set_error(GLS_ERR_INVALID_ARG, "NULL converter");
+    if (!conv->calibrate) return set_error(GLS_ERR_INVALID_ARG, "the converter was not created to calibrate from images");
+    if (!conv->nlf_mw) return set_error(GLS_ERR_INVALID_ARG, "no frame has been measured");
+    if (raw) *raw = conv->nlf_raw;
+    if (pyramid)
+        for (int i = 0; i < conv->nlf_levels && i < max_levels; i++) pyramid[i] = conv->nlf_pyr[i];
+    if (n_levels) *n_levels = conv->nlf_levels;
+    return GLS_OK;
+}

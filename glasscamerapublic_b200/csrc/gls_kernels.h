@@ -8,6 +8,7 @@
 #include "gls_common.cuh"
 
 struct gls_demosaic_params;
+struct gls_raw_nlf;
 
 namespace gls {
 
@@ -133,6 +134,18 @@ size_t post_ab_bytes(int w, int h);
 // returns the number of kernels launched
 template <class S, class O>
 int launch_post(const PostArgs<S>& pa, Plane<O, 4> out, cudaStream_t s);
+
+// noise-model measurement (gls_nlf.cu): statistics into the given float
+// planes (raw: (w/2) x (h/2); YCbCr: the level's size), then the fits, the
+// result written to *out (device memory; YCbCr: a[0..2], b[0..2]). scratch:
+// nlf_scratch_bytes(). Each returns the number of kernels launched.
+size_t nlf_scratch_bytes();
+template <class S>
+int launch_measure_raw_nlf(Plane<S, 1> scaled, int pattern, Plane<float, 4> mean, Plane<float, 4> var,
+                           float exposure, void* scratch, gls_raw_nlf* out, cudaStream_t s);
+template <class S>
+int launch_measure_ycc_nlf(Plane<S, 4> img, Plane<float, 4> stats, float exposure, void* scratch,
+                           gls_raw_nlf* out, cudaStream_t s);
 
 // ---- adjoint of the pyramid (gls_adjoint.cu); FP32 planes, tightly packed
 struct AdjointLevelArgs {

@@ -150,7 +150,10 @@ enum {
     GLS_PLANE_DESPECKLED = 3,    /* 4 ch YCbCr input of the pyramid (after despeckle) */
     GLS_PLANE_OUTPUT = 4,        /* 4 ch final camera RGB */
     GLS_PLANE_ADJ_DESPECKLED = 5, /* 3 ch FP32: dL/d(despeckled YCbCr) of the last gls_demosaic_denoise_vjp */
-    GLS_PLANE_DENOISED_L0 = 8    /* + level: 4 ch denoised YCbCr of a pyramid level */
+    GLS_PLANE_NLF_MEAN = 6,      /* 4 ch FP32, half size: 9x9 raw channel means of the last raw noise measurement */
+    GLS_PLANE_NLF_VAR = 7,       /* 4 ch FP32, half size: the matching variances */
+    GLS_PLANE_DENOISED_L0 = 8,   /* + level: 4 ch denoised YCbCr of a pyramid level */
+    GLS_PLANE_NLF_STATS = 13     /* 4 ch FP32: 5x5 mean Y, var Y, Cb, Cr of the last YCbCr noise measurement */
 };
 
 typedef struct gls_converter gls_converter;
@@ -162,8 +165,17 @@ const char* gls_last_error_message(void);
 const char* gls_version(void);
 
 /* RawConverter(device, icc, calibrateFromImage), raw_converter.hpp:128-156.
- * icc may be NULL (xyz_sRGB). calibrate_from_image must be 0: the noise
- * measurement path is not part of this library. */
+ * icc may be NULL (xyz_sRGB). With calibrate_from_image the converter
+ * measures the noise model of every frame it converts, as the reference
+ * does (raw_converter.cpp:160, 188-189; pyramid_processor.cpp:113-117):
+ * the raw model on the scaled frame replaces params->raw_nlf for that frame
+ * (and the high-noise raw branch is off), and each pyramid level's model,
+ * measured on the level before the denoise, replaces params->pyramid_nlf
+ * (despeckling keeps the given level-0 model). The caller's parameters are
+ * not written; gls_converter_noise_model returns the measured models. Each
+ * measurement reads its result back to the host (the reference's regression
+ * runs on the host), so calibrating calls are synchronous and cannot be
+ * recorded with GLS_GRAPH. */
 gls_status gls_converter_create(int32_t device, const uint8_t* icc, size_t icc_len,
                                 int32_t calibrate_from_image, gls_converter** out);
 gls_status gls_converter_destroy(gls_converter* conv);
@@ -213,6 +225,32 @@ gls_status gls_pyramid_denoise(gls_converter* conv, const gls_image_view* ycc,
 
 /* View of an internal plane of the last call (device memory). */
 gls_status gls_converter_plane(gls_converter* conv, int32_t which, gls_image_view* view);
+
+/* RawConverter::MeasureRawNLF, raw_converter.cpp:339-490: the raw noise
+ * model var = a + b * value of the four Bayer channels (R, G, B, G2),
+ * measured on a scaled raw frame (1 ch, GLS_F32 or GLS_F16, device memory,
+ * the output of scaleRawData): basicRawNoiseStatistics' 9x9 statistics
+ * (demosaic.metal:1110-1136), then the reference's two least-squares fits,
+ * with a and b multiplied by exposure_multiplier^2. Synchronous. The
+ * statistics stay readable as GLS_PLANE_NLF_MEAN / GLS_PLANE_NLF_VAR. */
+gls_status gls_measure_raw_nlf(gls_converter* conv, const gls_image_view* scaled_raw, int32_t bayer_pattern,
+                               float exposure_multiplier, gls_raw_nlf* out, void* stream);
+
+/* PyramidProcessor::MeasureYCbCrNLF, pyramid_processor.cpp:173-324: the
+ * noise model var = a + b * Y of Y, Cb and Cr measured on one YCbCr image
+ * (4 ch, GLS_F32 or GLS_F16, device memory): basicNoiseStatistics' 5x5
+ * statistics (demosaic.metal:1138-1159), then the two fits, scaled by
+ * exposure_multiplier^2. Synchronous. The statistics stay readable as
+ * GLS_PLANE_NLF_STATS. */
+gls_status gls_measure_ycbcr_nlf(gls_converter* conv, const gls_image_view* ycc, float exposure_multiplier,
+                                 gls_ycbcr_nlf* out, void* stream);
+
+/* The noise models the last calibrating call measured (a converter created
+ * with calibrate_from_image): the raw model and *n_levels pyramid models
+ * (at most max_levels are written). dumpNoiseModel's data
+ * (demosaic.hpp:70-84). */
+gls_status gls_converter_noise_model(gls_converter* conv, gls_raw_nlf* raw, gls_ycbcr_nlf* pyramid,
+                                     int32_t max_levels, int32_t* n_levels);
 
 /* Strided copy between two views of equal width, height, channels and
  * dtype (no reference counterpart: the reference maps shared-storage

@@ -1,0 +1,138 @@
+"""GPU parity of the noise-model measurement (calibrateFromImage,
+gls_nlf.cu) against the oracle (oracle/gls_oracle_nlf.hpp, itself
+bit-exact to the reference's kernels and regressions), through the C ABI.
+
+  * statistics (basicRawNoiseStatistics, basicNoiseStatistics): bit-exact,
+    FP32 and FP16 inputs alike (the kernels widen to FP32 and round once
+    per operation in the reference's order);
+  * fitted models: the device sums the same FP64 terms in another order,
+    so a and b agree to a relative 1e-6;
+  * a calibrating converter end to end (FP32 path) against the oracle's
+    calibrated pipeline: the raw model to 1e-6 (its input, the scaled frame,
+    is bit-exact), the pyramid models to 2e-3 (their inputs carry the
+    denoise path's last-ulp differences), the output to the raw path's
+    tolerance (99.9th percentile <= 1e-4).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import _oracle as O
+import glasscamerapublic_b200 as g
+from glasscamerapublic_b200 import scene
+
+pytestmark = pytest.mark.gpu
+
+
+def _frame(w=512, h=384, iso=1600, gain=0.5, read=4.0, seed=5, pattern=2, chart=True, levels=5):
+    wl = scene.Workload("nlf", w, h, levels=levels, gain=gain, read=read, iso=iso, seed=seed, pattern=pattern)
+    raw, _ = (scene.make_chart_raw if chart else scene.make_raw)(wl)
+    return raw, scene.make_params(wl)
+
+
+def _plane(conv, which):
+    return conv.plane(which)
+
+
+def _close(a, b, rtol):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.all(np.abs(a - b) <= rtol * np.maximum(np.abs(b), 1e-30)), (a, b)
+
+
+@pytest.mark.parametrize("pattern", [0, 2, 3])
+@pytest.mark.parametrize("w,h", [(512, 384), (262, 198)])
+@pytest.mark.parametrize("half", [False, True])
+def test_raw_statistics_and_fit(converter, pattern, w, h, half):
+    import torch
+    raw, p = _frame(w, h, pattern=pattern)
+    s = O.stage("scale", p=p, w=w, h=h, out_shape=(h, w), raw=raw)
+    if half:
+        s = s.astype(np.float16).astype(np.float32)
+    t = torch.from_numpy(s).cuda()
+    a, b = converter.MeasureRawNLF(t.half() if half else t, pattern, 1.3)
+    mean, var = _plane(converter, g.PLANE_NLF_MEAN), _plane(converter, g.PLANE_NLF_VAR)
+    om, ov = O.raw_noise_stats(s, pattern)
+    assert np.array_equal(mean, om) and np.array_equal(var, ov)
+    oa, ob = O.measure_raw_nlf(om, ov, w, h, 1.3)
+    ok, info = _close(np.r_[a, b], np.r_[oa, ob], 1e-6)
+    assert ok, info
+
+
+@pytest.mark.parametrize("chart", [True, False])
+@pytest.mark.parametrize("half", [False, True])
+def test_ycbcr_statistics_and_fit(converter, chart, half):
+    import torch
+    raw, p = _frame(chart=chart)
+    ds = O.raw_pipeline(raw, p, denoise=True, f64=False, stages=True)["despeckled"]
+    lvl = ds
+    for i in range(4):
+        x = lvl.astype(np.float16).astype(np.float32) if half else lvl
+        t = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+        a, b = converter.MeasureYCbCrNLF(t.half() if half else t, 0.8)
+        st = _plane(converter, g.PLANE_NLF_STATS)
+        ost = O.ycc_noise_stats(x)
+        assert np.array_equal(st, ost), i
+        oa, ob = O.measure_ycc_nlf(ost, 0.8)
+        ok, info = _close(np.r_[a, b], np.r_[oa, ob], 1e-6)
+        assert ok, (i, info)
+        lvl = O.downsample(lvl, lvl.shape[1] // 2, lvl.shape[0] // 2, f64=False)
+
+
+def test_calibrating_converter_matches_the_oracle():
+    conv = g.RawConverter(0, calibrateFromImage=True)
+    try:
+        raw, p = _frame(512, 384, iso=1600, gain=0.5, read=4.0)
+        assert p.high_noise_image  # the calibrating converter turns the branch off
+        out = conv.demosaic(raw, p)
+        (ra, rb), pyr = conv.noise_model()
+        ref, (oa, ob), opyr = O.raw_pipeline_calibrated(raw, p)
+        ok, info = _close(np.r_[ra, rb], np.r_[oa, ob], 1e-6)
+        assert ok, info
+        assert len(pyr) == p.levels
+        for l in range(p.levels):
+            ok, info = _close(np.r_[pyr[l][0], pyr[l][1]], np.r_[opyr[l, 0], opyr[l, 1]], 2e-3)
+            assert ok, (l, info)
+        d = np.abs(out[..., :3].astype(np.float64) - ref[..., :3])
+        assert np.quantile(d, 0.999) <= 1e-4, (np.quantile(d, 0.999), d.max())
+        # the caller's parameters are not written
+        assert p.high_noise_image
+    finally:
+        conv.close()
+
+
+def test_calibrating_converter_fp16_and_post_processing():
+    conv = g.RawConverter(0, calibrateFromImage=True)
+    try:
+        raw, p = _frame(512, 384, iso=800, gain=1.0, read=3.0, chart=False)
+        out = conv.demosaic(raw, p, fp16=True, postProcess=True)
+        (ra, rb), pyr = conv.noise_model()
+        _, (oa, ob), _ = O.raw_pipeline_calibrated(raw, p)
+        ok, info = _close(np.r_[ra, rb], np.r_[oa, ob], 1e-2)  # statistics of the half-precision scaled frame
+        assert ok, info
+        assert np.isfinite(out).all() and out[..., :3].min() >= 0 and out[..., :3].max() <= 1
+    finally:
+        conv.close()
+
+
+def test_calibrating_converter_refuses_graph_recording():
+    import torch
+    conv = g.RawConverter(0, calibrateFromImage=True)
+    try:
+        frames = [_frame(256, 192, seed=s) for s in (1, 2)]
+        raws = [torch.from_numpy(r.view(np.int16)).cuda() for r, _ in frames]
+        outs = [torch.empty((192, 256, 4), dtype=torch.float16, device="cuda") for _ in frames]
+        stream = torch.cuda.Stream()
+        with pytest.raises(g.GlsError) as e:
+            conv.demosaic_batch(raws, [p for _, p in frames], outs, stream=stream, graph=True)
+        assert e.value.code == g.GLS_ERR_INVALID_ARG
+        conv.demosaic_batch(raws, [p for _, p in frames], outs, stream=stream, sync=True)
+        torch.cuda.synchronize()
+        assert torch.isfinite(outs[0].float()).all()
+    finally:
+        conv.close()
+
+
+def test_noise_model_needs_a_calibrating_converter(converter):
+    with pytest.raises(g.GlsError):
+        converter.noise_model()
