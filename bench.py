@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-post", action="store_true", help="skip the display post-processing leg")
     ap.add_argument("--post-only", action="store_true", help="run only the post-processing leg")
     ap.add_argument("--post-frames", type=int, default=N_ROTATE, help="frames per batch of the post-processing leg")
+    ap.add_argument("--no-calibrate", action="store_true", help="skip the noise-model measurement leg")
+    ap.add_argument("--calibrate-only", action="store_true", help="run only the noise-model measurement leg")
     return ap.parse_args()
 
 
@@ -538,6 +540,85 @@ def post_leg(args, rank, local, conv, stream):
     }
 
 
+def calibrate_leg(args, rank, local, conv, stream):
+    """RawConverter with calibrateFromImage on the headline workload: one
+    12 MP frame at a time on the FP16 path, the raw noise model measured on
+    the scaled frame and each of the five pyramid levels' models measured
+    before the denoise (statistics kernels, then the two-pass FP64 fits on
+    the device, each model read back to the host as the reference's host
+    regressions return it), against the same frames through a converter
+    that takes the calibration's models. Roofline: the HBM bytes the
+    measurement moves per frame (statistics written once, read by each of
+    the four fit passes) over its device time."""
+    import torch
+
+    import glasscamerapublic_b200 as g
+    from glasscamerapublic_b200 import scene
+
+    wl = scene.WORKLOADS[args.workload]
+    params = scene.make_params(wl)
+    H, W = wl.height, wl.width
+    dev = f"cuda:{local}"
+    # neutral step charts, the captures a noise model is measured on
+    raws = [torch.from_numpy(scene.make_chart_raw(wl, frame=200 + rank * 2 + f)[0].view(np.int16)).to(dev)
+            for f in range(2)]
+    out = torch.empty((H, W, 4), dtype=torch.float16, device=dev)
+    cal = g.RawConverter(local, calibrateFromImage=True)
+    lib = g.lib()
+
+    def frame_ms(c, n):
+        for i in range(2):
+            c.demosaic(raws[i % 2], params, fp16=True, out=out, out_fp16=True, stream=stream, sync=False)
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        for i in range(n):
+            c.demosaic(raws[i % 2], params, fp16=True, out=out, out_fp16=True, stream=stream, sync=False)
+        e1.record(stream)
+        stream.synchronize()
+        return max(e0.elapsed_time(e1), 1e3 * (time.perf_counter() - t0)) / n
+
+    n = max(3, args.steps // 2)
+    with torch.cuda.stream(stream):
+        ms_plain = frame_ms(conv, n)
+        ms_cal = frame_ms(cal, n)
+        st = (g.KernelStat * 32)()
+        k = C.c_int32()
+        g.check(lib.gls_converter_reset_stats(cal.handle))
+        g.check(lib.gls_converter_set_profiling(cal.handle, 1))
+        for i in range(2):
+            cal.demosaic(raws[i], params, fp16=True, out=out, out_fp16=True, stream=stream, sync=False)
+        stream.synchronize()
+        g.check(lib.gls_converter_stats(cal.handle, st, 32, C.byref(k)))
+        nm = {st[i].name.decode(): (int(st[i].launches), st[i].ms) for i in range(k.value)}["noise_model"]
+        g.check(lib.gls_converter_set_profiling(cal.handle, 0))
+        (ra, rb), pyr = cal.noise_model()
+    cal.close()
+    nlf_ms = nm[1] / 2
+    lv = [(W >> l) * (H >> l) for l in range(wl.levels)]
+    q = (W // 2) * (H // 2)
+    bytes_frame = (W * H * 2 + q * 32 + 3 * q * 32        # raw: scaled in, mean + var out, three fit passes
+                   + sum(lv) * (8 + 16) + 3 * sum(lv) * 16)  # levels: FP16 in, statistics out, three fit passes
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    gbs = bytes_frame / (nlf_ms / 1e3) / 1e9
+    return {
+        "workload": f"{W}x{H} RGGB 12-bit step chart, demosaic + 5-level denoise, FP16 storage, calibrateFromImage",
+        "value": 1e3 / ms_cal, "unit": "frames/s",
+        "ms_per_frame_calibrating": ms_cal, "ms_per_frame_given_model": ms_plain,
+        "measurement_ms_per_frame": nlf_ms, "measurement_launches_per_frame": nm[0] / 2,
+        "measured_raw_b": [float(x) for x in rb], "given_raw_b": [float(params.raw_nlf.b[c]) for c in range(4)],
+        "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                     "bytes_per_frame": bytes_frame,
+                     "note": "all measurement kernels of a frame together (raw and five YCbCr levels: statistics "
+                             "with the class histogram, then three fit passes each); peak "
+                             + ("of measured" if peaks else "of fallback")},
+        "note": "each measured model is read back to the host before the frame continues (six host syncs "
+                "per frame), as the reference's host regressions are; frames run one at a time",
+    }
+
+
 def run_reference(args, rank):
     """The reference arm: the reference's path on the host cores. The Metal
     runtime cannot run here; the reference's own kernel source, compiled
@@ -590,9 +671,9 @@ def main():
     conv = g.RawConverter(local)
     lib = g.lib()
     stream = torch.cuda.Stream()
-    if args.burst_only or args.adjoint_only or args.mixed_only or args.post_only:
+    if args.burst_only or args.adjoint_only or args.mixed_only or args.post_only or args.calibrate_only:
         leg = (burst_leg if args.burst_only else adjoint_leg if args.adjoint_only else
-               mixed_leg if args.mixed_only else post_leg)
+               mixed_leg if args.mixed_only else post_leg if args.post_only else calibrate_leg)
         b = leg(args, rank, local, conv, stream)
         if rank == 0:
             print(json.dumps({leg.__name__: True, **b}), flush=True)
@@ -762,6 +843,12 @@ def main():
         (pp["ms_per_batch_post"],) = max_over_ranks([pp["ms_per_batch_post"]], dist if world > 1 else None)
         pp["value"] = world * max(1, args.post_frames) / (pp["ms_per_batch_post"] / 1e3)
         line["post_process"] = pp
+    if not args.no_calibrate:
+        cl = calibrate_leg(args, rank, local, conv, stream)
+        (cl["ms_per_frame_calibrating"],) = max_over_ranks([cl["ms_per_frame_calibrating"]],
+                                                           dist if world > 1 else None)
+        cl["value"] = world * 1e3 / cl["ms_per_frame_calibrating"]
+        line["calibrate"] = cl
     if not args.no_adjoint:
         a = adjoint_leg(args, rank, local, conv, stream)
         (a["ms_per_batch"],) = max_over_ranks([a["ms_per_batch"]], dist if world > 1 else None)

@@ -288,7 +288,7 @@ static gls_status measure_raw_nlf(gls_converter* cv, Plane<S, 1> scaled, int pat
                                   gls_raw_nlf* out, cudaStream_t s) {
     const int mw = scaled.w / 2, mh = scaled.h / 2;
     if (mw < 1 || mh < 1) return set_error(GLS_ERR_INVALID_ARG, "raw noise measurement needs a frame of at least 2 x 2");
-    GLS_TRY(cv->nlf_scratch.ensure(nlf_scratch_bytes() + sizeof(gls_raw_nlf)));
+    GLS_TRY(cv->nlf_scratch.ensure_zeroed(nlf_scratch_bytes() + sizeof(gls_raw_nlf), s));
     GLS_TRY(cv->nlf_mean.ensure(size_t(mw) * mh * 4 * sizeof(float)));
     GLS_TRY(cv->nlf_var.ensure(size_t(mw) * mh * 4 * sizeof(float)));
     auto* dres = reinterpret_cast<gls_raw_nlf*>(static_cast<char*>(cv->nlf_scratch.p) + nlf_scratch_bytes());
@@ -306,7 +306,7 @@ static gls_status measure_raw_nlf(gls_converter* cv, Plane<S, 1> scaled, int pat
 template <class S>
 static gls_status measure_ycc_nlf(gls_converter* cv, Plane<S, 4> img, float exposure, gls_ycbcr_nlf* out,
                                   cudaStream_t s) {
-    GLS_TRY(cv->nlf_scratch.ensure(nlf_scratch_bytes() + sizeof(gls_raw_nlf)));
+    GLS_TRY(cv->nlf_scratch.ensure_zeroed(nlf_scratch_bytes() + sizeof(gls_raw_nlf), s));
     GLS_TRY(cv->nlf_stats.ensure(size_t(img.w) * img.h * 4 * sizeof(float)));
     auto* dres = reinterpret_cast<gls_raw_nlf*>(static_cast<char*>(cv->nlf_scratch.p) + nlf_scratch_bytes());
     {
