@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-post", action="store_true", help="skip the display post-processing leg")
     ap.add_argument("--post-only", action="store_true", help="run only the post-processing leg")
     ap.add_argument("--post-frames", type=int, default=N_ROTATE, help="frames per batch of the post-processing leg")
+    ap.add_argument("--no-dng", action="store_true", help="skip the DNG-file leg")
+    ap.add_argument("--dng-only", action="store_true", help="run only the DNG-file leg")
     ap.add_argument("--no-calibrate", action="store_true", help="skip the noise-model measurement leg")
     ap.add_argument("--calibrate-only", action="store_true", help="run only the noise-model measurement leg")
     return ap.parse_args()
@@ -619,6 +621,68 @@ def calibrate_leg(args, rank, local, conv, stream):
     }
 
 
+def dng_leg(args, rank, local, conv, stream):
+    """RawConverter::demosaic from DNG files, as pipelineTest's demosaicFile
+    and PyramidFusion's runPipeline run it (pipelineTest.cpp:110-175,
+    pyramidFusion.cpp:46-60): a 12 MP DNG with lossless-JPEG 256x256 tiles,
+    as phone DNGs carry, read and decoded on the host's cores, parameters
+    from its metadata and the camera calibration at its ISO, then demosaic,
+    denoise and display post-processing on the GPU with the sRGB result back
+    in host memory. Frames one at a time, wall clock."""
+    import tempfile
+
+    import glasscamerapublic_b200 as g
+    from glasscamerapublic_b200 import dng, scene
+
+    wl = scene.WORKLOADS[args.workload]
+    tmp = tempfile.mkdtemp(prefix="gls_dng_")
+    paths = []
+    for f in range(2):
+        raw, _ = scene.make_raw(wl, frame=300 + rank * 2 + f)
+        info = g.DngInfo()
+        info.cfa_pattern[:] = [0, 1, 1, 2]
+        info.black_level, info.white_level, info.iso = wl.black, wl.white, wl.iso
+        info.has_color_matrix2 = 1
+        info.color_matrix2[:] = [0.66, -0.13, -0.07, -0.39, 1.21, 0.17, -0.06, 0.17, 0.55]
+        info.has_as_shot_neutral = 1
+        info.as_shot_neutral[:] = [0.52, 1.0, 0.61]
+        info.make, info.model = b"Apple", b"iPhone 14 Pro"
+        path = os.path.join(tmp, f"frame{f}.dng")
+        dng.write_dng(path, raw, info, dng.COMPRESSION_LJ92, 256)
+        paths.append(path)
+    size = os.path.getsize(paths[0])
+
+    def one(path):
+        raw, info = dng.read_dng(path)
+        p = dng.demosaic_params(info)
+        return conv.demosaic(raw, p, fp16=True, out_fp16=True, postProcess=True)
+
+    for path in paths:
+        one(path)
+    n = max(3, args.steps // 2)
+    t0 = time.perf_counter()
+    for i in range(n):
+        out = one(paths[i % 2])
+    t_frame = (time.perf_counter() - t0) / n
+    t0 = time.perf_counter()
+    for i in range(n):
+        dng.read_dng(paths[i % 2])
+    t_read = (time.perf_counter() - t0) / n
+    for path in paths:
+        os.remove(path)
+    os.rmdir(tmp)
+    return {
+        "workload": f"{wl.width}x{wl.height} RGGB 12-bit DNG, lossless JPEG 256x256 tiles, "
+                    "demosaic + 5-level denoise + post-processing, FP16 storage",
+        "value": 1.0 / t_frame, "unit": "frames/s",
+        "ms_per_frame": 1e3 * t_frame, "read_ms_per_frame": 1e3 * t_read,
+        "decode_mp_per_s": wl.width * wl.height / 1e6 / t_read, "file_mb": size / 1e6,
+        "host_threads": os.cpu_count(), "output": list(out.shape),
+        "note": "wall clock per file: DNG read and lossless-JPEG decode on the host (tiles in parallel), "
+                "parameters from the metadata, the GPU path with host I/O (FP16 sRGB out)",
+    }
+
+
 def run_reference(args, rank):
     """The reference arm: the reference's path on the host cores. The Metal
     runtime cannot run here; the reference's own kernel source, compiled
@@ -671,9 +735,11 @@ def main():
     conv = g.RawConverter(local)
     lib = g.lib()
     stream = torch.cuda.Stream()
-    if args.burst_only or args.adjoint_only or args.mixed_only or args.post_only or args.calibrate_only:
+    if (args.burst_only or args.adjoint_only or args.mixed_only or args.post_only or args.calibrate_only
+            or args.dng_only):
         leg = (burst_leg if args.burst_only else adjoint_leg if args.adjoint_only else
-               mixed_leg if args.mixed_only else post_leg if args.post_only else calibrate_leg)
+               mixed_leg if args.mixed_only else post_leg if args.post_only else
+               calibrate_leg if args.calibrate_only else dng_leg)
         b = leg(args, rank, local, conv, stream)
         if rank == 0:
             print(json.dumps({leg.__name__: True, **b}), flush=True)
@@ -843,6 +909,11 @@ def main():
         (pp["ms_per_batch_post"],) = max_over_ranks([pp["ms_per_batch_post"]], dist if world > 1 else None)
         pp["value"] = world * max(1, args.post_frames) / (pp["ms_per_batch_post"] / 1e3)
         line["post_process"] = pp
+    if not args.no_dng:
+        dl = dng_leg(args, rank, local, conv, stream)
+        (dl["ms_per_frame"],) = max_over_ranks([dl["ms_per_frame"]], dist if world > 1 else None)
+        dl["value"] = world * 1e3 / dl["ms_per_frame"]
+        line["dng_file"] = dl
     if not args.no_calibrate:
         cl = calibrate_leg(args, rank, local, conv, stream)
         (cl["ms_per_frame_calibrating"],) = max_over_ranks([cl["ms_per_frame_calibrating"]],

@@ -111,6 +111,20 @@ class DemosaicParams(C.Structure):
     ]
 
 
+class DngInfo(C.Structure):
+    """gls_dng_info: a DNG's raw layout and the metadata the parameters
+    are built from."""
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("bits_per_sample", C.c_int32),
+                ("compression", C.c_int32), ("cfa_pattern", C.c_uint8 * 4), ("bayer_pattern", C.c_int32),
+                ("black_level", C.c_float), ("white_level", C.c_float), ("baseline_exposure", C.c_float),
+                ("has_color_matrix1", C.c_int32), ("has_color_matrix2", C.c_int32),
+                ("has_as_shot_neutral", C.c_int32), ("color_matrix1", C.c_float * 9),
+                ("color_matrix2", C.c_float * 9), ("as_shot_neutral", C.c_float * 3),
+                ("calibration_illuminant1", C.c_int32), ("calibration_illuminant2", C.c_int32),
+                ("iso", C.c_int32), ("exposure_time", C.c_float), ("active_area", C.c_int32 * 4),
+                ("make", C.c_char * 64), ("model", C.c_char * 64), ("lens_model", C.c_char * 96)]
+
+
 class ImageView(C.Structure):
     _fields_ = [
         ("data", C.c_void_p),
@@ -170,6 +184,10 @@ _SIGNATURES = {
     "gls_converter_reset_stats": (C.c_int, [C.c_void_p]),
     "gls_block_match_tiles": (C.c_int, [C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)]),
     "gls_grain_tables": (C.c_int, [C.c_uint32, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
+    "gls_dng_read": (C.c_int, [C.c_char_p, C.POINTER(DngInfo), C.c_void_p, C.c_size_t]),
+    "gls_dng_write": (C.c_int, [C.c_char_p, C.POINTER(DngInfo), C.c_void_p, C.c_size_t, C.c_int32, C.c_int32]),
+    "gls_dng_demosaic_params": (C.c_int, [C.POINTER(DngInfo), C.c_void_p, C.c_int32, C.POINTER(DemosaicParams)]),
+    "gls_dng_camera": (C.c_int32, [C.POINTER(DngInfo)]),
     "gls_measure_raw_nlf": (C.c_int, [C.c_void_p, C.POINTER(ImageView), C.c_int32, C.c_float, C.POINTER(RawNLF),
                                       C.c_void_p]),
     "gls_measure_ycbcr_nlf": (C.c_int, [C.c_void_p, C.POINTER(ImageView), C.c_float, C.POINTER(YCbCrNLF),

@@ -317,6 +317,70 @@ gls_status gls_block_match_tiles(int32_t* entries, int32_t max_entries, int32_t*
 enum { GLS_CAMERA_IPHONE14_WIDE = 0 };
 gls_status gls_calibration_fill(int32_t camera, int32_t iso, gls_demosaic_params* params);
 
+/* ==== DNG ingest (no live reference code: the reference reads DNGs with
+ * the un-vendored GlassImage library, gls::image::read_dng_file, used at
+ * pipelineTest.cpp:114-115 and pyramidFusion.cpp:50, 297, 322) ====
+ * A self-contained TIFF/DNG reader for the CFA raw image of a DNG: the raw
+ * IFD is the first IFD (IFD0 or a SubIFD) with NewSubFileType 0 and CFA
+ * photometric interpretation; its samples are uncompressed (8, 16 or
+ * 10/12/14-bit packed MSB first, rows byte-aligned) or lossless JPEG
+ * (ITU-T T.81 process 14, predictors 1-7, any component interleave; DNG
+ * Compression 7), in strips or tiles; tiles are decoded in parallel on the
+ * host. gls_dng_info carries the metadata unpackDNGMetadata and
+ * CameraCalibration::getDemosaicParameters read (demosaic_utils.cpp:268-366,
+ * CameraCalibration.cpp:25-58). */
+typedef struct gls_dng_info {
+    int32_t width, height;              /* raw image */
+    int32_t bits_per_sample;
+    int32_t compression;                /* 1 or 7 */
+    uint8_t cfa_pattern[4];             /* CFAPattern (0 R, 1 G, 2 B) */
+    int32_t bayer_pattern;              /* GLS_GRBG .. GLS_BGGR, from cfa_pattern as the reference maps it */
+    float black_level;                  /* BlackLevel[0], 0 if absent */
+    float white_level;                  /* WhiteLevel[0], 65535 if absent */
+    float baseline_exposure;            /* BaselineExposure (EV), 0 if absent */
+    int32_t has_color_matrix1, has_color_matrix2, has_as_shot_neutral;
+    float color_matrix1[9], color_matrix2[9]; /* XYZ -> camera, row-major */
+    float as_shot_neutral[3];
+    int32_t calibration_illuminant1, calibration_illuminant2;
+    int32_t iso;                        /* EXIF RecommendedExposureIndex, else ISOSpeedRatings, else 0 */
+    float exposure_time;                /* EXIF ExposureTime (s), 0 if absent */
+    int32_t active_area[4];             /* top, left, bottom, right (the whole image if absent) */
+    char make[64], model[64], lens_model[96];
+} gls_dng_info;
+
+/* Reads a DNG's raw image and metadata. With raw NULL only *info is filled
+ * (to size the buffer). raw: width x height uint16 host memory, row stride
+ * raw_stride_elems (>= width). */
+gls_status gls_dng_read(const char* path, gls_dng_info* info, uint16_t* raw, size_t raw_stride_elems);
+
+/* Writes raw (width x height uint16, host) as a DNG carrying info's
+ * metadata (a single CFA IFD0 with an EXIF IFD): compression 1
+ * (uncompressed 16-bit) or 7 (lossless JPEG, predictor 1, tiles of
+ * tile_size x tile_size, two components per row as DNG writers interleave
+ * Bayer rows; tile_size 0: one strip). The reference captures DNGs through
+ * the operating system; this writer exists for round trips and tests. */
+gls_status gls_dng_write(const char* path, const gls_dng_info* info, const uint16_t* raw, size_t raw_stride_elems,
+                         int32_t compression, int32_t tile_size);
+
+/* CameraCalibration::getDemosaicParameters (CameraCalibration.cpp:25-58)
+ * with unpackDNGMetadata (demosaic_utils.cpp:268-366) without automatic
+ * white balance: black and white levels, Bayer pattern, exposure
+ * multiplier (2^BaselineExposure, at most 1; scale_mul takes the rest),
+ * rgb_cam from ColorMatrix2 (else ColorMatrix1) and xyz_rgb
+ * (cam_xyz_coeff, demosaic_utils.cpp:78-101), the white balance from
+ * AsShotNeutral (else the matrix's white), scale_mul, then the camera's
+ * noise model and denoise schedule at the EXIF ISO. camera: a
+ * GLS_CAMERA_* id. xyz_rgb may be NULL (sRGB). Returns GLS_ERR_RANGE for a
+ * singular colour matrix or an ISO the calibration does not cover. */
+gls_status gls_dng_demosaic_params(const gls_dng_info* info, const float* xyz_rgb, int32_t camera,
+                                   gls_demosaic_params* params);
+
+/* The camera a DNG was taken with, as pipelineTest.cpp:133-160 selects it
+ * (Apple iPhone 14 Pro / Pro Max by lens model; unknown lenses use the
+ * wide camera): a GLS_CAMERA_* id, or -1 for a device without a
+ * calibration. */
+int32_t gls_dng_camera(const gls_dng_info* info);
+
 /* Gaussian kernel folded into bilinear taps (weight, dx, dy) per tap,
  * gaussianKernelBilinearWeights, demosaic_utils.cpp:987-1006. Writes at
  * most max_taps taps; *n_taps receives the count. */

@@ -1,0 +1,51 @@
+"""A DNG file through the whole path on the GPU: gls_dng_read ->
+gls_dng_demosaic_params -> gls_demosaic (noise reduction and display
+post-processing), as the reference's pipelineTest demosaicFile and
+PyramidFusion runPipeline do (pipelineTest.cpp:110-175,
+pyramidFusion.cpp:46-60). The raw comes back bit-exact from the file, and
+the output matches the oracle's pipeline on the DNG's parameters to the raw
+path's tolerance."""
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import _oracle as O
+import glasscamerapublic_b200 as g
+from glasscamerapublic_b200 import dng, scene
+
+sys.path.insert(0, str(Path(__file__).resolve().parents[1] / "oracle"))
+
+pytestmark = pytest.mark.gpu
+
+
+def _dng(tmp_path, w=512, h=384, iso=1600, comp=7, tile=128):
+    wl = scene.Workload("dng", w, h, levels=5, gain=0.5, read=3.0, iso=iso, seed=21)
+    raw, _ = scene.make_raw(wl)
+    info = g.DngInfo()
+    info.cfa_pattern[:] = [0, 1, 1, 2]
+    info.black_level, info.white_level, info.iso = wl.black, wl.white, iso
+    info.has_color_matrix2 = 1
+    info.color_matrix2[:] = [0.66, -0.13, -0.07, -0.39, 1.21, 0.17, -0.06, 0.17, 0.55]
+    info.has_as_shot_neutral = 1
+    info.as_shot_neutral[:] = [0.52, 1.0, 0.61]
+    info.make, info.model = b"Apple", b"iPhone 14 Pro"
+    f = tmp_path / "frame.dng"
+    dng.write_dng(f, raw, info, comp, tile)
+    return f, raw
+
+
+@pytest.mark.parametrize("comp,tile", [(7, 128), (1, 0)])
+def test_dng_file_through_the_path(converter, tmp_path, comp, tile):
+    f, raw = _dng(tmp_path, comp=comp, tile=tile)
+    back, info = dng.read_dng(f)
+    assert np.array_equal(back, raw)
+    p = dng.demosaic_params(info)
+    assert p.bayer_pattern == 2 and p.levels == 5
+    out = converter.demosaic(back, p)  # linear camera RGB
+    ref = O.raw_pipeline(back, p, denoise=True, f64=False)["out"]
+    d = np.abs(out[..., :3].astype(np.float64) - ref[..., :3])
+    assert np.quantile(d, 0.999) <= 1e-4, np.quantile(d, 0.999)
+    srgb = converter.demosaic(back, p, fp16=True, postProcess=True)
+    assert np.isfinite(srgb).all() and srgb[..., :3].min() >= 0 and srgb[..., :3].max() <= 1
