@@ -381,6 +381,20 @@ gls_status gls_dng_demosaic_params(const gls_dng_info* info, const float* xyz_rg
  * calibration. */
 int32_t gls_dng_camera(const gls_dng_info* info);
 
+/* ==== Burst driver host side (PyramidFusion/pyramidFusion.cpp) ==== */
+
+/* findBursts (pyramidFusion.cpp:166-195) over paths in directory order
+ * (parseDirectory sorts them, :36-44): a file whose stem contains "_1_"
+ * starts a burst; later files join it when their stem has the same prefix
+ * up to that position. burst_of[i] receives file i's burst (0, 1, ...) or
+ * -1; *n_bursts the number of bursts. */
+gls_status gls_find_bursts(const char* const* paths, int32_t n, int32_t* burst_of, int32_t* n_bursts);
+
+/* saveFusedImage (pyramidFusion.cpp:152-164): an RGBA (or RGB) F32/F16
+ * image, host or device memory, written as an uncompressed 8-bit RGB TIFF
+ * with (uint8) (255 * clamp(v, 0, 1)) per channel. */
+gls_status gls_write_tiff_rgb8(const char* path, const gls_image_view* rgba, void* stream);
+
 /* Gaussian kernel folded into bilinear taps (weight, dx, dy) per tap,
  * gaussianKernelBilinearWeights, demosaic_utils.cpp:987-1006. Writes at
  * most max_taps taps; *n_taps receives the count. */

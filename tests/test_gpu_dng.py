@@ -49,3 +49,34 @@ def test_dng_file_through_the_path(converter, tmp_path, comp, tile):
     assert np.quantile(d, 0.999) <= 1e-4, np.quantile(d, 0.999)
     srgb = converter.demosaic(back, p, fp16=True, postProcess=True)
     assert np.isfinite(srgb).all() and srgb[..., :3].min() >= 0 and srgb[..., :3].max() <= 1
+
+
+def test_burst_of_dng_files_through_the_driver(converter, tmp_path):
+    # PyramidFusion's main(): four DNGs found by name, the "_4_" frame the reference
+    import torch
+    from glasscamerapublic_b200 import burst
+    wl = scene.Workload("b", 1024, 768, levels=5, gain=1.5, read=4.0, iso=800, seed=3000)
+    raws, cleans, Hs = scene.make_burst(wl, 4)
+    raw_dir = tmp_path / "Raw"
+    raw_dir.mkdir()
+    names = ["IMG_7_4_.dng", "IMG_7_1_.dng", "IMG_7_2_.dng", "IMG_7_3_.dng"]  # frame 0 is the reference
+    for raw, name in zip(raws, names):
+        info = g.DngInfo()
+        info.cfa_pattern[:] = [0, 1, 1, 2]
+        info.black_level, info.white_level, info.iso = wl.black, wl.white, wl.iso
+        info.has_color_matrix2 = 1
+        info.color_matrix2[:] = [0.66, -0.13, -0.07, -0.39, 1.21, 0.17, -0.06, 0.17, 0.55]
+        info.make, info.model = b"Apple", b"iPhone 14 Pro"
+        dng.write_dng(raw_dir / name, raw, info, 7, 256)
+    bursts = burst.find_bursts(burst.parse_directory(raw_dir))
+    assert len(bursts) == 1 and [p.rsplit("/", 1)[-1] for p in bursts[0]] == names[1:] + names[:1]
+    fused, Hest, out = burst.fuse_burst(converter, bursts[0])
+    assert out.endswith("Fusion/IMG_7aRH_fork.tiff")
+    errs = [scene.corner_error(He, Ht, wl.width, wl.height) for He, Ht in zip(Hest, Hs[1:])]
+    assert max(errs) < 3.0, errs
+    got = burst.read_tiff_rgb8(out)
+    want = (255 * np.clip(fused.cpu().numpy()[..., :3], 0, 1)).astype(np.uint8)
+    assert np.array_equal(got, want)
+    p = dng.demosaic_params(dng.read_dng(bursts[0][3])[1])
+    ref = converter.demosaic(torch.from_numpy(raws[0].view(np.int16)).cuda(), p, fp16=True, postProcess=True)
+    assert scene.psnr(fused.cpu().numpy()[64:-64, 64:-64, :3], ref.float().cpu().numpy()[64:-64, 64:-64, :3]) > 28.0
