@@ -664,6 +664,15 @@ def dng_leg(args, rank, local, conv, stream):
     for i in range(n):
         out = one(paths[i % 2])
     t_frame = (time.perf_counter() - t0) / n
+    # pipelined over files: the next file decoded on a host thread into a
+    # pinned buffer while the GPU converts the current one
+    seq = [paths[i % 2] for i in range(2 * n)]
+    for _ in dng.convert_files(conv, paths):
+        pass
+    t0 = time.perf_counter()
+    for _ in dng.convert_files(conv, seq):
+        pass
+    t_pipe = (time.perf_counter() - t0) / len(seq)
     t0 = time.perf_counter()
     for i in range(n):
         dng.read_dng(paths[i % 2])
@@ -674,12 +683,15 @@ def dng_leg(args, rank, local, conv, stream):
     return {
         "workload": f"{wl.width}x{wl.height} RGGB 12-bit DNG, lossless JPEG 256x256 tiles, "
                     "demosaic + 5-level denoise + post-processing, FP16 storage",
-        "value": 1.0 / t_frame, "unit": "frames/s",
-        "ms_per_frame": 1e3 * t_frame, "read_ms_per_frame": 1e3 * t_read,
+        "value": 1.0 / t_pipe, "unit": "frames/s",
+        "ms_per_frame": 1e3 * t_pipe, "ms_per_frame_one_at_a_time": 1e3 * t_frame,
+        "read_ms_per_frame": 1e3 * t_read,
         "decode_mp_per_s": wl.width * wl.height / 1e6 / t_read, "file_mb": size / 1e6,
         "host_threads": os.cpu_count(), "output": list(out.shape),
         "note": "wall clock per file: DNG read and lossless-JPEG decode on the host (tiles in parallel), "
-                "parameters from the metadata, the GPU path with host I/O (FP16 sRGB out)",
+                "parameters from the metadata, the GPU path with host I/O (FP16 sRGB out); value: files "
+                "pipelined (dng.convert_files: the next file decoded into pinned memory while the GPU "
+                "converts the current one); ms_per_frame_one_at_a_time: read, then convert, per file",
     }
 
 

@@ -80,3 +80,18 @@ def test_burst_of_dng_files_through_the_driver(converter, tmp_path):
     p = dng.demosaic_params(dng.read_dng(bursts[0][3])[1])
     ref = converter.demosaic(torch.from_numpy(raws[0].view(np.int16)).cuda(), p, fp16=True, postProcess=True)
     assert scene.psnr(fused.cpu().numpy()[64:-64, 64:-64, :3], ref.float().cpu().numpy()[64:-64, 64:-64, :3]) > 28.0
+
+
+def test_pipelined_file_conversion_matches_one_at_a_time(converter, tmp_path):
+    paths = []
+    for k in range(3):
+        d = tmp_path / f"{k}"
+        d.mkdir()
+        f, _ = _dng(d, w=384, h=256)
+        paths.append(f)
+    got = [(p, o.numpy().copy()) for p, o in dng.convert_files(converter, paths)]
+    assert [p for p, _ in got] == [str(p) for p in paths]
+    for path, out in got:
+        back, info = dng.read_dng(path)
+        ref = converter.demosaic(back, dng.demosaic_params(info), fp16=True, out_fp16=True, postProcess=True)
+        assert np.array_equal(out, ref)
