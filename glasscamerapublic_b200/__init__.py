@@ -185,6 +185,8 @@ _SIGNATURES = {
     "gls_block_match_tiles": (C.c_int, [C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)]),
     "gls_grain_tables": (C.c_int, [C.c_uint32, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     "gls_find_bursts": (C.c_int, [C.POINTER(C.c_char_p), C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "gls_convert_to_grayscale": (C.c_int, [C.POINTER(ImageView), C.POINTER(C.c_float), C.POINTER(ImageView),
+                                           C.c_void_p]),
     "gls_write_tiff_rgb8": (C.c_int, [C.c_char_p, C.POINTER(ImageView), C.c_void_p]),
     "gls_dng_read": (C.c_int, [C.c_char_p, C.POINTER(DngInfo), C.c_void_p, C.c_size_t]),
     "gls_dng_write": (C.c_int, [C.c_char_p, C.POINTER(DngInfo), C.c_void_p, C.c_size_t, C.c_int32, C.c_int32]),

@@ -108,3 +108,20 @@ def fuse_burst(converter, paths, out_path=None, fp16: bool = True, stream=None):
         out_path = out_dir / (base + "aRH_fork.tiff")
     write_tiff_rgb8(out_path, fused)
     return fused, Hs, str(out_path)
+
+
+def convert_to_grayscale(rgb, transform, out=None, stream=None):
+    """convertToGrayscale (demosaic.metal:1707-1723) on a CUDA RGBA tensor:
+    max(t . ((rgb - 0.1) / 0.9), 0) as an (h, w) float32 CUDA tensor."""
+    import torch
+
+    from .api import _ptr, _row_stride, _stream_handle
+
+    h, w = rgb.shape[:2]
+    if out is None:
+        out = torch.empty((h, w), dtype=torch.float32, device=rgb.device)
+    iv = ImageView(C.c_void_p(_ptr(rgb)), w, h, 4, F32 if rgb.dtype == torch.float32 else 1, _row_stride(rgb))
+    ov = ImageView(C.c_void_p(_ptr(out)), w, h, 1, F32, _row_stride(out))
+    t = (C.c_float * 3)(*[float(v) for v in transform])
+    check(lib().gls_convert_to_grayscale(C.byref(iv), t, C.byref(ov), _stream_handle(stream)))
+    return out

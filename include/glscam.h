@@ -390,6 +390,14 @@ int32_t gls_dng_camera(const gls_dng_info* info);
  * -1; *n_bursts the number of bursts. */
 gls_status gls_find_bursts(const char* const* paths, int32_t n, int32_t* burst_of, int32_t* n_bursts);
 
+/* convertToGrayscale (demosaic.metal:1707-1723), the luma image
+ * PyramidFusion's main_full registers on (convertImage,
+ * pyramidFusion.cpp:80-98, transform = rgb_cam's first row):
+ * gray = max(t . ((rgb - 0.1) / 0.9), 0). rgb: 4 ch F32/F16, gray: 1 ch
+ * F32, both device memory; asynchronous on stream. */
+gls_status gls_convert_to_grayscale(const gls_image_view* rgb, const float* transform, gls_image_view* gray,
+                                    void* stream);
+
 /* saveFusedImage (pyramidFusion.cpp:152-164): an RGBA (or RGB) F32/F16
  * image, host or device memory, written as an uncompressed 8-bit RGB TIFF
  * with (uint8) (255 * clamp(v, 0, 1)) per channel. */

@@ -547,6 +547,18 @@ int ref_demosaic_post(const uint16_t* raw, int w, int h, const gls_demosaic_para
     return ref_postprocess(levels.data(), grad.data(), cam.data(), w, h, p, raw[0], out, stats);
 }
 
+// convertToGrayscale (demosaic.metal:1707-1723): rgb w x h x 4, gray w x h
+int ref_convert_to_grayscale(const float* rgb, int w, int h, const float* t, float* gray) {
+    Tex in(w, h, 4), out(w, h, 1);
+    std::copy(rgb, rgb + size_t(w) * h * 4, in.f.begin());
+    auto ti = in.t<float>();
+    auto to = out.t<float, access::write>();
+    const metal::float3 tr(t[0], t[1], t[2]);
+    run_grid(w, h, [&](metal::uint2 i) { convertToGrayscale(ti, to, tr, i); });
+    std::copy(out.f.begin(), out.f.end(), gray);
+    return 0;
+}
+
 void ref_set_threads(int n) { orc::num_threads() = n > 0 ? n : 1; }
 
 }  // extern "C"

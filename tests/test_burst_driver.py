@@ -59,3 +59,27 @@ def test_tiff_rgb8_is_the_clamped_truncation(tmp_path):
     got = burst.read_tiff_rgb8(f)
     want = (255 * np.clip(img[..., :3], 0, 1)).astype(np.uint8)
     assert np.array_equal(got, want)
+
+
+def _gray_formula(rgb, t):
+    """max(t . ((rgb - 0.1) / 0.9), 0) in float32, one rounding per operation."""
+    f = np.float32
+    p = ((rgb[..., :3].astype(f) - f(0.1)) / f(0.9)).astype(f)
+    d = (f(t[0]) * p[..., 0] + f(t[1]) * p[..., 1]).astype(f) + (f(t[2]) * p[..., 2]).astype(f)
+    return np.maximum(d.astype(f), f(0))
+
+
+def test_grayscale_formula_is_the_reference_kernel():
+    import _ref as R
+    if not R.available():
+        pytest.skip("reference kernels not built (make -C oracle ref)")
+    import ctypes as C
+    L = R.lib()
+    fp = C.POINTER(C.c_float)
+    L.ref_convert_to_grayscale.argtypes = [fp, C.c_int, C.c_int, fp, fp]
+    rng = np.random.default_rng(4)
+    rgb = rng.uniform(-0.1, 1.2, (24, 40, 4)).astype(np.float32)
+    t = np.array([1.9, -0.7, -0.2], np.float32)
+    gray = np.zeros((24, 40), np.float32)
+    L.ref_convert_to_grayscale(rgb.ctypes.data_as(fp), 40, 24, t.ctypes.data_as(fp), gray.ctypes.data_as(fp))
+    assert np.array_equal(gray, _gray_formula(rgb, t))

@@ -95,3 +95,20 @@ def test_pipelined_file_conversion_matches_one_at_a_time(converter, tmp_path):
         back, info = dng.read_dng(path)
         ref = converter.demosaic(back, dng.demosaic_params(info), fp16=True, out_fp16=True, postProcess=True)
         assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("half", [False, True])
+def test_grayscale_conversion(converter, half):
+    import torch
+    from glasscamerapublic_b200 import burst
+    sys.path.insert(0, str(Path(__file__).resolve().parent))
+    from test_burst_driver import _gray_formula
+    rng = np.random.default_rng(5)
+    rgb = rng.uniform(-0.1, 1.2, (200, 328, 4)).astype(np.float32)
+    if half:
+        rgb = rgb.astype(np.float16).astype(np.float32)
+    t = [1.9, -0.7, -0.2]
+    dev = torch.from_numpy(rgb).cuda()
+    out = burst.convert_to_grayscale(dev.half() if half else dev, t)
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), _gray_formula(rgb, t))
