@@ -162,10 +162,8 @@ __global__ void __launch_bounds__(352) k_pca_cov(Plane<S, 4> img, double* __rest
 // Symmetric eigen-solve of the 25x25 patch covariance (replaces Eigen's
 // SelfAdjointEigenSolver, PCA.cpp:36): parallel cyclic Jacobi in FP64 on a
 // 26x26 matrix (25 + one zero pad row/column) with the round-robin pair
-// schedule (13 disjoint rotations per round, 25 rounds per sweep, each
-// round one barrier: every thread forms the rotations it needs and writes
-// its element of the rotated matrix to a second buffer). One block of 1024
-// threads; every sweep is a bounded loop (at most 40 sweeps),
+// schedule (13 disjoint rotations per round, 25 rounds per sweep). One
+// block of 1024 threads; every sweep is a bounded loop (at most 40 sweeps),
 // so the kernel always ends. The top-8 eigenvectors (descending eigenvalue,
 // each signed so its largest-magnitude entry is positive) are written as a
 // row-major 25x8 FP32 basis. status receives the sweep count, or -1 when
@@ -176,6 +174,8 @@ __global__ void __launch_bounds__(1024) k_pca_eigen(const double* __restrict__ p
                                                    float* __restrict__ basis, int* status) {
     __shared__ double acc[kPcaAcc];
     __shared__ double A[EJ_N][EJ_N + 1], B[EJ_N][EJ_N + 1], V[EJ_N][EJ_N + 1], V2[EJ_N][EJ_N + 1];
+    __shared__ double rc[EJ_N], rs[EJ_N];  // per index: rotation (c, s)
+    __shared__ int partner[EJ_N], isp[EJ_N];
     __shared__ double red[32];
     __shared__ int done, order[25];
     const int t = threadIdx.x;
@@ -210,14 +210,12 @@ __global__ void __launch_bounds__(1024) k_pca_eigen(const double* __restrict__ p
     if (t == 0) done = 0;
     __syncthreads();
 
-    // the current matrices and the buffers of the next round
-    double(*Ac)[EJ_N + 1] = A, (*An)[EJ_N + 1] = B, (*Vc)[EJ_N + 1] = V, (*Vn)[EJ_N + 1] = V2;
     int sweep = 0;
     for (; sweep < 40; sweep++) {
         // convergence test: off-diagonal vs total Frobenius mass
         double off = 0.0, tot = 0.0;
         if (act) {
-            const double a = Ac[i][j];
+            const double a = A[i][j];
             tot = a * a;
             off = (i != j) ? a * a : 0.0;
         }
@@ -242,58 +240,56 @@ __global__ void __launch_bounds__(1024) k_pca_eigen(const double* __restrict__ p
         __syncthreads();
         if (done) break;
         for (int round = 0; round < 25; round++) {
-            // pairs of this round: (25, round) and ((round+m)%25, (round-m+25)%25),
-            // m = 1..12: index k's partner is 25 for k = round, round for k = 25,
-            // else (2 round - k) mod 25. Every thread forms the rotations of its
-            // row's and its column's pair from the current matrix (the same
-            // values for every thread), so a round needs one barrier: the new
-            // A = J^T A J and V = V J go to the other buffers.
-            auto rot = [&](int k, int& pk, double& c, double& s) {  // returns whether k is its pair's p
-                pk = k == 25 ? round : (k == round ? 25 : (2 * round - k + 50) % 25);
-                const int p = min(k, pk), q = max(k, pk);
-                const double apq = Ac[p][q], app = Ac[p][p], aqq = Ac[q][q];
-                c = 1.0;
-                s = 0.0;
+            // pairs of this round: (25, round) and ((round+m)%25, (round-m+25)%25), m = 1..12
+            if (t < 13) {
+                int p, q;
+                if (t == 0) {
+                    p = round;
+                    q = 25;
+                } else {
+                    p = (round + t) % 25;
+                    q = (round - t + 25) % 25;
+                }
+                if (p > q) {
+                    const int tmp = p;
+                    p = q;
+                    q = tmp;
+                }
+                const double apq = A[p][q], app = A[p][p], aqq = A[q][q];
+                double c = 1.0, s = 0.0;
                 if (fabs(apq) >= 1e-300) {
                     const double theta = (aqq - app) / (2.0 * apq);
                     const double tt = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
                     c = 1.0 / sqrt(tt * tt + 1.0);
                     s = tt * c;
                 }
-                return k == p;
-            };
-            if (act) {
-                int pi, pj;
-                double ci, si, cj, sj;
-                const bool ispi = rot(i, pi, ci, si), ispj = rot(j, pj, cj, sj);
-                // columns (B = A J) of rows i and pi, then the row rotation
-                double bij, bpj;
-                if (ispj) {
-                    bij = cj * Ac[i][j] - sj * Ac[i][pj];
-                    bpj = cj * Ac[pi][j] - sj * Ac[pi][pj];
-                    Vn[i][j] = cj * Vc[i][j] - sj * Vc[i][pj];
-                } else {
-                    bij = sj * Ac[i][pj] + cj * Ac[i][j];
-                    bpj = sj * Ac[pi][pj] + cj * Ac[pi][j];
-                    Vn[i][j] = sj * Vc[i][pj] + cj * Vc[i][j];
-                }
-                An[i][j] = ispi ? ci * bij - si * bpj : si * bpj + ci * bij;
+                rc[p] = c; rs[p] = s; partner[p] = q; isp[p] = 1;
+                rc[q] = c; rs[q] = s; partner[q] = p; isp[q] = 0;
             }
             __syncthreads();
-            double(*ta)[EJ_N + 1] = Ac;
-            Ac = An;
-            An = ta;
-            double(*tv)[EJ_N + 1] = Vc;
-            Vc = Vn;
-            Vn = tv;
+            // columns: B = A J, V2 = V J
+            if (act) {
+                const int pj = partner[j];
+                const double c = rc[j], s = rs[j];
+                if (isp[j]) {
+                    B[i][j] = c * A[i][j] - s * A[i][pj];
+                    V2[i][j] = c * V[i][j] - s * V[i][pj];
+                } else {
+                    B[i][j] = s * A[i][pj] + c * A[i][j];
+                    V2[i][j] = s * V[i][pj] + c * V[i][j];
+                }
+            }
+            __syncthreads();
+            // rows: A = J^T B
+            if (act) {
+                const int pi = partner[i];
+                const double c = rc[i], s = rs[i];
+                if (isp[i]) A[i][j] = c * B[i][j] - s * B[pi][j];
+                else A[i][j] = s * B[pi][j] + c * B[i][j];
+                V[i][j] = V2[i][j];
+            }
+            __syncthreads();
         }
-    }
-    if (Ac != A) {  // the result in A and V
-        if (act) {
-            A[i][j] = Ac[i][j];
-            V[i][j] = Vc[i][j];
-        }
-        __syncthreads();
     }
     // order eigenvalues descending (stable by index)
     if (t == 0) {
