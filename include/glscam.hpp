@@ -70,6 +70,14 @@ class CameraCalibration {
         p.levels = int32_t(levels);
         return p;
     }
+    // getDemosaicParameters(raw, xyz_rgb, &dng_metadata, &exif_metadata)
+    // (CameraCalibration.cpp:25-58) from a DNG's metadata (read_dng_file)
+    DemosaicParameters getDemosaicParameters(const gls_dng_info& dng, const float* xyz_rgb = nullptr) const {
+        DemosaicParameters p{};
+        check(gls_dng_demosaic_params(&dng, xyz_rgb, camera_, &p));
+        p.levels = int32_t(levels);
+        return p;
+    }
     std::pair<gls_raw_nlf, std::array<gls_ycbcr_nlf, levels>> nlfFromIso(int iso) const {
         const DemosaicParameters p = getDemosaicParameters(iso);
         std::array<gls_ycbcr_nlf, levels> y{};
@@ -124,10 +132,29 @@ class RawConverter {
     // memory with host_io), asynchronous on the stream unless host_io
     void demosaic(const uint16_t* raw, int width, int height, size_t stride_bytes, const DemosaicParameters* params,
                   ImageView* out, bool noiseReduction = true, bool fp16 = true, bool host_io = false,
-                  void* stream = nullptr) {
+                  void* stream = nullptr, bool postProcess = false) {
         uint32_t flags = flag_if(noiseReduction, GLS_DENOISE) | flag_if(fp16, GLS_FP16_STORAGE) |
-                         flag_if(host_io, GLS_HOST_IO);
+                         flag_if(host_io, GLS_HOST_IO) | flag_if(postProcess, GLS_POSTPROCESS);
         check(gls_demosaic(conv_, raw, width, height, stride_bytes, params, flags, out, stream));
+    }
+
+    // MeasureRawNLF (raw_converter.cpp:339-490) on a scaled raw frame
+    // (1 ch F32/F16 device memory); synchronous
+    gls_raw_nlf MeasureRawNLF(const ImageView& scaled, BayerPattern pattern, float exposure_multiplier = 1,
+                              void* stream = nullptr) {
+        gls_raw_nlf n{};
+        check(gls_measure_raw_nlf(conv_, &scaled, int32_t(pattern), exposure_multiplier, &n, stream));
+        return n;
+    }
+
+    // the models the last call of a calibrateFromImage converter measured
+    std::pair<gls_raw_nlf, std::vector<gls_ycbcr_nlf>> noiseModel() const {
+        gls_raw_nlf r{};
+        std::vector<gls_ycbcr_nlf> y(GLS_MAX_LEVELS);
+        int32_t n = 0;
+        check(gls_converter_noise_model(conv_, &r, y.data(), GLS_MAX_LEVELS, &n));
+        y.resize(size_t(n));
+        return {r, y};
     }
 
     // many frames of any sizes in one call (no reference counterpart); graph
@@ -185,6 +212,14 @@ class PyramidProcessor {
         p.levels = int32_t(levels);
         check(gls_pyramid_denoise_vjp(conv_, &ycc, &gradient, &p, &g_out, flag_if(host_io, GLS_HOST_IO), grad->data(),
                                       g_ycc, stream));
+    }
+
+    // MeasureYCbCrNLF (pyramid_processor.cpp:173-324) on a YCbCr image
+    // (4 ch F32/F16 device memory); synchronous
+    gls_ycbcr_nlf MeasureYCbCrNLF(const ImageView& image, float exposure_multiplier = 1, void* stream = nullptr) {
+        gls_ycbcr_nlf n{};
+        check(gls_measure_ycbcr_nlf(conv_, &image, exposure_multiplier, &n, stream));
+        return n;
     }
 
    private:
@@ -318,6 +353,43 @@ inline std::array<float, 9> FindHomography(SURF& ctx, const std::vector<std::pai
     if (inlier_indices) inlier_indices->assign(inl.begin(), inl.begin() + n);
     return H;
 }
+
+// ---------------------------------------------------------------- files and bursts
+// gls::image<luma_pixel_16>::read_dng_file (pipelineTest.cpp:114-115): the
+// raw samples (row-major, width x height) and the metadata
+inline std::vector<uint16_t> read_dng_file(const std::string& path, gls_dng_info* info) {
+    check(gls_dng_read(path.c_str(), info, nullptr, 0));
+    std::vector<uint16_t> raw(size_t(info->width) * size_t(info->height));
+    check(gls_dng_read(path.c_str(), info, raw.data(), size_t(info->width)));
+    return raw;
+}
+
+// findBursts(parseDirectory(dir)) (pyramidFusion.cpp:36-44, 166-195) over
+// paths in directory order
+inline std::vector<std::vector<std::string>> findBursts(const std::vector<std::string>& paths) {
+    std::vector<const char*> c;
+    for (const auto& p : paths) c.push_back(p.c_str());
+    std::vector<int32_t> of(paths.size());
+    int32_t n = 0;
+    check(gls_find_bursts(c.data(), int32_t(c.size()), of.data(), &n));
+    std::vector<std::vector<std::string>> bursts(size_t(n > 0 ? n : 0));
+    for (size_t i = 0; i < paths.size(); i++)
+        if (of[i] >= 0) bursts[size_t(of[i])].push_back(paths[i]);
+    return bursts;
+}
+
+// saveFusedImage (pyramidFusion.cpp:152-164): 8-bit RGB TIFF
+inline void saveFusedImage(const ImageView& fused, const std::string& path, void* stream = nullptr) {
+    check(gls_write_tiff_rgb8(path.c_str(), &fused, stream));
+}
+
+// convertToGrayscale (demosaic_kernels.hpp:673-688, demosaic.metal:1707-1723)
+struct convertToGrayscale {
+    void operator()(const ImageView& linearImage, ImageView* grayscaleImage, const std::array<float, 3>& transform,
+                    void* stream = nullptr) const {
+        check(gls_convert_to_grayscale(&linearImage, transform.data(), grayscaleImage, stream));
+    }
+};
 
 // ScaleHomography (Homography.hpp:29-37)
 inline std::array<float, 9> ScaleHomography(const std::array<float, 9>& H, float scale) {

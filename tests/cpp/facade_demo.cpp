@@ -1,9 +1,12 @@
 // facade_demo.cpp — exercises include/glscam.hpp the way a caller of the
 // reference's C++ API would: calibration -> RawConverter::demosaic with
-// noise reduction -> SURF on a shifted pair -> FindHomography. Prints
+// noise reduction -> SURF on a shifted pair -> FindHomography; then a DNG
+// file -> parameters from its metadata -> demosaic with post-processing,
+// and findBursts. Prints
 // "facade ok" and exits 0 when every result is sane.
 #include <cmath>
 #include <cstdio>
+#include <string>
 #include <vector>
 
 #include "glscam.hpp"
@@ -80,6 +83,41 @@ int main() {
         range_thrown = true;
     }
     if (!(mean > 0.05 && mean < 1.5) || k1.empty() || !shift_ok || !range_thrown) {
+        std::printf("facade check failed\n");
+        return 1;
+    }
+
+    // the file path: a DNG written and read back, parameters from its
+    // metadata, demosaic with display post-processing into host memory
+    gls_dng_info info{};
+    info.width = W;
+    info.height = H;
+    const uint8_t rggb[4] = {0, 1, 1, 2};
+    for (int c = 0; c < 4; c++) info.cfa_pattern[c] = rggb[c];
+    info.black_level = 512;
+    info.white_level = 4095;
+    info.iso = 400;
+    info.has_color_matrix2 = 1;
+    const float cm[9] = {0.66f, -0.13f, -0.07f, -0.39f, 1.21f, 0.17f, -0.06f, 0.17f, 0.55f};
+    for (int k = 0; k < 9; k++) info.color_matrix2[k] = cm[k];
+    const std::string path = "facade_demo_frame.dng";
+    gls::check(gls_dng_write(path.c_str(), &info, raw.data(), size_t(W), 7, 64));
+    gls_dng_info back{};
+    const std::vector<uint16_t> raw2 = gls::read_dng_file(path, &back);
+    std::remove(path.c_str());
+    gls::iPhone14WideCalibration<5> cal5;
+    gls::DemosaicParameters pd = cal5.getDemosaicParameters(back, xyz);
+    std::vector<float> srgb(size_t(W) * H * 4);
+    gls::ImageView sout{srgb.data(), W, H, 4, GLS_F32, size_t(W) * 16};
+    conv.demosaic(raw2.data(), W, H, size_t(W) * 2, &pd, &sout, /*noiseReduction=*/true, /*fp16=*/true,
+                  /*host_io=*/true, nullptr, /*postProcess=*/true);
+    bool srgb_ok = raw2 == raw && back.iso == 400;
+    for (size_t i = 0; i < srgb.size(); i++) srgb_ok = srgb_ok && srgb[i] >= 0.f && srgb[i] <= 1.f;
+    const auto bursts = gls::findBursts({"d/A_1_x.dng", "d/A_2_x.dng", "d/B.dng", "d/C_1_y.dng"});
+    const bool bursts_ok = bursts.size() == 2 && bursts[0].size() == 2 && bursts[1].size() == 1;
+    std::printf("dng round trip %s, sRGB in range %s, bursts %zu\n", raw2 == raw ? "exact" : "differs",
+                srgb_ok ? "yes" : "no", bursts.size());
+    if (!srgb_ok || !bursts_ok) {
         std::printf("facade check failed\n");
         return 1;
     }
