@@ -212,7 +212,9 @@ _SIGNATURES = {
     "gls_surf_detect_and_compute": (C.c_int, [C.c_void_p, C.POINTER(ImageView), C.c_int32, C.c_uint32, C.c_void_p]),
     "gls_surf_features": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
                                     C.POINTER(C.c_int32), C.c_void_p]),
-    "gls_surf_plane": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(ImageView)]),
+    "gls_surf_load_features": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_uint32,
+                                         C.c_void_p]),
+    "gls_surf_plane":(C.c_int, [C.c_void_p, C.c_int32, C.POINTER(ImageView)]),
     "gls_surf_match": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.POINTER(C.c_int32),
                                  C.c_void_p]),
     "gls_surf_find_homography": (C.c_int, [C.c_void_p, C.c_float, C.c_int32, C.POINTER(C.c_float),

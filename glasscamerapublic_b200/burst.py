@@ -101,13 +101,108 @@ def fuse_burst(converter, paths, out_path=None, fp16: bool = True, stream=None):
     torch.cuda.synchronize()
     surf.close()
     if out_path is None:
-        stem = Path(ref_path).stem
-        base = stem[:stem.find("_4_")] if "_4_" in stem else stem
-        out_dir = Path(ref_path).parent.parent / "Fusion"
-        out_dir.mkdir(parents=True, exist_ok=True)
-        out_path = out_dir / (base + "aRH_fork.tiff")
+        out_path = _fused_path(ref_path)
     write_tiff_rgb8(out_path, fused)
     return fused, Hs, str(out_path)
+
+
+def _fused_path(ref_path) -> Path:
+    """saveFusedImage's name: <name up to "_4_">aRH_fork.tiff in the raw
+    directory's sibling "Fusion"."""
+    stem = Path(ref_path).stem
+    base = stem[:stem.find("_4_")] if "_4_" in stem else stem
+    out_dir = Path(ref_path).parent.parent / "Fusion"
+    out_dir.mkdir(parents=True, exist_ok=True)
+    return out_dir / (base + "aRH_fork.tiff")
+
+
+def fuse_burst_sharded(converter, paths, dist=None, out_path=None, fp16: bool = True, stream=None):
+    """fuse_burst with the burst split over the ranks of a process group
+    (one process per GPU): rank 0 reads the reference frame, takes the
+    demosaic parameters from its metadata and detects its G and G2
+    features, and broadcasts both; member m of [reference, burst[0..2]]
+    belongs to rank m % world, which detects, registers, demosaics and
+    warps it on its own GPU; the homographies are all-gathered and the
+    per-rank running means of the warped frames reduced (sum) to rank 0,
+    which writes the TIFF.
+
+    The result is fuse_burst's: the same homographies bit for bit (each
+    registration is one member against the same reference features), and
+    the mean of the same warped frames summed in another grouping (float
+    rounding). As in fuse_burst, the reference frame's own pixels do not
+    enter the mean (registerAndFuse with count 1 replaces them). Returns
+    (fused RGBA float32 CUDA tensor on rank 0, None elsewhere; homographies
+    [3][3][3]; output path on rank 0, None elsewhere). Without a process
+    group (or world 1) this is one rank doing every member."""
+    import torch
+
+    from . import KEYPOINT_DTYPE, DemosaicParams, shard
+    from .registration import SURF, RegisterAndFuseKernel, register_image
+
+    if len(paths) != 4:
+        raise ValueError("a burst has four frames (pyramidFusion.cpp:286)")
+    active = shard._active(dist)
+    rank, world = (dist.get_rank(), dist.get_world_size()) if active else (0, 1)
+    order = [paths[3]] + list(paths[:3])
+    mine = shard.burst_members(len(order), world)[rank]
+    frames = {m: dng.read_dng(order[m]) for m in mine}
+    dev = torch.device("cuda", torch.cuda.current_device())
+    # parameters and image size from the reference frame's metadata
+    head = None
+    if rank == 0:
+        raw0, info0 = frames[0]
+        head = bytes(dng.demosaic_params(info0)) + np.array(raw0.shape, np.int64).tobytes()
+    head = shard.broadcast_bytes(head, dist)
+    psize = C.sizeof(DemosaicParams)
+    params = DemosaicParams.from_buffer_copy(head[:psize])
+    h, w = (int(v) for v in np.frombuffer(head[psize:], np.int64))
+    surf = SURF(w // 2, h // 2, max_features=1500, nOctaves=4, nOctaveLayers=2, hessianThreshold=0.02)
+    try:
+        planes = {c: torch.empty((h // 2, w // 2), dtype=torch.float32, device=dev) for c in (1, 3)}
+        for m in mine:
+            raw, info = frames[m]
+            if raw.shape != (h, w):
+                raise ValueError(f"{order[m]} is {raw.shape[1]}x{raw.shape[0]}, the reference {w}x{h}")
+            surf.raw_channels(raw, info.bayer_pattern, info.black_level, info.white_level,
+                              float(2.0 ** info.baseline_exposure), outs=planes, stream=stream)
+            surf.detect_slot(planes[1], 2 * m, stream)
+            surf.detect_slot(planes[3], 2 * m + 1, stream)
+        # the reference features: rank 0's slots 0 and 1, broadcast to the others
+        for c in (0, 1):
+            kf, df = surf.features(c, stream) if rank == 0 else (np.zeros(0, KEYPOINT_DTYPE), np.zeros((0, 64)))
+            kb, db = shard.broadcast_features(kf, df, dist)
+            if rank != 0:
+                if kb.is_cuda:
+                    surf.load_features(c, kb, db, stream)
+                else:
+                    surf.load_features(c, kb.numpy().view(KEYPOINT_DTYPE), db.numpy(), stream)
+        members = [m for m in mine if m > 0]
+        Hs = (surf.register_frames([0, 1], [[2 * m, 2 * m + 1] for m in members], 1.0, 2000, True, stream)
+              if members else np.zeros((0, 3, 3), np.float32))
+        Hall = shard.all_gather_rows(Hs.reshape(-1, 9), [m - 1 for m in members], len(order) - 1,
+                                     dist).reshape(-1, 3, 3)
+        # this rank's running mean of its warped members (registerAndFuse
+        # with counts 1, 2, ...; count 1 ignores the fused input)
+        part = torch.zeros((h, w, 4), dtype=torch.float32, device=dev)
+        fuse = RegisterAndFuseKernel()
+        for k, m in enumerate(members):
+            raw, _ = frames[m]
+            rgb = converter.demosaic(torch.from_numpy(raw.view(np.int16)).to(dev), params, fp16=fp16,
+                                     postProcess=True)
+            if k == 0:
+                register_image(rgb, part, Hall[m - 1], stream=stream)
+            else:
+                fuse(part, rgb, part, Hall[m - 1], k + 1, stream=stream)
+        torch.cuda.synchronize()
+        fused = shard.reduce_mean(part, len(members), len(order) - 1, dist)
+    finally:
+        surf.close()
+    if rank != 0:
+        return None, Hall, None
+    if out_path is None:
+        out_path = _fused_path(paths[3])
+    write_tiff_rgb8(out_path, fused)
+    return fused, Hall, str(out_path)
 
 
 def convert_to_grayscale(rgb, transform, out=None, stream=None):

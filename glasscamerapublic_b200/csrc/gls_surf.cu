@@ -1719,6 +1719,32 @@ gls_status gls_surf_features(gls_surf* s, int32_t slot, gls_keypoint* kps, float
     return GLS_OK;
 }
 
+gls_status gls_surf_load_features(gls_surf* s, int32_t slot, const gls_keypoint* kps, const float* desc, int32_t n,
+                                  uint32_t flags, void* stream) {
+    clear_error();
+    GLS_TRY(check_surf(s));
+    if (slot < 0 || slot >= GLS_SURF_SLOTS) return set_error(GLS_ERR_INVALID_ARG, "slot %d out of range", slot);
+    if (n < 0 || n > s->capacity)
+        return set_error(GLS_ERR_INVALID_ARG, "%d features, the detector keeps at most %d", n, s->capacity);
+    if (n > 0 && (!kps || !desc)) return set_error(GLS_ERR_INVALID_ARG, "NULL features");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const cudaMemcpyKind kind = (flags & GLS_HOST_IO) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    SurfSlotState& sl = s->slot[slot];
+    if (n > 0) {
+        GLS_CUDA(cudaMemcpyAsync(sl.kps.p, kps, size_t(n) * sizeof(gls_keypoint), kind, st));
+        GLS_CUDA(cudaMemcpyAsync(sl.desc.p, desc, size_t(n) * 64 * sizeof(float), kind, st));
+    }
+    // the count goes through a pageable host value: the copy has read it
+    // when cudaMemcpyAsync returns, and the stream orders it before any match
+    const int count = n;
+    GLS_CUDA(cudaMemcpyAsync(sl.count.p, &count, sizeof(int), cudaMemcpyHostToDevice, st));
+    if (flags & (GLS_SYNC | GLS_HOST_IO)) GLS_CUDA(cudaStreamSynchronize(st));
+    sl.count_host = n;
+    sl.valid = true;
+    if (s->match_query == slot || s->match_train == slot) s->match_query = s->match_train = -1;
+    return GLS_OK;
+}
+
 gls_status gls_surf_plane(gls_surf* s, int32_t which, gls_image_view* view) {
     clear_error();
     GLS_TRY(check_surf(s));

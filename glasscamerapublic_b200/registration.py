@@ -99,6 +99,22 @@ class SURF:
                                       _stream_handle(stream)))
         return kps[:n.value].copy(), desc[:n.value].copy()
 
+    def load_features(self, slot: int, kps, desc, stream=None) -> int:
+        """Loads keypoints (KEYPOINT_DTYPE records, or their bytes as a
+        uint8 CUDA tensor) and descriptors ([n][64] float32, numpy or CUDA)
+        into a slot, as features() returned them on another detector."""
+        if isinstance(kps, np.ndarray):
+            k = np.ascontiguousarray(kps).view(KEYPOINT_DTYPE)
+            d = np.ascontiguousarray(desc, np.float32).reshape(-1, 64)
+            n, kp, dp, flags = len(k), k.ctypes.data, d.ctypes.data, HOST_IO
+        else:
+            n = kps.numel() // KEYPOINT_DTYPE.itemsize
+            kp, dp, flags = _ptr(kps), _ptr(desc), 0
+        if desc.shape[0] != n:
+            raise ValueError(f"{n} keypoints but {desc.shape[0]} descriptors")
+        check(lib().gls_surf_load_features(self._h, slot, kp, dp, n, flags, _stream_handle(stream)))
+        return slot
+
     def detectAndCompute(self, img, slot: int | None = None, stream=None):
         """SURF::detectAndCompute (SURF.hpp:57-58): keypoints (KEYPOINT_DTYPE
         records) and descriptors ([n][64] float32) on the host."""

@@ -520,6 +520,15 @@ gls_status gls_surf_detect_and_compute(gls_surf* s, const gls_image_view* img, i
 gls_status gls_surf_features(gls_surf* s, int32_t slot, gls_keypoint* kps, float* desc, int32_t capacity, int32_t* n,
                              void* stream);
 
+/* Loads n keypoints and their descriptors ([n][64] floats), as
+ * gls_surf_features returns them, into a feature slot, for matching
+ * against features another detector (another GPU) computed: a burst split
+ * over ranks receives the reference frame's features by broadcast instead
+ * of detecting them again. Device pointers, or host pointers with
+ * GLS_HOST_IO (then synchronous). n <= the detector's max_features. */
+gls_status gls_surf_load_features(gls_surf* s, int32_t slot, const gls_keypoint* kps, const float* desc, int32_t n,
+                                  uint32_t flags, void* stream);
+
 /* Device view of a detector plane: GLS_SURF_PLANE_INTEGRAL is the summed-area
  * table of the last detection, (width+1) x (height+1) F32 with a zero first
  * row and column (integralImageKernel, SURF.cpp:776-825). */

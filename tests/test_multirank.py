@@ -79,3 +79,80 @@ def test_two_gloo_ranks_shard_and_reduce():
 
 def test_mean_gradient_without_a_process_group():
     assert np.allclose(mean_gradient(np.arange(4.0) * 2, 2), np.arange(4.0))
+
+
+def test_burst_members_cover_the_burst():
+    from glasscamerapublic_b200.shard import burst_members
+    for n in (1, 4, 8):
+        for world in (1, 2, 3, 4, 8):
+            parts = burst_members(n, world)
+            assert len(parts) == world and 0 in parts[0]
+            assert sorted(m for p in parts for m in p) == list(range(n))
+    assert burst_members(4, 2) == [[0, 2], [1, 3]]
+    with pytest.raises(ValueError):
+        burst_members(4, 0)
+
+
+def _burst_worker(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+    from glasscamerapublic_b200 import KEYPOINT_DTYPE, shard
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        rng = np.random.default_rng(7)
+        kps = np.zeros(37, KEYPOINT_DTYPE)
+        kps.view(np.float32).reshape(37, -1)[:] = rng.normal(size=(37, KEYPOINT_DTYPE.itemsize // 4))
+        desc = rng.normal(size=(37, 64)).astype(np.float32)
+        # rank 0 holds the features and the header; the others pass nothing
+        kb, db = shard.broadcast_features(kps if rank == 0 else np.zeros(0, KEYPOINT_DTYPE),
+                                          desc if rank == 0 else np.zeros((0, 64), np.float32), dist)
+        head = shard.broadcast_bytes(b"params:" + bytes(range(200)) if rank == 0 else None, dist)
+        empty = shard.broadcast_bytes(b"" if rank == 0 else None, dist)
+        # homographies: member m > 0 of rank m % world fills row m - 1
+        members = [m for m in shard.burst_members(4, world)[rank] if m > 0]
+        rows = np.array([np.full(9, 10.0 * m + 0.5) for m in members], np.float32).reshape(-1, 9)
+        Hall = shard.all_gather_rows(rows, [m - 1 for m in members], 3, dist)
+        # running means of warped members: member m's frame is the constant m
+        part = torch.full((4, 6, 4), float(np.mean(members)) if members else 0.0)
+        mean = shard.reduce_mean(part, len(members), 3, dist)
+        q.put((rank, kb.numpy().tobytes() == kps.tobytes(), np.array_equal(db.numpy(), desc), head, empty,
+               Hall.tolist(), None if mean is None else mean.numpy().tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_split_a_burst(world):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_burst_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    want_H = [[10.0 * m + 0.5] * 9 for m in (1, 2, 3)]
+    for rank, k_ok, d_ok, head, empty, Hall, mean in res:
+        assert k_ok and d_ok
+        assert head == b"params:" + bytes(range(200)) and empty == b""
+        assert Hall == want_H
+        if rank == 0:
+            assert np.allclose(mean, 2.0)  # the mean of members 1, 2, 3
+        else:
+            assert mean is None
+
+
+def test_burst_helpers_without_a_process_group():
+    import torch
+    from glasscamerapublic_b200 import KEYPOINT_DTYPE, shard
+    kps = np.zeros(3, KEYPOINT_DTYPE)
+    kb, db = shard.broadcast_features(kps, np.ones((3, 64), np.float32))
+    assert kb.numel() == 3 * KEYPOINT_DTYPE.itemsize and db.shape == (3, 64)
+    assert shard.broadcast_bytes(b"abc") == b"abc"
+    assert np.array_equal(shard.all_gather_rows(np.ones((2, 9)), [0, 2], 3), [[1] * 9, [0] * 9, [1] * 9])
+    t = torch.ones(2, 2)
+    assert shard.reduce_mean(t, 3, 3) is t
