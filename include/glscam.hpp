@@ -280,6 +280,19 @@ class SURF {
         return slot;
     }
 
+    // Features that another detector computed (another GPU's
+    // detectAndCompute, received by broadcast) into a slot of this one, for
+    // matchKeyPoints; host memory. Returns the slot.
+    int loadFeatures(const std::vector<KeyPoint>& keypoints, const std::vector<float>& descriptors) {
+        if (descriptors.size() != keypoints.size() * 64)
+            throw std::runtime_error("loadFeatures: 64 descriptor floats per keypoint");
+        const int slot = next_;
+        next_ = (next_ + 1) % GLS_SURF_SLOTS;
+        check(gls_surf_load_features(s_, slot, keypoints.data(), descriptors.data(), int32_t(keypoints.size()),
+                                     GLS_HOST_IO, nullptr));
+        return slot;
+    }
+
     // matchKeyPoints (SURF.cpp:931-974) between two detection slots
     std::vector<DMatch> matchKeyPoints(int query_slot, int train_slot, void* stream = nullptr) {
         const int cap = max_features_ >= 0 ? max_features_ : GLS_SURF_MAX_KEYPOINTS;

@@ -71,6 +71,12 @@ int main() {
     const int s1 = surf.detectAndCompute(a.data(), SW, SH, size_t(SW) * 4, &k1, &d1, /*host_input=*/true);
     const int s2 = surf.detectAndCompute(b.data(), SW, SH, size_t(SW) * 4, &k2, &d2, /*host_input=*/true);
     const auto matches = surf.findMatches(s1, k1, s2, k2);
+    // the first frame's features as another GPU would receive them
+    const int s1b = surf.loadFeatures(k1, d1);
+    const auto m_direct = surf.matchKeyPoints(s1, s2), m_loaded = surf.matchKeyPoints(s1b, s2);
+    bool loaded_ok = m_direct.size() == m_loaded.size();
+    for (size_t i = 0; loaded_ok && i < m_direct.size(); i++)
+        loaded_ok = m_direct[i].train_idx == m_loaded[i].train_idx && m_direct[i].distance == m_loaded[i].distance;
     std::vector<int> inliers;
     const auto Hm = gls::FindHomography(surf, matches, 1.0f, 2000, &inliers);
     const bool shift_ok = std::fabs(Hm[2] - 5) < 0.5 && std::fabs(Hm[5] - 3) < 0.5;
@@ -82,7 +88,7 @@ int main() {
     } catch (const std::range_error&) {
         range_thrown = true;
     }
-    if (!(mean > 0.05 && mean < 1.5) || k1.empty() || !shift_ok || !range_thrown) {
+    if (!(mean > 0.05 && mean < 1.5) || k1.empty() || !shift_ok || !range_thrown || !loaded_ok) {
         std::printf("facade check failed\n");
         return 1;
     }
