@@ -189,8 +189,17 @@ __global__ void __launch_bounds__(1024) k_pca_eigen(const double* __restrict__ p
     }
     // block partials summed in block order (deterministic)
     if (t < kPcaAcc) {
+        // eight loads in flight, added in block order
         double v = 0.0;
-        for (int b = 0; b < n_blocks; b++) v += part[b * kPcaAcc + t];
+        int b = 0;
+        for (; b + 8 <= n_blocks; b += 8) {
+            double x[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) x[k] = part[(b + k) * kPcaAcc + t];
+#pragma unroll
+            for (int k = 0; k < 8; k++) v += x[k];
+        }
+        for (; b < n_blocks; b++) v += part[b * kPcaAcc + t];
         acc[t] = v;
     }
     __syncthreads();
@@ -258,10 +267,25 @@ __global__ void __launch_bounds__(1024) k_pca_eigen(const double* __restrict__ p
                 const double apq = A[p][q], app = A[p][p], aqq = A[q][q];
                 double c = 1.0, s = 0.0;
                 if (fabs(apq) >= 1e-300) {
-                    const double theta = (aqq - app) / (2.0 * apq);
-                    const double tt = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-                    c = 1.0 / sqrt(tt * tt + 1.0);
-                    s = tt * c;
+                    // The angle needs only FP32 accuracy: a rotation a little
+                    // off the exact one leaves a_pq at about 1e-7 of its
+                    // value, which later sweeps remove. It has to be
+                    // orthogonal to FP64 precision, which two Newton steps
+                    // for 1 / sqrt(c^2 + s^2) from 1 restore. This keeps the
+                    // FP64 divisions and square roots off the chain.
+                    double r;
+                    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(2.0 * apq));
+                    const float th = float((aqq - app) * r);
+                    const float at = fabsf(th);
+                    float tt = at < 1e18f ? __fdividef(1.f, at + sqrtf(fmaf(at, at, 1.f))) : 0.5f / at;
+                    tt = copysignf(tt, th);
+                    const float c32 = rsqrtf(fmaf(tt, tt, 1.f));
+                    const double cd = c32, sd = double(tt * c32);
+                    const double n2 = cd * cd + sd * sd;
+                    double y = 1.5 - 0.5 * n2;
+                    y = y * (1.5 - 0.5 * n2 * y * y);
+                    c = cd * y;
+                    s = sd * y;
                 }
                 rc[p] = c; rs[p] = s; partner[p] = q; isp[p] = 1;
                 rc[q] = c; rs[q] = s; partner[q] = p; isp[q] = 0;
