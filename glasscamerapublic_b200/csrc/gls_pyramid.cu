@@ -160,36 +160,59 @@ __global__ void __launch_bounds__(352) k_pca_cov(Plane<S, 4> img, double* __rest
 
 // --------------------------------------------------------------------------
 // Symmetric eigen-solve of the 25x25 patch covariance (replaces Eigen's
-// SelfAdjointEigenSolver, PCA.cpp:36): parallel cyclic Jacobi in FP64 on a
-// 26x26 matrix (25 + one zero pad row/column) with the round-robin pair
-// schedule (13 disjoint rotations per round, 25 rounds per sweep). One
-// block of 1024 threads; every sweep is a bounded loop (at most 40 sweeps),
-// so the kernel always ends. The top-8 eigenvectors (descending eigenvalue,
-// each signed so its largest-magnitude entry is positive) are written as a
-// row-major 25x8 FP32 basis. status receives the sweep count, or -1 when
-// the sweep limit was hit before convergence.
-constexpr int EJ_N = 26;
+// SelfAdjointEigenSolver, PCA.cpp:36): one-sided (Hestenes) Jacobi in FP64,
+// one warp. Lane j holds column j of the covariance in registers; a
+// round-robin schedule (25 columns + one empty, 13 disjoint pairs per
+// round, 25 rounds per sweep) pairs the lanes, the partner's column comes
+// by shuffles, and both lanes of a pair form the same rotation from the
+// two columns' Gram entries (alpha, beta, gamma) and rotate their own
+// column. A sweep without a rotation (|gamma| <= 1e-14 sqrt(alpha beta)
+// for every pair) ends the solve; at most 40 sweeps, so the kernel always
+// ends. The covariance C is symmetric positive semi-definite, so the
+// converged columns are C V = Q Lambda: eigenvalue j is the norm of
+// column j and its eigenvector the normalised column. The top-8
+// eigenvectors (descending eigenvalue, each signed so its largest-magnitude
+// entry is positive) are written as a row-major 25x8 FP32 basis. status
+// receives the sweep count, or -1 when the sweep limit was hit.
+constexpr int EJ_THREADS = 352;
 
-__global__ void __launch_bounds__(1024) k_pca_eigen(const double* __restrict__ part, int n_blocks, int n_patches,
-                                                   float* __restrict__ basis, int* status) {
+__device__ __forceinline__ void jacobi_rotation(double app, double aqq, double apq, double& c, double& s) {
+    // The angle needs only FP32 accuracy: a rotation a little off the exact
+    // one leaves gamma at about 1e-7 of its value, which later sweeps
+    // remove. It has to be orthogonal to FP64 precision, which two Newton
+    // steps for 1 / sqrt(c^2 + s^2) from 1 restore.
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(2.0 * apq));
+    const float th = float((aqq - app) * r);
+    const float at = fabsf(th);
+    float tt = at < 1e18f ? __fdividef(1.f, at + sqrtf(fmaf(at, at, 1.f))) : 0.5f / at;
+    tt = copysignf(tt, th);
+    const float c32 = rsqrtf(fmaf(tt, tt, 1.f));
+    const double cd = c32, sd = double(tt * c32);
+    const double n2 = cd * cd + sd * sd;
+    double y = 1.5 - 0.5 * n2;
+    y = y * (1.5 - 0.5 * n2 * y * y);
+    c = cd * y;
+    s = sd * y;
+}
+
+__global__ void __launch_bounds__(EJ_THREADS) k_pca_eigen(const double* __restrict__ part, int n_blocks,
+                                                         int n_patches, float* __restrict__ basis, int* status) {
     __shared__ double acc[kPcaAcc];
-    __shared__ double A[EJ_N][EJ_N + 1], B[EJ_N][EJ_N + 1], V[EJ_N][EJ_N + 1], V2[EJ_N][EJ_N + 1];
-    __shared__ double rc[EJ_N], rs[EJ_N];  // per index: rotation (c, s)
-    __shared__ int partner[EJ_N], isp[EJ_N];
-    __shared__ double red[32];
-    __shared__ int done, order[25];
+    __shared__ double C[25][25];          // covariance
+    __shared__ double U[25][26];          // normalised final columns (column j = lane j)
+    __shared__ double B[25][26];          // eigenvectors, column c = the c-th largest
+    __shared__ double ev_l[25], ev[25], work[200];
+    __shared__ int order[25];
     const int t = threadIdx.x;
-    const int i = t / EJ_N, j = t % EJ_N;
-    const bool act = t < EJ_N * EJ_N;
 
     if (n_patches < 2) {
-        if (t < 25 * 8) basis[t] = ((t / 8) == (t % 8)) ? 1.f : 0.f;
+        for (int k = t; k < 25 * 8; k += blockDim.x) basis[k] = ((k / 8) == (k % 8)) ? 1.f : 0.f;
         if (t == 0 && status) *status = 0;
         return;
     }
-    // block partials summed in block order (deterministic)
+    // block partials summed in block order (deterministic), eight loads in flight
     if (t < kPcaAcc) {
-        // eight loads in flight, added in block order
         double v = 0.0;
         int b = 0;
         for (; b + 8 <= n_blocks; b += 8) {
@@ -204,124 +227,75 @@ __global__ void __launch_bounds__(1024) k_pca_eigen(const double* __restrict__ p
     }
     __syncthreads();
     // covariance from raw moments
-    if (act) {
-        double v = 0.0;
-        if (i < 25 && j < 25) {
-            const int r = min(i, j), c = max(i, j);
-            const int idx = r * 25 - r * (r - 1) / 2 + (c - r);  // upper-triangle index (row-major)
-            const double n = double(n_patches);
-            const double mi = acc[325 + i] / n, mj = acc[325 + j] / n;
-            v = (acc[idx] - n * mi * mj) / (n - 1.0);
-        }
-        A[i][j] = v;
-        V[i][j] = (i == j) ? 1.0 : 0.0;
+    for (int k = t; k < 625; k += blockDim.x) {
+        const int i = k / 25, j = k % 25;
+        const int r = min(i, j), c = max(i, j);
+        const int idx = r * 25 - r * (r - 1) / 2 + (c - r);  // upper-triangle index (row-major)
+        const double n = double(n_patches);
+        const double mi = acc[325 + i] / n, mj = acc[325 + j] / n;
+        C[i][j] = (acc[idx] - n * mi * mj) / (n - 1.0);
     }
-    if (t == 0) done = 0;
     __syncthreads();
-
+    if (t >= 32) return;  // one warp solves
+    const int lane = t;
+    double a[25];
+#pragma unroll
+    for (int r = 0; r < 25; r++) a[r] = lane < 25 ? C[r][lane] : 0.0;
     int sweep = 0;
     for (; sweep < 40; sweep++) {
-        // convergence test: off-diagonal vs total Frobenius mass
-        double off = 0.0, tot = 0.0;
-        if (act) {
-            const double a = A[i][j];
-            tot = a * a;
-            off = (i != j) ? a * a : 0.0;
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            off += __shfl_down_sync(0xffffffffu, off, o);
-            tot += __shfl_down_sync(0xffffffffu, tot, o);
-        }
-        __shared__ double red2[32];
-        if ((t & 31) == 0) {
-            red[t >> 5] = off;
-            red2[t >> 5] = tot;
-        }
-        __syncthreads();
-        if (t == 0) {
-            double so = 0, st = 0;
-            for (int k = 0; k < 32; k++) {
-                so += red[k];
-                st += red2[k];
-            }
-            done = (so <= 1e-26 * st || so == 0.0) ? 1 : 0;  // off-diagonal norm <= 1e-13 x total
-        }
-        __syncthreads();
-        if (done) break;
+        bool rotated = false;
+#pragma unroll 1
         for (int round = 0; round < 25; round++) {
-            // pairs of this round: (25, round) and ((round+m)%25, (round-m+25)%25), m = 1..12
-            if (t < 13) {
-                int p, q;
-                if (t == 0) {
-                    p = round;
-                    q = 25;
-                } else {
-                    p = (round + t) % 25;
-                    q = (round - t + 25) % 25;
-                }
-                if (p > q) {
-                    const int tmp = p;
-                    p = q;
-                    q = tmp;
-                }
-                const double apq = A[p][q], app = A[p][p], aqq = A[q][q];
-                double c = 1.0, s = 0.0;
-                if (fabs(apq) >= 1e-300) {
-                    // The angle needs only FP32 accuracy: a rotation a little
-                    // off the exact one leaves a_pq at about 1e-7 of its
-                    // value, which later sweeps remove. It has to be
-                    // orthogonal to FP64 precision, which two Newton steps
-                    // for 1 / sqrt(c^2 + s^2) from 1 restore. This keeps the
-                    // FP64 divisions and square roots off the chain.
-                    double r;
-                    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(2.0 * apq));
-                    const float th = float((aqq - app) * r);
-                    const float at = fabsf(th);
-                    float tt = at < 1e18f ? __fdividef(1.f, at + sqrtf(fmaf(at, at, 1.f))) : 0.5f / at;
-                    tt = copysignf(tt, th);
-                    const float c32 = rsqrtf(fmaf(tt, tt, 1.f));
-                    const double cd = c32, sd = double(tt * c32);
-                    const double n2 = cd * cd + sd * sd;
-                    double y = 1.5 - 0.5 * n2;
-                    y = y * (1.5 - 0.5 * n2 * y * y);
-                    c = cd * y;
-                    s = sd * y;
-                }
-                rc[p] = c; rs[p] = s; partner[p] = q; isp[p] = 1;
-                rc[q] = c; rs[q] = s; partner[q] = p; isp[q] = 0;
+            // pairs of this round: (round, 25) and the lanes whose indices sum to 2 round (mod 25)
+            int partner = lane;
+            if (lane < 25) partner = lane == round ? 25 : (2 * round - lane + 50) % 25;
+            else if (lane == 25) partner = round;
+            double b[25];
+#pragma unroll
+            for (int r = 0; r < 25; r++) b[r] = __shfl_sync(0xffffffffu, a[r], partner);
+            // Gram entries, two partial sums each (the same order in both lanes of a pair)
+            double al0 = 0, al1 = 0, be0 = 0, be1 = 0, ga0 = 0, ga1 = 0;
+#pragma unroll
+            for (int r = 0; r < 24; r += 2) {
+                al0 = fma(a[r], a[r], al0);
+                be0 = fma(b[r], b[r], be0);
+                ga0 = fma(a[r], b[r], ga0);
+                al1 = fma(a[r + 1], a[r + 1], al1);
+                be1 = fma(b[r + 1], b[r + 1], be1);
+                ga1 = fma(a[r + 1], b[r + 1], ga1);
             }
-            __syncthreads();
-            // columns: B = A J, V2 = V J
-            if (act) {
-                const int pj = partner[j];
-                const double c = rc[j], s = rs[j];
-                if (isp[j]) {
-                    B[i][j] = c * A[i][j] - s * A[i][pj];
-                    V2[i][j] = c * V[i][j] - s * V[i][pj];
-                } else {
-                    B[i][j] = s * A[i][pj] + c * A[i][j];
-                    V2[i][j] = s * V[i][pj] + c * V[i][j];
-                }
+            const double al = fma(a[24], a[24], al0 + al1), be = fma(b[24], b[24], be0 + be1);
+            const double ga = fma(a[24], b[24], ga0 + ga1);
+            const bool low = lane < partner;
+            if (partner < 25 && lane < 25 && partner != lane && ga * ga > 1e-28 * al * be && fabs(ga) >= 1e-300) {
+                double c, s;
+                jacobi_rotation(low ? al : be, low ? be : al, ga, c, s);
+                rotated = true;
+                // the lower index p: c a_p - s a_q; the higher q: s a_p + c a_q
+#pragma unroll
+                for (int r = 0; r < 25; r++) a[r] = low ? fma(c, a[r], -s * b[r]) : fma(s, b[r], c * a[r]);
             }
-            __syncthreads();
-            // rows: A = J^T B
-            if (act) {
-                const int pi = partner[i];
-                const double c = rc[i], s = rs[i];
-                if (isp[i]) A[i][j] = c * B[i][j] - s * B[pi][j];
-                else A[i][j] = s * B[pi][j] + c * B[i][j];
-                V[i][j] = V2[i][j];
-            }
-            __syncthreads();
         }
+        if (!__any_sync(0xffffffffu, rotated)) break;
     }
+    if (lane < 25) {
+        double nn = 0.0;
+#pragma unroll
+        for (int r = 0; r < 25; r++) nn = fma(a[r], a[r], nn);
+        const double e = sqrt(nn);
+        const double inv = e > 0.0 ? 1.0 / e : 0.0;
+        ev_l[lane] = e;
+#pragma unroll
+        for (int r = 0; r < 25; r++) U[r][lane] = a[r] * inv;
+    }
+    __syncwarp();
     // order eigenvalues descending (stable by index)
-    if (t == 0) {
+    if (lane == 0) {
         for (int k = 0; k < 25; k++) order[k] = k;
         for (int k = 1; k < 25; k++) {  // insertion sort, stable
             const int e = order[k];
             int m = k - 1;
-            while (m >= 0 && A[order[m]][order[m]] < A[e][e]) {
+            while (m >= 0 && ev_l[order[m]] < ev_l[e]) {
                 order[m + 1] = order[m];
                 m--;
             }
@@ -329,13 +303,11 @@ __global__ void __launch_bounds__(1024) k_pca_eigen(const double* __restrict__ p
         }
         if (status) *status = sweep < 40 ? sweep : -1;
     }
-    __syncthreads();
-    // sorted eigenpairs into B (column c = c-th largest), then the top-8 basis
-    __shared__ double ev[25], work[200];
-    if (t < 25) ev[t] = A[order[t]][order[t]];
-    if (t < 625) B[t / 25][t % 25] = V[t / 25][order[t % 25]];
-    __syncthreads();
-    if (t == 0) select_pca_basis(ev, &B[0][0], EJ_N + 1, work, basis);
+    __syncwarp();
+    if (lane < 25) ev[lane] = ev_l[order[lane]];
+    for (int k = lane; k < 625; k += 32) B[k / 25][k % 25] = U[k / 25][order[k % 25]];
+    __syncwarp();
+    if (lane == 0) select_pca_basis(ev, &B[0][0], 26, work, basis);
 }
 
 // --------------------------------------------------------------------------
@@ -432,7 +404,7 @@ template void launch_pca_cov_rows<float>(Plane<float, 4>, double*, int, cudaStre
 template void launch_pca_cov_rows<__half>(Plane<__half, 4>, double*, int, cudaStream_t);
 
 void launch_pca_eigen(const double* part, int n_blocks, int n_patches, float* basis, int* status, cudaStream_t s) {
-    k_pca_eigen<<<1, 1024, 0, s>>>(part, n_blocks, n_patches, basis, status);
+    k_pca_eigen<<<1, EJ_THREADS, 0, s>>>(part, n_blocks, n_patches, basis, status);
 }
 
 template <class S>
