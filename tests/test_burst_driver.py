@@ -83,3 +83,10 @@ def test_grayscale_formula_is_the_reference_kernel():
     gray = np.zeros((24, 40), np.float32)
     L.ref_convert_to_grayscale(rgb.ctypes.data_as(fp), 40, 24, t.ctypes.data_as(fp), gray.ctypes.data_as(fp))
     assert np.array_equal(gray, _gray_formula(rgb, t))
+
+
+def test_burst_drivers_want_four_frames():
+    from glasscamerapublic_b200 import burst
+    for fn in (burst.fuse_burst, burst.fuse_burst_sharded):
+        with pytest.raises(ValueError):
+            fn(None, ["a.dng", "b.dng", "c.dng"])
