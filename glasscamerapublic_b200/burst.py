@@ -116,7 +116,7 @@ def _fused_path(ref_path) -> Path:
     return out_dir / (base + "aRH_fork.tiff")
 
 
-def fuse_burst_sharded(converter, paths, dist=None, out_path=None, fp16: bool = True, stream=None):
+def fuse_burst_sharded(converter, paths, dist=None, out_path=None, fp16: bool = True, stream=None, device=None):
     """fuse_burst with the burst split over the ranks of a process group
     (one process per GPU): rank 0 reads the reference frame, takes the
     demosaic parameters from its metadata and detects its G and G2
@@ -133,7 +133,8 @@ def fuse_burst_sharded(converter, paths, dist=None, out_path=None, fp16: bool = 
     enter the mean (registerAndFuse with count 1 replaces them). Returns
     (fused RGBA float32 CUDA tensor on rank 0, None elsewhere; homographies
     [3][3][3]; output path on rank 0, None elsewhere). Without a process
-    group (or world 1) this is one rank doing every member."""
+    group (or world 1) this is one rank doing every member. device: where
+    the frames live (default the current CUDA device)."""
     import torch
 
     from . import KEYPOINT_DTYPE, DemosaicParams, shard
@@ -146,7 +147,7 @@ def fuse_burst_sharded(converter, paths, dist=None, out_path=None, fp16: bool = 
     order = [paths[3]] + list(paths[:3])
     mine = shard.burst_members(len(order), world)[rank]
     frames = {m: dng.read_dng(order[m]) for m in mine}
-    dev = torch.device("cuda", torch.cuda.current_device())
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
     # parameters and image size from the reference frame's metadata
     head = None
     if rank == 0:
@@ -193,7 +194,8 @@ def fuse_burst_sharded(converter, paths, dist=None, out_path=None, fp16: bool = 
                 register_image(rgb, part, Hall[m - 1], stream=stream)
             else:
                 fuse(part, rgb, part, Hall[m - 1], k + 1, stream=stream)
-        torch.cuda.synchronize()
+        if dev.type == "cuda":
+            torch.cuda.synchronize()
         fused = shard.reduce_mean(part, len(members), len(order) - 1, dist)
     finally:
         surf.close()

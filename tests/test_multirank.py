@@ -156,3 +156,100 @@ def test_burst_helpers_without_a_process_group():
     assert np.array_equal(shard.all_gather_rows(np.ones((2, 9)), [0, 2], 3), [[1] * 9, [0] * 9, [1] * 9])
     t = torch.ones(2, 2)
     assert shard.reduce_mean(t, 3, 3) is t
+
+
+def _fake_burst_rank(rank, world, port, q):
+    """fuse_burst_sharded's orchestration with the detector, the warps, the
+    DNG reader and the converter replaced by CPU fakes whose outputs encode
+    which frame (and which broadcast reference) they came from."""
+    import types
+    import torch
+    import torch.distributed as dist
+    import glasscamerapublic_b200 as g
+    from glasscamerapublic_b200 import KEYPOINT_DTYPE, burst, dng, registration
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        def read_dng(path):
+            m = int(str(path)[1:])
+            info = types.SimpleNamespace(bayer_pattern=2, black_level=0, white_level=4095, baseline_exposure=0.0)
+            return np.full((8, 12), 100 * m + 7, np.uint16), info
+
+        class FakeSURF:
+            def __init__(self, w, h, **kw):
+                self.slots = {}
+
+            def raw_channels(self, raw, pattern, black, white, exposure, outs=None, stream=None):
+                outs[1].fill_(float(raw[0, 0]))
+                outs[3].fill_(float(raw[0, 0]) + 0.5)
+
+            def detect_slot(self, plane, slot, stream=None):
+                v = float(plane[0, 0])
+                k = np.zeros(3, KEYPOINT_DTYPE)
+                k["x"] = v
+                self.slots[slot] = (k, np.full((3, 64), v, np.float32))
+
+            def features(self, slot, stream=None):
+                return self.slots[slot]
+
+            def load_features(self, slot, kps, desc, stream=None):
+                self.slots[slot] = (np.array(kps).copy(), np.array(desc).copy())
+
+            def register_frames(self, ref_slots, frame_slots, *a):
+                out = []
+                for f0, f1 in frame_slots:
+                    H = np.eye(3, dtype=np.float32)
+                    H[0, 2] = self.slots[f0][1][0, 0] - self.slots[ref_slots[0]][1][0, 0]
+                    H[1, 2] = self.slots[f1][0]["x"][0] - self.slots[ref_slots[1]][0]["x"][0]
+                    out.append(H)
+                return np.array(out, np.float32).reshape(-1, 3, 3)
+
+            def close(self):
+                pass
+
+        def fuse(fused, inp, out, H, count, stream=None):
+            out.copy_(((count - 1) * fused + inp + float(H[0][2])) / count)
+
+        def register_image(inp, out, H, stream=None):
+            out.copy_(inp + float(H[0][2]))
+
+        conv = types.SimpleNamespace(
+            demosaic=lambda raw, p, fp16=True, postProcess=True: torch.full(
+                (raw.shape[0], raw.shape[1], 4), float(raw[0, 0])))
+        dng.read_dng = read_dng
+        dng.demosaic_params = lambda info: g.DemosaicParams()
+        registration.SURF = FakeSURF
+        registration.RegisterAndFuseKernel = lambda: fuse
+        registration.register_image = register_image
+        written = []
+        burst.write_tiff_rgb8 = lambda path, rgba, stream=None: written.append(str(path))
+        fused, Hall, out = burst.fuse_burst_sharded(conv, ["f1", "f2", "f3", "f0"], dist, out_path="fused.tiff",
+                                                    device="cpu")
+        q.put((rank, Hall.tolist(), None if fused is None else fused.numpy().tolist(), out, written))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [1, 2, 5])
+def test_burst_split_orchestration_with_more_ranks_than_frames(world):
+    # world 5 > 4 frames: rank 4 holds nothing and rank 0 only the
+    # reference, yet every rank takes the same collective steps
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_fake_burst_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=180) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    want_H = [[[1.0, 0.0, 100.0 * m], [0.0, 1.0, 100.0 * m], [0.0, 0.0, 1.0]] for m in (1, 2, 3)]
+    for rank, Hall, fused, out, written in res:
+        assert Hall == want_H, rank
+        if rank == 0:
+            # member m's frame is 100 m + 7, warped by + 100 m: the mean of 207, 407, 607
+            assert np.allclose(fused, 407.0) and out == "fused.tiff" and written == ["fused.tiff"]
+        else:
+            assert fused is None and out is None and written == []
