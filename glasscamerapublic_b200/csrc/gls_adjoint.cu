@@ -600,13 +600,8 @@ void launch_adj_head(const float* den0, const float* target, int tstride, int w,
 }
 
 void launch_bm_bwd(const AdjointLevelArgs& a, cudaStream_t s) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_bm_bwd_center, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(CenterSmem)));
-        cudaFuncSetAttribute(k_bm_bwd_neighbor, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(sizeof(NeighborSmem)));
-        attr = true;
-    }
+    ensure_dynamic_smem(reinterpret_cast<const void*>(k_bm_bwd_center), int(sizeof(CenterSmem)));
+    ensure_dynamic_smem(reinterpret_cast<const void*>(k_bm_bwd_neighbor), int(sizeof(NeighborSmem)));
     const dim3 b(AT_X, AT_Y), g((a.w + AT_X - 1) / AT_X, (a.h + AT_Y - 1) / AT_Y);
     k_bm_bwd_center<<<g, b, sizeof(CenterSmem), s>>>(a);
     k_bm_bwd_neighbor<<<g, b, sizeof(NeighborSmem), s>>>(a);

@@ -462,11 +462,7 @@ template <int TY>
 static void launch_pair(Plane<__half, 4> img, Plane<__half, 2> grad, const float* basis, Plane<__half, 4> out,
                         const BlockMatchArgs& a, cudaStream_t s) {
     const size_t smem = sizeof(BmPairSmem<TY>) + sizeof(__half) * BX_LW * BxTile<TY>::LH;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_block_match_pair<TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        attr = true;
-    }
+    ensure_dynamic_smem(reinterpret_cast<const void*>(k_block_match_pair<TY>), int(smem));
     dim3 b(BX_TX, TY);
     dim3 g((img.w + BX_TX - 1) / BX_TX, (img.h + BX_NP * TY - 1) / (BX_NP * TY));
     k_block_match_pair<TY><<<g, b, smem, s>>>(img, grad, basis, out, a);
@@ -541,12 +537,7 @@ void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, cons
         if (ty == 8) launch_pair<8>(img, grad, basis, out, a, s);
         else if (ty == 4) launch_pair<4>(img, grad, basis, out, a, s);
     } else {
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(k_block_match_plain<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(sizeof(BmPlainSmem)));
-            attr = true;
-        }
+        ensure_dynamic_smem(reinterpret_cast<const void*>(k_block_match_plain<S>), int(sizeof(BmPlainSmem)));
         dim3 b(BP_TX, BP_TY);
         dim3 g((img.w + BP_TX - 1) / BP_TX, (img.h + 2 * BP_TY - 1) / (2 * BP_TY));
         k_block_match_plain<S><<<g, b, sizeof(BmPlainSmem), s>>>(img, grad, pca, out, a);

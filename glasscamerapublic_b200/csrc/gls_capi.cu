@@ -7,7 +7,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
+#include <set>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "gls_common.cuh"
@@ -30,6 +33,19 @@ gls_status set_error(gls_status code, const char* fmt, ...) {
     return code;
 }
 void clear_error() { g_last_error.clear(); }
+
+cudaError_t ensure_dynamic_smem(const void* func, int bytes) {
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.count({func, dev})) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) done.insert({func, dev});
+    return e;
+}
 
 template <class S, int C>
 static Plane<S, C> plane(DevBuf& b, int w, int h) {

@@ -496,11 +496,7 @@ void launch_raw_denoise(Plane<S, 1> bayer, Plane<S, 2> grad, Plane<S, 4> quad, c
 
 template <class S>
 void launch_demosaic(Plane<S, 1> raw, Plane<S, 2> grad, Plane<S, 4> out, const DemosaicArgs& a, cudaStream_t s) {
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_demosaic<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(DemosaicSmem)));
-        attr_set = true;
-    }
+    ensure_dynamic_smem(reinterpret_cast<const void*>(k_demosaic<S>), int(sizeof(DemosaicSmem)));
     dim3 b(32, 8);
     dim3 g((raw.w + DM_TW - 1) / DM_TW, (raw.h + DM_TH - 1) / DM_TH);
     k_demosaic<S><<<g, b, sizeof(DemosaicSmem), s>>>(raw, grad, out, a);

@@ -12,6 +12,13 @@ struct gls_raw_nlf;
 
 namespace gls {
 
+// Raise `func`'s dynamic shared-memory limit to `bytes` on the current
+// device. The attribute belongs to the device's context, so it is set once
+// per (kernel, device) pair; the record of pairs done is guarded by a
+// mutex, so converters on several host threads and devices may launch
+// concurrently. Returns the CUDA error of the first, failed setting.
+cudaError_t ensure_dynamic_smem(const void* func, int bytes);
+
 constexpr int kMaxTaps = 32;
 
 struct ScaleArgs {

@@ -8,6 +8,7 @@
 
 #include "gls_common.cuh"
 #include "gls_kernels.h"
+#include "gls_pca_pairs.h"
 
 namespace gls {
 
@@ -120,8 +121,8 @@ __global__ void __launch_bounds__(256) k_subtract_noise(Plane<S, 4> in, Plane<S,
 // entry of sum p p^T and thread 325 + r the sum of component r, in FP64.
 // Each block writes its partial sums to its own row of `part`; the rows are
 // summed in block order afterwards, so the result does not depend on
-// scheduling (no atomics).
-__constant__ uint8_t kPairR[325], kPairC[325];
+// scheduling (no atomics). A thread finds its (r, c) from its index
+// (pca_pair), so the kernel needs no table loaded per device.
 
 constexpr int PC_CHUNK = 64;
 
@@ -133,9 +134,8 @@ __global__ void __launch_bounds__(352) k_pca_cov(Plane<S, 4> img, double* __rest
     const int t = threadIdx.x;
     double sum = 0.0;
     int r = 0, c = 0;
-    if (t < 325) {
-        r = kPairR[t];
-        c = kPairC[t];
+    if (t < kPcaTri) {
+        pca_pair(t, r, c);
     } else if (t < 350) {
         r = t - 325;
     }
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(EJ_THREADS) k_pca_eigen(const double* __restri
     for (int k = t; k < 625; k += blockDim.x) {
         const int i = k / 25, j = k % 25;
         const int r = min(i, j), c = max(i, j);
-        const int idx = r * 25 - r * (r - 1) / 2 + (c - r);  // upper-triangle index (row-major)
+        const int idx = pca_tri_index(r, c);
         const double n = double(n_patches);
         const double mi = acc[325 + i] / n, mj = acc[325 + j] / n;
         C[i][j] = (acc[idx] - n * mi * mj) / (n - 1.0);
@@ -367,21 +367,6 @@ void launch_subtract_noise(Plane<S, 4> in, Plane<S, 4> coarse, Plane<S, 4> coars
                                                           float(coarse.w) / float(in.w), float(coarse.h) / float(in.h));
 }
 
-static void init_pairs() {
-    static bool done = false;
-    if (done) return;
-    uint8_t r[325], c[325];
-    int k = 0;
-    for (int i = 0; i < 25; i++)
-        for (int j = i; j < 25; j++, k++) {
-            r[k] = uint8_t(i);
-            c[k] = uint8_t(j);
-        }
-    cudaMemcpyToSymbol(kPairR, r, sizeof(r));
-    cudaMemcpyToSymbol(kPairC, c, sizeof(c));
-    done = true;
-}
-
 int pca_cov_blocks(int w, int h) {
     const int n = (w / 8) * (h / 8);
     return n <= 0 ? 0 : std::max(1, std::min(kPcaMaxBlocks, (n + PC_CHUNK - 1) / PC_CHUNK));
@@ -389,7 +374,6 @@ int pca_cov_blocks(int w, int h) {
 
 template <class S>
 void launch_pca_cov(Plane<S, 4> img, double* part, cudaStream_t s) {
-    init_pairs();
     const int blocks = pca_cov_blocks(img.w, img.h);
     if (blocks == 0) return;
     k_pca_cov<S><<<blocks, 352, 0, s>>>(img, part);
@@ -397,7 +381,6 @@ void launch_pca_cov(Plane<S, 4> img, double* part, cudaStream_t s) {
 
 template <class S>
 void launch_pca_cov_rows(Plane<S, 4> img, double* part, int rows, cudaStream_t s) {
-    init_pairs();
     if (rows > 0) k_pca_cov<S><<<rows, 352, 0, s>>>(img, part);
 }
 template void launch_pca_cov_rows<float>(Plane<float, 4>, double*, int, cudaStream_t);
@@ -431,7 +414,7 @@ void host_pca_basis(const double* part, int n_blocks, int n_patches, float* basi
     for (int i = 0; i < 25; i++)
         for (int j = 0; j < 25; j++) {
             const int r = std::min(i, j), c = std::max(i, j);
-            const int idx = r * 25 - r * (r - 1) / 2 + (c - r);
+            const int idx = pca_tri_index(r, c);
             A[i][j] = (acc[idx] - n * (acc[325 + i] / n) * (acc[325 + j] / n)) / (n - 1.0);
             V[i][j] = i == j ? 1.0 : 0.0;
         }

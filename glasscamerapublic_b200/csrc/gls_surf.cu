@@ -182,6 +182,9 @@ __device__ __forceinline__ float det3(const float a[3], const float b[3], const 
 
 constexpr int DT_X = 32, DT_Y = 8;  // NMS positions per detector tile
 
+// A feature slot's count, set from a host value (gls_surf_load_features).
+__global__ void k_store_count(int* count, int n) { *count = n; }
+
 // calcDetAndTrace for the four layers of an octave over a tile plus a
 // one-sample halo, into shared memory; then findMaximaInLayer
 // (SURF.metal:249-313) with interpolateKeypoint (:207-247) for the two
@@ -1734,10 +1737,10 @@ gls_status gls_surf_load_features(gls_surf* s, int32_t slot, const gls_keypoint*
         GLS_CUDA(cudaMemcpyAsync(sl.kps.p, kps, size_t(n) * sizeof(gls_keypoint), kind, st));
         GLS_CUDA(cudaMemcpyAsync(sl.desc.p, desc, size_t(n) * 64 * sizeof(float), kind, st));
     }
-    // the count goes through a pageable host value: the copy has read it
-    // when cudaMemcpyAsync returns, and the stream orders it before any match
-    const int count = n;
-    GLS_CUDA(cudaMemcpyAsync(sl.count.p, &count, sizeof(int), cudaMemcpyHostToDevice, st));
+    // the count is written by a kernel on the stream (no host buffer has to
+    // outlive the call, and the write can be recorded in a graph)
+    k_store_count<<<1, 1, 0, st>>>(static_cast<int*>(sl.count.p), n);
+    GLS_TRY(launch_check(s, "store_count"));
     if (flags & (GLS_SYNC | GLS_HOST_IO)) GLS_CUDA(cudaStreamSynchronize(st));
     sl.count_host = n;
     sl.valid = true;
