@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-full-frame", action="store_true", help="reference arm: skip the one whole-frame check")
     ap.add_argument("--workload", default=WORKLOAD, help="workload name (cfg2_4032x3024 or cfg1_1024x768)")
     ap.add_argument("--quick", action="store_true", help="timed FP16 loop only (for profiler captures)")
     ap.add_argument("--no-burst", action="store_true", help="skip the burst registration + fusion leg")
@@ -119,44 +120,90 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline(wl, params_fn, seconds: float):
-    """The reference's path on all host cores, over a bounded sample: a
-    1008x756 frame of the same scene recipe and 5-level schedule (1/16 of
-    the 12 MP area), repeated for about `seconds`; frames/s scaled to 12 MP
-    by the pixel-count ratio. It runs the reference's own Metal kernels
-    compiled for the CPU (oracle/_ref, kind "reference") where they were
-    built, else the oracle's FP32 restatement (kind "port")."""
+TILES = 4  # the CPU baseline's sample: one of the 4 x 4 full-resolution tiles of a frame
+
+
+def cpu_frame_setup(wl):
+    """The reference's path on the host cores, set up on one full frame of
+    the workload: (run_tile(i), kind, what, threads, tile size). run_tile(i)
+    converts tile i of the frame's TILES x TILES full-resolution tiles
+    (1008x756 of 4032x3024) with the same scene, noise, ISO and 5-level
+    schedule, so TILES^2 tiles are the frame's pixel work. It runs the
+    reference's own Metal kernels compiled for the CPU with the parameters
+    of the reference's own iPhone14WideCalibration (oracle/_ref, kind
+    "reference") where they were built, else the oracle's FP32 restatement
+    (kind "port"). Nothing of the library under test is loaded on the
+    reference path."""
     sys.path.insert(0, str(ROOT / "tests"))
     import _oracle as O
     import _ref as R
     from glasscamerapublic_b200 import scene
-    sw, sh = wl.width // 4, wl.height // 4
-    swl = scene.Workload("cpu_sample", sw, sh, levels=wl.levels, black=wl.black, white=wl.white, gain=wl.gain,
-                         read=wl.read, iso=wl.iso, seed=wl.seed)
-    raw, _ = scene.make_raw(swl)
-    p = params_fn(swl)
+    raw, _ = scene.make_raw(wl)
     threads = os.cpu_count() or 1
+    tw, th = wl.width // TILES, wl.height // TILES
+    tiles = [np.ascontiguousarray(raw[j * th:(j + 1) * th, i * tw:(i + 1) * tw])
+             for j in range(TILES) for i in range(TILES)]
     if R.available():
-        kind, what = "reference", "reference Metal kernels compiled for the CPU"
+        kind, what = "reference", "reference Metal kernels and iPhone14WideCalibration compiled for the CPU"
+        p = scene.make_params(wl, calibration=R.iPhone14WideCalibration(levels=wl.levels))
         R.lib().ref_set_threads(threads)
-        run = lambda: R.raw_pipeline(raw, p, denoise=True)
+        run_tile = lambda i: R.raw_pipeline(tiles[i % len(tiles)], p, denoise=True)
+        run_frame = lambda: R.raw_pipeline(raw, p, denoise=True)
     else:
         kind, what = "port", "FP32 oracle"
+        p = scene.make_params(wl)
         O.lib().orc_set_threads(threads)
-        run = lambda: O.raw_pipeline(raw, p, denoise=True, f64=False)
+        run_tile = lambda i: O.raw_pipeline(tiles[i % len(tiles)], p, denoise=True, f64=False)
+        run_frame = lambda: O.raw_pipeline(raw, p, denoise=True, f64=False)
+    return run_tile, run_frame, kind, what, threads, (tw, th)
+
+
+def cpu_baseline(wl, seconds: float):
+    """The reference's path on all host cores over a bounded sample of the
+    workload: consecutive full-resolution tiles of one 12 MP frame
+    (cpu_frame_setup) for about `seconds`; frames/s = tiles/s / TILES^2."""
+    run_tile, _, kind, what, threads, (tw, th) = cpu_frame_setup(wl)
+    run_tile(0)  # first-touch of the harness's buffers, untimed
     t0 = time.perf_counter()
     n = 0
     while True:
-        run()
+        run_tile(n)
         n += 1
         if time.perf_counter() - t0 >= seconds:
             break
     dt = time.perf_counter() - t0
-    fps_sample = n / dt
-    scale = (sw * sh) / (wl.width * wl.height)
-    return {"value": fps_sample * scale, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{n} x {sw}x{sh} frame(s), 5 levels, {what}, {dt:.1f}s; frames/s scaled by area x{scale:.4f}",
+    return {"value": n / dt / (TILES * TILES), "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{n} consecutive {tw}x{th} full-resolution tiles (1/{TILES * TILES} each) of a "
+                      f"{wl.width}x{wl.height} frame, 5 levels, {what}, {dt:.1f}s; frames/s = tiles/s / "
+                      f"{TILES * TILES}",
             "registration": cpu_registration_baseline(threads)}
+
+
+def fp64_check_leg(wl, raw, clean, out16, out32):
+    """The error of one frame's outputs against the FP64 oracle (the
+    checker, run on the host cores outside every timed region): PSNR
+    against the FP64 output, the PSNR delta against the clean scene
+    (PSNR(out, clean) - PSNR(FP64, clean)) and the max |diff|, for the
+    FP16-storage batched path (what `value` times) and the FP32 plain path."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import _oracle as O
+    from glasscamerapublic_b200 import scene
+    O.lib().orc_set_threads(os.cpu_count() or 1)
+    p = scene.make_params(wl)
+    t0 = time.perf_counter()
+    ref = O.raw_pipeline(raw, p, denoise=True, f64=True)["out"][..., :3].astype(np.float64)
+    dt = time.perf_counter() - t0
+    tgt = scene.target_rgb(clean)
+    ps_ref = scene.psnr(ref, tgt)
+
+    def err(out):
+        o = np.asarray(out[..., :3], np.float64)
+        return {"psnr_db": scene.psnr(o, ref), "delta_psnr_db": scene.psnr(o, tgt) - ps_ref,
+                "max_abs": float(np.abs(o - ref).max()), "psnr_vs_clean_db": scene.psnr(o, tgt)}
+
+    return {"fp16_batched": err(out16), "fp32_plain": err(out32), "fp64_psnr_vs_clean_db": ps_ref,
+            "gate_delta_psnr_db": 0.05, "frame": f"{wl.width}x{wl.height}, {wl.levels} levels, ISO {wl.iso}",
+            "oracle_seconds": dt}
 
 
 def cpu_registration_baseline(threads: int):
@@ -451,6 +498,23 @@ def mixed_leg(args, rank, local, conv, stream):
         e1.record(stream)
         stream.synchronize()
         ms_stream = e0.elapsed_time(e1) / reps
+        # strong scaling: the one 16-frame batch split over the ranks by
+        # pixel count (shard.assign_frames); this rank's share as its own graph
+        from glasscamerapublic_b200.shard import assign_frames
+        world = dist_env()[1]
+        mine = assign_frames([(wl.width, wl.height) for wl in wls], world)[rank]
+        sub = ([raws[i] for i in mine], [params[i] for i in mine], [outs[i] for i in mine])
+        ms_share = 0.0
+        if mine:
+            for _ in range(2):
+                conv.demosaic_batch(*sub, stream=stream, graph=True)
+            stream.synchronize()
+            e0.record(stream)
+            for _ in range(reps):
+                conv.demosaic_batch(*sub, stream=stream, graph=True)
+            e1.record(stream)
+            stream.synchronize()
+            ms_share = e0.elapsed_time(e1) / reps
     return {
         "workload": "16 frames: 4 x 4032x3024, 4 x 6000x4000, 4 x 5472x3648, 4 x 8368x5584, RGGB, 12/14-bit, "
                     "demosaic + 5-level denoise, FP16 storage",
@@ -460,6 +524,9 @@ def mixed_leg(args, rank, local, conv, stream):
         "ms_per_batch_graph": ms_graph,
         "ms_per_batch_stream_launched": ms_stream,
         "gpu_launches_per_batch": per_batch,
+        "strong": {"frames_this_rank": mine, "ms_share": ms_share,
+                   "note": "the one batch split over the ranks by pixel count (longest-processing-time); "
+                           "value = batch MP / the slowest rank's share time"},
         "block_match_tile_heights": [list(t) for t in block_match_tiles()],
         "note": "one CUDA graph replay per batch; frames spread largest-first over 3 slot streams; "
                 "block_match_tile_heights: autotuned (width, height, thread rows: 8 = 32x32 px tiles, 4 = 32x16)",
@@ -696,30 +763,55 @@ def dng_leg(args, rank, local, conv, stream):
 
 
 def run_reference(args, rank):
-    """The reference arm: the reference's path on the host cores. The Metal
-    runtime cannot run here; the reference's own kernel source, compiled
-    for the CPU (oracle/_ref), stands in for it, else the oracle port."""
+    """The reference arm: the reference's path on the host cores, rank 0
+    only. The Metal runtime cannot run here; the reference's own kernel
+    source and camera calibration, compiled for the CPU (oracle/_ref),
+    stand in for it, else the oracle port. A step is one full-resolution
+    tile (1/16) of the 12 MP frame, the tiles taken in turn, so every 16
+    steps cover one whole frame; frames/s = 1 / (16 x time per step). After
+    the timed steps one whole 4032x3024 frame is converted once, untimed by
+    the step clock, to check that 16 tiles take the time of a frame."""
     if rank != 0:
         return
     from glasscamerapublic_b200 import scene
     wl = scene.WORKLOADS[WORKLOAD]
+    run_tile, run_frame, kind, what, threads, (tw, th) = cpu_frame_setup(wl)
+    for i in range(args.warmup):
+        run_tile(i)
     times = []
-    vals = []
-    for i in range(args.warmup + args.steps):
-        r = cpu_baseline(wl, scene.make_params, seconds=max(2.0, args.cpu_seconds / max(1, args.steps)))
-        if i >= args.warmup:
-            vals.append(r["value"])
-        last = r
-    v = float(np.median(vals)) if vals else last["value"]
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        run_tile(args.warmup + i)
+        times.append(time.perf_counter() - t0)
+    ms_step = 1e3 * sum(times) / len(times)
+    v = 1e3 / (ms_step * TILES * TILES)
+    full = None
+    if not args.no_full_frame:
+        t0 = time.perf_counter()
+        run_frame()
+        full = time.perf_counter() - t0
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f16/f32 (the reference's half/float kernels)",
-            "data": "synthetic",
-            "config": {"workload": WORKLOAD, "frame": "4032x3024 RGGB 12-bit", "levels": 5},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": last["cores"], "kind": last["kind"],
-                             "sample": last["sample"]},
+            "data": "synthetic", "config": main_config(wl, args.gpus),
+            "step": f"one {tw}x{th} full-resolution tile (1/{TILES * TILES}) of the {wl.width}x{wl.height} frame "
+                    f"through the reference's demosaic + 5-level pyramid denoise; tiles in turn",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": f"{args.steps} timed tiles of {tw}x{th}, {what}"},
+            "full_frame": None if full is None else {
+                "seconds": full, "frames_per_s": 1.0 / full,
+                "tiles_equivalent_s": ms_step * TILES * TILES / 1e3,
+                "note": "one whole 4032x3024 frame through the same code, timed once after the steps"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def main_config(wl, world):
+    """The workload description shared by both arms' lines."""
+    return {"workload": wl.name, "frame": f"{wl.width}x{wl.height} RGGB 12-bit", "levels": wl.levels,
+            "iso": wl.iso, "frames_per_step": N_ROTATE,
+            "l2": "each step reads 6 distinct frames; inputs + planes >> 126 MB L2",
+            "parallelism": f"frames sharded over {world} rank(s), {N_ROTATE}-frame batch per rank on 3 streams"}
 
 
 def main():
@@ -763,7 +855,10 @@ def main():
     B = N_ROTATE  # frames per step (one batch)
 
     # resident inputs: distinct frames per rank (weak scaling)
-    raws_host = [scene.make_raw(wl, frame=rank * B + f)[0] for f in range(B)]
+    made = [scene.make_raw(wl, frame=rank * B + f) for f in range(B)]
+    raws_host = [m[0] for m in made]
+    clean0 = made[0][1]
+    del made
     raws = [torch.from_numpy(r.view(np.int16)).to(f"cuda:{local}") for r in raws_host]
     outs = [torch.empty((H, W, 4), dtype=torch.float16, device=f"cuda:{local}") for _ in range(B)]
     plist = [params] * B
@@ -884,9 +979,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f16-storage/f32-math", "data": "synthetic",
-        "config": {"workload": args.workload, "frame": f"{W}x{H} RGGB 12-bit", "levels": wl.levels, "iso": wl.iso,
-                   "frames_per_step": B, "l2": "each step reads 6 distinct frames; inputs + planes >> 126 MB L2",
-                   "parallelism": f"frames sharded over {world} rank(s), {B}-frame batch per rank on 3 streams"},
+        "config": main_config(wl, world),
         "e2e": {"value": world * B / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": B * W * H * 2,
                 "d2h_bytes_per_step": B * W * H * 8,
                 "stream_launched_value": world * B / (e2e_stream_ms / 1e3),
@@ -915,6 +1008,10 @@ def main():
         mx = mixed_leg(args, rank, local, conv, stream)
         (mx["ms_per_batch_graph"],) = max_over_ranks([mx["ms_per_batch_graph"]], dist if world > 1 else None)
         mx["value"] = world * mx["megapixels_per_batch"] / (mx["ms_per_batch_graph"] / 1e3)
+        mx["scaling"] = "weak: every rank converts the whole batch"
+        (mx["strong"]["ms_share"],) = max_over_ranks([mx["strong"]["ms_share"]], dist if world > 1 else None)
+        mx["strong"]["value"] = mx["megapixels_per_batch"] / (mx["strong"]["ms_share"] / 1e3)
+        mx["strong"]["unit"] = "MP/s"
         line["mixed_batch"] = mx
     if not args.no_post:
         pp = post_leg(args, rank, local, conv, stream)
@@ -937,7 +1034,13 @@ def main():
         (a["ms_per_batch"],) = max_over_ranks([a["ms_per_batch"]], dist if world > 1 else None)
         line["adjoint"] = a
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(wl, scene.make_params, args.cpu_seconds)
+        # one frame's error against the FP64 oracle, through the same calls
+        # as the timed paths (batched FP16, plain FP32 with host PCA)
+        o16 = np.empty((H, W, 4), np.float16)
+        conv.demosaic_batch([raws_host[0]], [params], [o16], fp16=True, out_fp16=True, sync=True)
+        o32 = conv.demosaic(raws_host[0], params, noiseReduction=True, fp16=False, host_pca=True)
+        line["error_vs_fp64"] = fp64_check_leg(wl, raws_host[0], clean0, o16.astype(np.float32), o32)
+        line["cpu_baseline"] = cpu_baseline(wl, args.cpu_seconds)
     if rank == 0:
         print(json.dumps(line), flush=True)
     conv.close()

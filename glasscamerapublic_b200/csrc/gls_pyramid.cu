@@ -160,154 +160,323 @@ __global__ void __launch_bounds__(352) k_pca_cov(Plane<S, 4> img, double* __rest
 
 // --------------------------------------------------------------------------
 // Symmetric eigen-solve of the 25x25 patch covariance (replaces Eigen's
-// SelfAdjointEigenSolver, PCA.cpp:36): one-sided (Hestenes) Jacobi in FP64,
-// one warp. Lane j holds column j of the covariance in registers; a
-// round-robin schedule (25 columns + one empty, 13 disjoint pairs per
-// round, 25 rounds per sweep) pairs the lanes, the partner's column comes
-// by shuffles, and both lanes of a pair form the same rotation from the
-// two columns' Gram entries (alpha, beta, gamma) and rotate their own
-// column. A sweep without a rotation (|gamma| <= 1e-14 sqrt(alpha beta)
-// for every pair) ends the solve; at most 40 sweeps, so the kernel always
-// ends. The covariance C is symmetric positive semi-definite, so the
-// converged columns are C V = Q Lambda: eigenvalue j is the norm of
-// column j and its eigenvector the normalised column. The top-8
-// eigenvectors (descending eigenvalue, each signed so its largest-magnitude
-// entry is positive) are written as a row-major 25x8 FP32 basis. status
-// receives the sweep count, or -1 when the sweep limit was hit.
-constexpr int EJ_THREADS = 352;
+// SelfAdjointEigenSolver, PCA.cpp:36), FP64, one block. Only the 8 largest
+// eigenpairs are needed, so the solve is the tridiagonal route of Golub &
+// Van Loan (Matrix Computations, 4th ed.): section 8.3.1 and the
+// bisection / inverse-iteration methods of sections 8.4.1 and 8.2.2
+// (the tred2 / tridiagonal bisection / tinvit sequence of EISPACK):
+//   1. Householder tridiagonalisation, A = Q T Q^T, Q = H_0 ... H_22: 23
+//      reflector steps, each a warp-reduced column norm, the product
+//      p = beta A v (one warp per row), and the rank-2 update of the
+//      trailing block by all threads (matrix in shared memory);
+//   2. the 8 largest eigenvalues of T by Sturm-sequence multisection:
+//      warp w brackets eigenvalue 24 - w (ascending order); its 32 lanes
+//      count the eigenvalues below 32 points of the bracket, which shrinks
+//      33-fold per round (11 rounds reach FP64 resolution);
+//   3. each eigenvector of T by inverse iteration: the tridiagonal
+//      T - lambda I is factored once with partial pivoting (lane 0 of the
+//      eigenvalue's warp) and solved three times from a start vector of its
+//      own; tiny pivots are raised to eps ||T|| so the solve stays finite;
+//   4. the back-transform z = H_0 (H_1 (... H_22 y)) by the warp, one
+//      reflector at a time, and modified Gram-Schmidt of the 8 vectors in
+//      eigenvalue order (exactly equal eigenvalues give an orthonormal basis
+//      of their eigenspace; distinct ones are already orthogonal).
+// The top-8 eigenvectors (descending eigenvalue, each signed so its
+// largest-magnitude entry is positive; eigenvalues <= 1e-9 of the largest
+// completed as in select_pca_basis) are written as a row-major 25x8 FP32
+// basis. Every reduction has a fixed order, so the result is deterministic.
+// status receives the number of inverse-iteration solves per vector (3), or
+// -1 when a vector came out non-finite (the basis is then still written).
+constexpr int EJ_THREADS = 704;  // 22 warps: two partial sums per accumulator in the prologue
+constexpr int EJ_N = 25, EJ_TOP = 8, EJ_INV_ITERS = 3, EJ_MSEC_ROUNDS = 11;
 
-__device__ __forceinline__ void jacobi_rotation(double app, double aqq, double apq, double& c, double& s) {
-    // The angle needs only FP32 accuracy: a rotation a little off the exact
-    // one leaves gamma at about 1e-7 of its value, which later sweeps
-    // remove. It has to be orthogonal to FP64 precision, which two Newton
-    // steps for 1 / sqrt(c^2 + s^2) from 1 restore.
+// 1 / x to FP64 accuracy: the hardware approximation refined by two
+// Newton-Raphson steps r <- r + r (1 - x r), each doubling the correct bits.
+__device__ __forceinline__ double rcp_nr(double x) {
     double r;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(2.0 * apq));
-    const float th = float((aqq - app) * r);
-    const float at = fabsf(th);
-    float tt = at < 1e18f ? __fdividef(1.f, at + sqrtf(fmaf(at, at, 1.f))) : 0.5f / at;
-    tt = copysignf(tt, th);
-    const float c32 = rsqrtf(fmaf(tt, tt, 1.f));
-    const double cd = c32, sd = double(tt * c32);
-    const double n2 = cd * cd + sd * sd;
-    double y = 1.5 - 0.5 * n2;
-    y = y * (1.5 - 0.5 * n2 * y * y);
-    c = cd * y;
-    s = sd * y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
 }
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Number of eigenvalues of the symmetric tridiagonal (d, e) below x: the
+// signs of the pivots of T - x I (Sturm sequence); a pivot smaller than
+// pivmin in magnitude is replaced by -pivmin.
+__device__ __forceinline__ int sturm_count(const double* d, const double* ee, double x, double pivmin) {
+    double q = d[0] - x;
+    if (fabs(q) < pivmin) q = -pivmin;
+    int cnt = q < 0.0;
+#pragma unroll 8
+    for (int i = 1; i < EJ_N; i++) {
+        q = fma(-ee[i - 1], rcp_nr(q), d[i] - x);
+        if (fabs(q) < pivmin) q = -pivmin;
+        cnt += q < 0.0;
+    }
+    return cnt;
+}
+
+struct EigenSmem {
+    double acc[kPcaAcc];
+    double A[EJ_N][EJ_N + 1];       // covariance, reduced in place
+    double V[EJ_N - 2][EJ_N];       // Householder vectors (zero above k + 1)
+    double beta[EJ_N - 2];
+    double d[EJ_N], e[EJ_N], ee[EJ_N];
+    double p[EJ_N], w[EJ_N];
+    double lam[EJ_TOP];
+    // inverse iteration, per eigenvector: the pivoted LU of T - lambda I
+    double u0[EJ_TOP][EJ_N], u1[EJ_TOP][EJ_N], u2[EJ_TOP][EJ_N], l[EJ_TOP][EJ_N], ru0[EJ_TOP][EJ_N];
+    double y[EJ_TOP][EJ_N];
+    unsigned char piv[EJ_TOP][EJ_N];
+    double Z[EJ_N][EJ_TOP + 1];     // eigenvectors of A, column c = the c-th largest
+    double work[200];
+    double part2[kPcaAcc];
+    int bad;
+};
 
 __global__ void __launch_bounds__(EJ_THREADS) k_pca_eigen(const double* __restrict__ part, int n_blocks,
                                                          int n_patches, float* __restrict__ basis, int* status) {
-    __shared__ double acc[kPcaAcc];
-    __shared__ double C[25][25];          // covariance
-    __shared__ double U[25][26];          // normalised final columns (column j = lane j)
-    __shared__ double B[25][26];          // eigenvectors, column c = the c-th largest
-    __shared__ double ev_l[25], ev[25], work[200];
-    __shared__ int order[25];
-    const int t = threadIdx.x;
+    __shared__ EigenSmem sm;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
 
     if (n_patches < 2) {
         for (int k = t; k < 25 * 8; k += blockDim.x) basis[k] = ((k / 8) == (k % 8)) ? 1.f : 0.f;
         if (t == 0 && status) *status = 0;
         return;
     }
-    // block partials summed in block order (deterministic), eight loads in flight
-    if (t < kPcaAcc) {
+    // ---- block partials summed in a fixed order: two halves of the block
+    //      range per accumulator, eight loads in flight each, then added
+    {
+        const int h = t / kPcaAcc, a = t % kPcaAcc;  // h: 0 or 1 (t < 700)
+        const int half = (n_blocks + 1) / 2;
+        const int b0 = h == 0 ? 0 : half, b1 = h == 0 ? half : n_blocks;
         double v = 0.0;
-        int b = 0;
-        for (; b + 8 <= n_blocks; b += 8) {
-            double x[8];
+        if (t < 2 * kPcaAcc) {
+            int b = b0;
+            for (; b + 8 <= b1; b += 8) {
+                double x[8];
 #pragma unroll
-            for (int k = 0; k < 8; k++) x[k] = part[(b + k) * kPcaAcc + t];
+                for (int k = 0; k < 8; k++) x[k] = part[(b + k) * kPcaAcc + a];
 #pragma unroll
-            for (int k = 0; k < 8; k++) v += x[k];
+                for (int k = 0; k < 8; k++) v += x[k];
+            }
+            for (; b < b1; b++) v += part[b * kPcaAcc + a];
+            if (h == 1) sm.part2[a] = v;
         }
-        for (; b < n_blocks; b++) v += part[b * kPcaAcc + t];
-        acc[t] = v;
+        if (t == 0) sm.bad = 0;
+        __syncthreads();
+        if (t < kPcaAcc) sm.acc[t] = v + sm.part2[t];
     }
     __syncthreads();
-    // covariance from raw moments
-    for (int k = t; k < 625; k += blockDim.x) {
-        const int i = k / 25, j = k % 25;
-        const int r = min(i, j), c = max(i, j);
-        const int idx = pca_tri_index(r, c);
+    // ---- covariance from raw moments, (sum pp^T - n m m^T) / (n - 1)
+    for (int k = t; k < EJ_N * EJ_N; k += blockDim.x) {
+        const int i = k / EJ_N, j = k % EJ_N;
+        const int idx = pca_tri_index(min(i, j), max(i, j));
         const double n = double(n_patches);
-        const double mi = acc[325 + i] / n, mj = acc[325 + j] / n;
-        C[i][j] = (acc[idx] - n * mi * mj) / (n - 1.0);
+        const double mi = sm.acc[325 + i] / n, mj = sm.acc[325 + j] / n;
+        sm.A[i][j] = (sm.acc[idx] - n * mi * mj) / (n - 1.0);
     }
     __syncthreads();
-    if (t >= 32) return;  // one warp solves
-    const int lane = t;
-    double a[25];
-#pragma unroll
-    for (int r = 0; r < 25; r++) a[r] = lane < 25 ? C[r][lane] : 0.0;
-    int sweep = 0;
-    for (; sweep < 40; sweep++) {
-        bool rotated = false;
-#pragma unroll 1
-        for (int round = 0; round < 25; round++) {
-            // pairs of this round: (round, 25) and the lanes whose indices sum to 2 round (mod 25)
-            int partner = lane;
-            if (lane < 25) partner = lane == round ? 25 : (2 * round - lane + 50) % 25;
-            else if (lane == 25) partner = round;
-            double b[25];
-#pragma unroll
-            for (int r = 0; r < 25; r++) b[r] = __shfl_sync(0xffffffffu, a[r], partner);
-            // Gram entries, two partial sums each (the same order in both lanes of a pair)
-            double al0 = 0, al1 = 0, be0 = 0, be1 = 0, ga0 = 0, ga1 = 0;
-#pragma unroll
-            for (int r = 0; r < 24; r += 2) {
-                al0 = fma(a[r], a[r], al0);
-                be0 = fma(b[r], b[r], be0);
-                ga0 = fma(a[r], b[r], ga0);
-                al1 = fma(a[r + 1], a[r + 1], al1);
-                be1 = fma(b[r + 1], b[r + 1], be1);
-                ga1 = fma(a[r + 1], b[r + 1], ga1);
-            }
-            const double al = fma(a[24], a[24], al0 + al1), be = fma(b[24], b[24], be0 + be1);
-            const double ga = fma(a[24], b[24], ga0 + ga1);
-            const bool low = lane < partner;
-            if (partner < 25 && lane < 25 && partner != lane && ga * ga > 1e-28 * al * be && fabs(ga) >= 1e-300) {
-                double c, s;
-                jacobi_rotation(low ? al : be, low ? be : al, ga, c, s);
-                rotated = true;
-                // the lower index p: c a_p - s a_q; the higher q: s a_p + c a_q
-#pragma unroll
-                for (int r = 0; r < 25; r++) a[r] = low ? fma(c, a[r], -s * b[r]) : fma(s, b[r], c * a[r]);
+
+    // ---- 1. Householder tridiagonalisation
+    for (int k = 0; k < EJ_N - 2; k++) {
+        if (warp == 0) {
+            // v from column k below the diagonal: x = A[k+1..][k]
+            const double x = (lane > k && lane < EJ_N) ? sm.A[lane][k] : 0.0;
+            const double nrm2 = warp_sum(x * x);
+            const double x1 = __shfl_sync(0xffffffffu, x, k + 1);
+            const double nrm = sqrt(nrm2);
+            const double alpha = x1 >= 0.0 ? -nrm : nrm;
+            const double den = nrm2 - alpha * x1;  // v.v / 2 > 0 unless the column is zero
+            const bool skip = !(nrm2 > 1e-280);
+            const double v = skip ? 0.0 : (lane == k + 1 ? x1 - alpha : x);
+            if (lane < EJ_N) sm.V[k][lane] = v;
+            if (lane == 0) {
+                sm.beta[k] = skip ? 0.0 : 1.0 / den;
+                sm.d[k] = sm.A[k][k];
+                sm.e[k] = skip ? x1 : alpha;
             }
         }
-        if (!__any_sync(0xffffffffu, rotated)) break;
-    }
-    if (lane < 25) {
-        double nn = 0.0;
-#pragma unroll
-        for (int r = 0; r < 25; r++) nn = fma(a[r], a[r], nn);
-        const double e = sqrt(nn);
-        const double inv = e > 0.0 ? 1.0 / e : 0.0;
-        ev_l[lane] = e;
-#pragma unroll
-        for (int r = 0; r < 25; r++) U[r][lane] = a[r] * inv;
-    }
-    __syncwarp();
-    // order eigenvalues descending (stable by index)
-    if (lane == 0) {
-        for (int k = 0; k < 25; k++) order[k] = k;
-        for (int k = 1; k < 25; k++) {  // insertion sort, stable
-            const int e = order[k];
-            int m = k - 1;
-            while (m >= 0 && ev_l[order[m]] < ev_l[e]) {
-                order[m + 1] = order[m];
-                m--;
-            }
-            order[m + 1] = e;
+        __syncthreads();
+        const double beta = sm.beta[k];
+        if (beta == 0.0) continue;  // uniform: the column is already reduced
+        // p = beta A' v, one warp per row j > k
+        for (int j = k + 1 + warp; j < EJ_N; j += EJ_THREADS / 32) {
+            const double pr = warp_sum(lane < EJ_N ? sm.A[j][lane] * sm.V[k][lane] : 0.0);
+            if (lane == 0) sm.p[j] = beta * pr;
         }
-        if (status) *status = sweep < 40 ? sweep : -1;
+        __syncthreads();
+        if (warp == 0) {  // w = p - (beta/2)(p.v) v
+            const double vj = lane > k && lane < EJ_N ? sm.V[k][lane] : 0.0;
+            const double pj = lane > k && lane < EJ_N ? sm.p[lane] : 0.0;
+            const double pv = warp_sum(pj * vj);
+            if (lane > k && lane < EJ_N) sm.w[lane] = pj - 0.5 * beta * pv * vj;
+        }
+        __syncthreads();
+        // A' -= v w^T + w v^T on the trailing block
+        const int m = EJ_N - k - 1;
+        for (int q = t; q < m * m; q += blockDim.x) {
+            const int i = k + 1 + q / m, j = k + 1 + q % m;
+            sm.A[i][j] -= sm.V[k][i] * sm.w[j] + sm.w[i] * sm.V[k][j];
+        }
+        __syncthreads();
     }
-    __syncwarp();
-    if (lane < 25) ev[lane] = ev_l[order[lane]];
-    for (int k = lane; k < 625; k += 32) B[k / 25][k % 25] = U[k / 25][order[k % 25]];
-    __syncwarp();
-    if (lane == 0) select_pca_basis(ev, &B[0][0], 26, work, basis);
+    if (t == 0) {
+        sm.d[EJ_N - 2] = sm.A[EJ_N - 2][EJ_N - 2];
+        sm.d[EJ_N - 1] = sm.A[EJ_N - 1][EJ_N - 1];
+        sm.e[EJ_N - 2] = sm.A[EJ_N - 1][EJ_N - 2];
+        sm.e[EJ_N - 1] = 0.0;
+    }
+    __syncthreads();
+    if (t < EJ_N) sm.ee[t] = sm.e[t] * sm.e[t];
+    __syncthreads();
+
+    // ---- 2. the 8 largest eigenvalues by Sturm multisection, warp w for
+    //         eigenvalue index 24 - w (ascending)
+    double tnorm = 0.0, lo = 0.0, hi = 0.0;
+    {
+        double a = 0.0, b = 0.0, s = 0.0;
+        if (lane < EJ_N) {
+            const double r = fabs(sm.e[lane]) + (lane > 0 ? fabs(sm.e[lane - 1]) : 0.0);
+            a = sm.d[lane] - r;
+            b = sm.d[lane] + r;
+            s = fabs(sm.d[lane]) + r;
+        } else {
+            a = b = sm.d[0];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a = fmin(a, __shfl_xor_sync(0xffffffffu, a, o));
+            b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+            s = fmax(s, __shfl_xor_sync(0xffffffffu, s, o));
+        }
+        tnorm = s;
+        const double pad = 2.2e-16 * fmax(tnorm, 1e-300) * EJ_N;
+        lo = a - pad;
+        hi = b + pad;
+    }
+    const double pivmin = fmax(1e-290, 1e-290 * tnorm * tnorm);
+    if (warp < EJ_TOP) {
+        const int m = EJ_N - 1 - warp;
+        for (int r = 0; r < EJ_MSEC_ROUNDS; r++) {
+            if (!(hi - lo > 4.4e-16 * fmax(fabs(lo), fabs(hi)) + pivmin)) break;  // warp-uniform
+            const double x = lo + (hi - lo) * (double(lane + 1) / 33.0);
+            const int c = sturm_count(sm.d, sm.ee, x, pivmin);
+            const unsigned above = __ballot_sync(0xffffffffu, c > m);
+            const int first = above ? __ffs(above) - 1 : 32;
+            const double xl = __shfl_sync(0xffffffffu, x, max(first - 1, 0));
+            const double xh = __shfl_sync(0xffffffffu, x, min(first, 31));
+            if (first > 0) lo = xl;
+            if (first < 32) hi = xh;
+        }
+        if (lane == 0) sm.lam[warp] = 0.5 * (lo + hi);
+    }
+    __syncthreads();
+
+    // ---- 3. inverse iteration on T for eigenvector `warp` (lane 0)
+    if (warp < EJ_TOP && lane == 0) {
+        const int c = warp;
+        const double lam = sm.lam[c];
+        const double tiny = fmax(2.2e-16 * tnorm, 1e-290);
+        // factor T - lam I = P L U (Gaussian elimination, partial pivoting);
+        // U has the diagonal u0 and two super-diagonals u1, u2
+        double a = sm.d[0] - lam, b = sm.e[0];
+        for (int k = 0; k < EJ_N - 1; k++) {
+            const double cl = sm.e[k];                 // sub-diagonal entry of row k + 1
+            const double an = sm.d[k + 1] - lam;       // diagonal of row k + 1
+            const double bn = k + 1 < EJ_N - 1 ? sm.e[k + 1] : 0.0;
+            if (fabs(a) >= fabs(cl)) {                 // no interchange
+                double piv = a;
+                if (fabs(piv) < tiny) piv = piv < 0.0 ? -tiny : tiny;
+                const double rp = rcp_nr(piv);
+                const double mult = cl * rp;
+                sm.u0[c][k] = piv; sm.ru0[c][k] = rp; sm.u1[c][k] = b; sm.u2[c][k] = 0.0;
+                sm.l[c][k] = mult; sm.piv[c][k] = 0;
+                a = an - mult * b;
+                b = bn;
+            } else {                                   // rows k and k + 1 interchanged
+                const double pc = fabs(cl) < tiny ? (cl < 0.0 ? -tiny : tiny) : cl;
+                const double rp = rcp_nr(pc);
+                const double mult = a * rp;
+                sm.u0[c][k] = pc; sm.ru0[c][k] = rp; sm.u1[c][k] = an; sm.u2[c][k] = bn;
+                sm.l[c][k] = mult; sm.piv[c][k] = 1;
+                a = b - mult * an;
+                b = -mult * bn;
+            }
+        }
+        double piv = a;
+        if (fabs(piv) < tiny) piv = piv < 0.0 ? -tiny : tiny;
+        sm.u0[c][EJ_N - 1] = piv;
+        sm.ru0[c][EJ_N - 1] = rcp_nr(piv);
+        sm.u1[c][EJ_N - 1] = sm.u2[c][EJ_N - 1] = 0.0;
+        // start vector of its own per eigenvector (deterministic)
+        double* y = sm.y[c];
+        for (int i = 0; i < EJ_N; i++) y[i] = 1.0 + 0.25 * double(((i + 1) * (7 + 4 * c)) % 13) / 13.0;
+        for (int it = 0; it < EJ_INV_ITERS; it++) {
+            for (int k = 0; k < EJ_N - 1; k++) {       // apply P and L^-1
+                if (sm.piv[c][k]) {
+                    const double tmp = y[k];
+                    y[k] = y[k + 1];
+                    y[k + 1] = tmp - sm.l[c][k] * y[k];
+                } else {
+                    y[k + 1] -= sm.l[c][k] * y[k];
+                }
+            }
+            for (int k = EJ_N - 1; k >= 0; k--) {      // U^-1
+                double s = y[k];
+                if (k + 1 < EJ_N) s -= sm.u1[c][k] * y[k + 1];
+                if (k + 2 < EJ_N) s -= sm.u2[c][k] * y[k + 2];
+                y[k] = s * sm.ru0[c][k];
+            }
+            double mx = 0.0;                            // rescale by the largest entry
+            for (int i = 0; i < EJ_N; i++) mx = fmax(mx, fabs(y[i]));
+            const double inv = mx > 0.0 && mx < 1e300 ? 1.0 / mx : 0.0;
+            for (int i = 0; i < EJ_N; i++) y[i] *= inv;
+        }
+    }
+    __syncthreads();
+    // ---- 4. back-transform by the reflectors (warp c, lane = row), then
+    //         modified Gram-Schmidt in eigenvalue order (warp 0)
+    if (warp < EJ_TOP) {
+        const int c = warp;
+        double z = lane < EJ_N ? sm.y[c][lane] : 0.0;
+        for (int k = EJ_N - 3; k >= 0; k--) {
+            const double vk = lane < EJ_N ? sm.V[k][lane] : 0.0;
+            const double dot = warp_sum(vk * z);
+            z -= sm.beta[k] * dot * vk;
+        }
+        if (lane < EJ_N) sm.Z[lane][c] = z;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        for (int c = 0; c < EJ_TOP; c++) {
+            double z = lane < EJ_N ? sm.Z[lane][c] : 0.0;
+            for (int pass = 0; pass < 2; pass++)
+                for (int k = 0; k < c; k++) {
+                    const double zk = lane < EJ_N ? sm.Z[lane][k] : 0.0;
+                    z -= warp_sum(zk * z) * zk;
+                }
+            const double nn = warp_sum(z * z);
+            const bool ok = nn > 0.0 && nn < 1e300;
+            z = ok ? z * (1.0 / sqrt(nn)) : 0.0;
+            if (!ok && lane == 0) sm.bad = 1;
+            if (lane < EJ_N) sm.Z[lane][c] = z;
+            __syncwarp();
+        }
+        if (lane == 0) {
+            double ev[EJ_TOP];
+            for (int c = 0; c < EJ_TOP; c++) ev[c] = sm.lam[c];
+            select_pca_basis(ev, &sm.Z[0][0], EJ_TOP + 1, sm.work, basis);
+            if (status) *status = sm.bad ? -1 : EJ_INV_ITERS;
+        }
+    }
 }
 
 // --------------------------------------------------------------------------

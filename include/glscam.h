@@ -277,11 +277,10 @@ gls_status gls_converter_pca_basis(gls_converter* conv, int32_t level, float* ba
  * each device looks up the scratch array's device address; make that first
  * call before any stream capture. All calls share the one array: calls
  * whose GPU work overlaps (different streams, or different host threads)
- * race on it and must be serialised by the caller. The eigen-solve's
- * convergence is not reported: it stops after at most 40 Jacobi sweeps and
- * writes the basis it holds then (the converter path reports a solve that
- * hit the limit; on covariances of image patches the solve converges in
- * about 13 sweeps). */
+ * race on it and must be serialised by the caller. The eigen-solve runs a
+ * fixed number of steps and always writes a basis; it has no status word
+ * here (a non-finite eigenvector, which no finite covariance produces, is
+ * not reported). */
 gls_status gls_pca_basis_noalloc(const gls_image_view* image, float* basis25x8, void* stream);
 
 /* ---- launch accounting (no reference counterpart; the reference prints

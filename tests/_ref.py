@@ -36,6 +36,8 @@ def lib() -> C.CDLL:
         L.ref_pyramid_denoise.argtypes = [fp, fp, C.c_int, C.c_int, P, fp, fp, dp]
         L.ref_raw_pipeline.argtypes = [C.c_void_p, C.c_int, C.c_int, P, C.c_int, fp]
         L.ref_set_threads.argtypes = [C.c_int]
+        L.ref_calibration_fill.argtypes = [C.c_int, P]
+        L.ref_calibration_fill.restype = C.c_int
         L.ref_noise_tables.argtypes = [C.c_uint, C.POINTER(C.c_int32), fp]
         L.ref_postprocess.argtypes = [fp, fp, fp, C.c_int, C.c_int, P, C.c_uint, fp, fp]
         L.ref_demosaic_post.argtypes = [C.c_void_p, C.c_int, C.c_int, P, C.c_int, fp, fp]
@@ -193,3 +195,21 @@ def measure_ycc_nlf(stats, exposure=1.0):
     b = np.zeros(3, np.float32)
     lib().ref_measure_ycc_nlf(_fp(st), w, h, exposure, _fp(a), _fp(b))
     return a, b
+
+
+class iPhone14WideCalibration:
+    """The reference's own iPhone14WideCalibration<5> (nlfFromIso,
+    getDenoiseParameters, buildDemosaicParameters; oracle/ref_calib.cpp) as
+    a CameraCalibration for scene.make_params: the parameter block comes
+    from the reference's code, not from the library under test."""
+
+    def __init__(self, levels: int = 5):
+        self.levels = levels
+
+    def getDemosaicParameters(self, iso: int, params: DemosaicParams | None = None) -> DemosaicParams:
+        p = params if params is not None else DemosaicParams()
+        rc = lib().ref_calibration_fill(int(iso), C.byref(p))
+        if rc != 0:
+            raise ValueError(f"reference calibration rejected ISO {iso} (code {rc})")
+        p.levels = self.levels
+        return p

@@ -117,6 +117,32 @@ def test_full_pipeline_cfg1_fp32_and_fp16(converter):
     assert scene.psnr(out16[..., :3], ref64[..., :3]) >= 50.0
 
 
+def test_full_pipeline_cfg2_headline(converter):
+    """The configuration the headline metric is quoted on, at full size:
+    4032x3024 RGGB 12-bit, ISO 1600 (the high-noise raw branch on), 5-level
+    pyramid, through RawConverter::demosaic's sequence
+    (raw_converter.cpp:148-248, pyramid_processor.cpp:96-172):
+      * FP32 path vs the oracle's FP32 run: 99.9th pct |diff| <= 1e-4;
+      * FP16-storage path vs the oracle's FP64 run: PSNR >= 50 dB, and its
+        PSNR against the clean scene within 0.05 dB of the FP64 oracle's."""
+    wl = scene.WORKLOADS["cfg2_4032x3024"]
+    raw, clean = scene.make_raw(wl)
+    p = scene.make_params(wl)
+    assert p.levels == 5 and p.high_noise_image == 1
+    ref32 = O.raw_pipeline(raw, p, denoise=True, f64=False)["out"]
+    out32 = _run(converter, raw, p)
+    q, m = _p999(out32[..., :3], ref32[..., :3])
+    assert q <= 1e-4, (q, m)
+    del ref32, out32
+    ref64 = O.raw_pipeline(raw, p, denoise=True, f64=True)["out"]
+    out16 = _run(converter, raw, p, fp16=True)
+    tgt = scene.target_rgb(clean)
+    ps16 = scene.psnr(out16[..., :3], tgt)
+    ps64 = scene.psnr(ref64[..., :3], tgt)
+    assert abs(ps16 - ps64) <= 0.05, (ps16, ps64)
+    assert scene.psnr(out16[..., :3], ref64[..., :3]) >= 50.0
+
+
 def test_host_pca_and_device_pca_agree(converter):
     wl, raw, clean, p = _small(seed=23)
     a = _run(converter, raw, p, host_pca=False)

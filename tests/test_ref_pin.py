@@ -136,3 +136,34 @@ def test_full_chain_reference_kernels_vs_oracle():
     ref = R.transform(den, inv)
     orc = O.raw_pipeline(raw, p, denoise=True, f64=False)["out"]
     assert scene.psnr(ref[..., :3], orc[..., :3]) >= 60.0
+
+
+# ---------------------------------------------------------------- calibration
+_ISOS = [1, 49, 50, 51, 99, 100, 150, 199, 200, 399, 400, 640, 800, 1000, 1599, 1600, 2500, 3200, 5000, 6399, 6400,
+         6500, 10000, 12199, 12200, 12499, 12500, 20000]
+
+
+def _fields(p):
+    """The parameter fields a camera calibration fills, as float lists."""
+    out = {"raw_a": list(p.raw_nlf.a), "raw_b": list(p.raw_nlf.b), "high_noise": p.high_noise_image,
+           "raw_strength": p.raw_denoise_strength, "iso": p.iso, "lsc": p.lens_shading_correction,
+           "rgb": [p.rgb_conversion.contrast, p.rgb_conversion.saturation, p.rgb_conversion.tone_curve_slope,
+                   p.rgb_conversion.exposure_bias, p.rgb_conversion.blacks, p.rgb_conversion.local_tone_mapping],
+           "ltm": [p.ltm.eps, p.ltm.shadows, p.ltm.highlights] + list(p.ltm.detail)}
+    for l in range(5):
+        out[f"nlf{l}"] = list(p.pyramid_nlf[l].a) + list(p.pyramid_nlf[l].b)
+        d = p.denoise[l]
+        out[f"den{l}"] = [d.luma, d.chroma, d.chroma_boost, d.gradient_boost, d.gradient_threshold, d.sharpening]
+    return out
+
+
+@pytest.mark.parametrize("iso", _ISOS)
+def test_calibration_bit_exact_to_reference(native, iso):
+    """gls_calibration_fill (the library's CameraCalibration) against the
+    reference's own iPhone14WideCalibration compiled for the CPU
+    (iPhone14WideCalibration.cpp:33-137, CameraCalibration.cpp:39-54):
+    every field equal, including the integer-division ISO interpolation."""
+    from glasscamerapublic_b200.api import iPhone14WideCalibration
+    ours = _fields(iPhone14WideCalibration(levels=5).getDemosaicParameters(iso))
+    ref = _fields(R.iPhone14WideCalibration(levels=5).getDemosaicParameters(iso))
+    assert ours == ref, {k: (ours[k], ref[k]) for k in ours if ours[k] != ref[k]}
