@@ -389,6 +389,10 @@ def adjoint_leg(args, rank, local, conv, stream):
         targets.append(torch.from_numpy(scene.target_rgb(clean).astype(np.float32)).to(dev))
     out = torch.empty((wl.height, wl.width, 4), dtype=torch.float32, device=dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    import glasscamerapublic_b200 as g
+    torch.cuda.synchronize()
+    lib0, _ = g.device_memory(reset_peak=True)
+    torch.cuda.reset_peak_memory_stats(dev)
     with torch.cuda.stream(stream):
         for f in range(2):
             A.loss_and_grad(conv, raws[f], params, targets[f], stream=stream)
@@ -408,6 +412,8 @@ def adjoint_leg(args, rank, local, conv, stream):
         stream.synchronize()
         wall = (time.perf_counter() - t0) / reps
         ms_vjp = max(e0.elapsed_time(e1) / reps, 1e3 * wall)
+        _, lib_peak = g.device_memory()
+        torch_peak = torch.cuda.max_memory_allocated(dev)
         e0.record(stream)
         for _ in range(reps):
             for f in range(n):
@@ -423,6 +429,13 @@ def adjoint_leg(args, rank, local, conv, stream):
         "forward_ms_per_frame": ms_fwd / n,
         "adjoint_ms_per_frame": (ms_vjp - ms_fwd) / n,
         "params_differentiated": 32,
+        "device_memory_gb": {"library_peak": lib_peak / 1e9, "library_before": lib0 / 1e9,
+                             "torch_peak": torch_peak / 1e9, "total_peak": (lib_peak + torch_peak) / 1e9,
+                             "limit": 8.0,
+                             "note": "peak over the 8-frame batch's forward + adjoint: the library's own buffers "
+                                     "(gls_device_memory, every converter buffer of the process) plus torch's "
+                                     "(inputs, targets); frames are differentiated one at a time, so the batch "
+                                     "holds one frame's activations"},
         "mean_loss": lsum / (reps * n),
         "grad_norm": float(np.linalg.norm(gsum / reps)),
         "ranks_in_gradient": dist.get_world_size() if dist.is_available() and dist.is_initialized() else 1,

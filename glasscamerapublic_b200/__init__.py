@@ -168,6 +168,7 @@ class GlsError(RuntimeError):
 _SIGNATURES = {
     "gls_last_error_message": (C.c_char_p, []),
     "gls_version": (C.c_char_p, []),
+    "gls_device_memory": (C.c_int, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_int32]),
     "gls_converter_create": (C.c_int, [C.c_int32, C.c_void_p, C.c_size_t, C.c_int32, C.POINTER(C.c_void_p)]),
     "gls_converter_destroy": (C.c_int, [C.c_void_p]),
     "gls_demosaic": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_size_t,
@@ -261,6 +262,13 @@ def check(code: int) -> None:
 
 def exported_symbols() -> list[str]:
     return list(_SIGNATURES)
+
+
+def device_memory(reset_peak: bool = False) -> tuple[int, int]:
+    """(current, peak) bytes of device memory the library holds (all devices)."""
+    cur, peak = C.c_uint64(0), C.c_uint64(0)
+    check(lib().gls_device_memory(C.byref(cur), C.byref(peak), 1 if reset_peak else 0))
+    return int(cur.value), int(peak.value)
 
 
 def block_match_tiles() -> list:

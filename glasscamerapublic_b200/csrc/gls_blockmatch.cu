@@ -16,6 +16,7 @@
 #include <cmath>
 
 #include <cstdlib>
+#include <cstring>
 #include <map>
 #include <mutex>
 
@@ -468,6 +469,301 @@ static void launch_pair(Plane<__half, 4> img, Plane<__half, 2> grad, const float
     k_block_match_pair<TY><<<g, b, smem, s>>>(img, grad, basis, out, a);
 }
 
+// ============================================================ FP16-storage path, tensor-core form
+// The window sums as matrix products on the tensor cores, one warp per
+// group of 16 pixels (a 4 x 4 block, the block shape whose windows overlap
+// most: their union is 24 x 24 positions, of which each pixel's 21 x 21
+// window is 76.6%). The union is walked as 72 tiles of 8 neighbours (24
+// rows x 3 row segments). Per tile:
+//   * S = -2 p'.q' + |q'|^2 for the 16 pixels x 8 neighbours by one
+//     mma.sync m16n8k8 (FP16 in, FP32 accumulate): A holds each pixel's
+//     centred coefficients times -2, B the neighbours' centred
+//     coefficients, C the neighbours' |q'|^2. The coefficients are stored
+//     in FP16 and the scaling by -2 is exact, so the products are exact
+//     and the sum is an FP32 sum, as in a scalar FP32 evaluation;
+//   * the weights from the accumulator fragment, two neighbours of a pixel
+//     at a time: luma exponent kl S + (kl |p'|^2 + log2 sqrt(lk)) by one
+//     packed FP32 FMA, both exponentials as ex2.approx.f16x2 (the
+//     reference evaluates its weights in half precision,
+//     demosaic.metal:851-874), chroma exponent in packed FP32;
+//   * the weights, already in the accumulator layout of S, are the A
+//     operand of two more MMAs (two tiles per k-step) against B = the
+//     neighbours' (Y, 0, 0, 1) and (0, Cb, Cr, 0, 1) columns, which add
+//     sum w Y, sum w Cb, sum w Cr and both kernel norms in FP32.
+// A neighbour outside a pixel's window has spatial weight 0 (and
+// -log2 weight +inf), which zeroes both of its weights. The spatial
+// Gaussian is separable: its x part per lane and row segment is held in
+// registers, its y part per union row comes from a 27-entry table.
+constexpr int BM_T = 32, BM_W = BM_T + 20, BM_N = BM_W * BM_W, BM_LW = BM_W + 4, BM_THREADS = 256;
+
+struct BmMmaSmem {
+    uint4 q[BM_N];               // q - c, 8 halves
+    float nn[BM_N];              // |q - c|^2
+    __half y[BM_N], cb[BM_N], cr[BM_N];
+    float lswy[32];              // -log2 of the spatial weight's y part, dy = -13..13 (+inf outside +-10)
+    __half swy[32];              // its y part / sqrt(lk) (0 outside)
+    __half luma[BM_LW * BM_LW];  // the luma tile of the projection patches, origin (x0 - 12, y0 - 12)
+};
+
+__device__ __forceinline__ uint32_t cvt_h2(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+__device__ __forceinline__ uint32_t ex2_h2(uint32_t x) {
+    uint32_t r;
+    asm("ex2.approx.f16x2 %0, %1;" : "=r"(r) : "r"(x));
+    return r;
+}
+__device__ __forceinline__ uint32_t hmul2_u(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm("mul.rn.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+__device__ __forceinline__ u64 h2_to_f2(uint32_t h) {
+    const float2 f = __half22float2(u2h_(h));
+    return pk2(f.x, f.y);
+}
+__device__ __forceinline__ void mma1688(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t b0, float c0, float c1,
+                                        float c2, float c3) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%7,%8,%9,%10};"
+        : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
+        : "r"(a0), "r"(a1), "r"(b0), "f"(c0), "f"(c1), "f"(c2), "f"(c3));
+}
+__device__ __forceinline__ uint32_t hmin2_u(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm("min.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
+__device__ __forceinline__ void mma16816_acc(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                             uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// Per pixel row of a lane (pixel g or g + 8 of the group): the constants
+// of its two neighbours' weights, as packed pairs.
+struct BmRow {
+    u64 kl, base;          // luma exponent kl S + base
+    u64 c1, c2, no1, no2;  // chroma: d = c v - o
+};
+
+// The weights of one pixel row for the lane's two neighbours of a tile:
+// (wy, wc) as half2 pairs, from its S pair (s0, s1).
+__device__ __forceinline__ void bm_weights(const BmRow& R, float s0, float s1, u64 cbf, u64 crf, u64 lsw,
+                                           uint32_t swp, uint32_t& wy, uint32_t& wc) {
+    float e0, e1;
+    upk2(fma2(R.kl, pk2(s0, s1), R.base), e0, e1);
+    // sqrt(lk) lw for both neighbours; the exponent is at most log2 sqrt(lk)
+    // but for rounding, and is held below 2 as the FP32 kernel holds it
+    const uint32_t lws = ex2_h2(hmin2_u(cvt_h2(e0, e1), 0x40004000u));
+    const u64 lf = h2_to_f2(lws);
+    const u64 d1 = fma2(R.c1, cbf, R.no1), d2 = fma2(R.c2, crf, R.no2);
+    float q0, q1;
+    upk2(fma2(lf, lf, fma2(d1, d1, fma2(d2, d2, lsw))), q0, q1);
+    wc = ex2_h2(cvt_h2(-q0, -q1));                    // sw cw
+    wy = hmul2_u(lws, swp);                           // sw lw
+}
+
+__global__ void __launch_bounds__(BM_THREADS, 2)
+    k_block_match_mma(Plane<__half, 4> img, Plane<__half, 2> grad, const float* __restrict__ basis,
+                      Plane<__half, 4> out, BlockMatchArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BmMmaSmem& sm = *reinterpret_cast<BmMmaSmem*>(smem_raw);
+    __shared__ float cen[8];
+    __shared__ float bsm[25][8];
+    const int x0 = blockIdx.x * BM_T, y0 = blockIdx.y * BM_T;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
+    const float kLog2e = 1.4426950408889634f, lk = 2.f * kLog2e, isq = rsqrtf(lk);
+    // ---- staging: spatial y table, basis, luma tile, Y/Cb/Cr of the window region
+    if (tid < 32) {
+        const int dy = tid - 13;
+        const bool in = dy >= -10 && dy <= 10;
+        const float w = in ? spatial_weight(0, dy) : 0.f;
+        sm.lswy[tid] = in ? -log2f(w) : __int_as_float(0x7f800000);
+        sm.swy[tid] = __float2half_rn(w * isq);
+    }
+    for (int k = tid; k < 200; k += BM_THREADS) bsm[k / 8][k % 8] = basis[k];
+    for (int k = tid; k < BM_LW * BM_LW; k += BM_THREADS) {
+        const int ty = k / BM_LW, tx = k % BM_LW;
+        sm.luma[k] = *img.pxc(x0 - 12 + tx, y0 - 12 + ty);
+    }
+    for (int k = tid; k < BM_N; k += BM_THREADS) {
+        const int ty = k / BM_W, tx = k % BM_W;
+        const __half* p = img.pxc(x0 - 10 + tx, y0 - 10 + ty);
+        sm.y[k] = p[0];
+        sm.cb[k] = p[1];
+        sm.cr[k] = p[2];
+    }
+    __syncthreads();
+    if (tid < 8) {  // centring vector: the coefficients (FP32) of the tile's centre pixel
+        const int cx = BM_T / 2 + 12, cy = BM_T / 2 + 12;
+        float c = 0.f;
+        for (int k = 0; k < 25; k++) c += bsm[k][tid] * __half2float(sm.luma[(cy + k / 5 - 2) * BM_LW + cx + k % 5 - 2]);
+        cen[tid] = c;
+    }
+    // pcaProjection (demosaic.metal:774-796) of every staged position:
+    // 16 positions x 5x5 patch (K = 25 padded to 32) x 25x8 basis per MMA
+    uint32_t bf[2][2];
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+        auto bk = [&](int k) { return k < 25 ? bsm[k][g] : 0.f; };
+        const int k0 = 16 * s + 2 * t;
+        bf[s][0] = h2u(__floats2half2_rn(bk(k0), bk(k0 + 1)));
+        bf[s][1] = h2u(__floats2half2_rn(bk(k0 + 8), bk(k0 + 9)));
+    }
+    __syncthreads();
+    uint32_t* q32 = reinterpret_cast<uint32_t*>(sm.q);  // [position][4] half2
+    for (int ch = warp; ch < BM_N / 16; ch += BM_THREADS / 32) {
+        const int m0 = ch * 16 + g, m1 = m0 + 8;
+        auto lidx = [&](int m) {  // the clamped image position of window position m, in the luma tile
+            const int px = clampi(x0 - 10 + m % BM_W, 0, img.w - 1) - (x0 - 12);
+            const int py = clampi(y0 - 10 + m / BM_W, 0, img.h - 1) - (y0 - 12);
+            return py * BM_LW + px;
+        };
+        const int l0 = lidx(m0), l1 = lidx(m1);
+        auto av = [&](int l, int k) { return k < 25 ? sm.luma[l + (k / 5 - 2) * BM_LW + (k % 5 - 2)] : __float2half(0.f); };
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            const int k0 = 16 * s + 2 * t;
+            mma16816_acc(c, h2u(__halves2half2(av(l0, k0), av(l0, k0 + 1))), h2u(__halves2half2(av(l1, k0), av(l1, k0 + 1))),
+                         h2u(__halves2half2(av(l0, k0 + 8), av(l0, k0 + 9))),
+                         h2u(__halves2half2(av(l1, k0 + 8), av(l1, k0 + 9))), bf[s][0], bf[s][1]);
+        }
+        const __half2 h0 = __floats2half2_rn(c[0] - cen[2 * t], c[1] - cen[2 * t + 1]);
+        const __half2 h1 = __floats2half2_rn(c[2] - cen[2 * t], c[3] - cen[2 * t + 1]);
+        q32[m0 * 4 + t] = h2u(h0);
+        q32[m1 * 4 + t] = h2u(h1);
+        const float2 f0 = __half22float2(h0), f1 = __half22float2(h1);
+        float n0 = f0.x * f0.x + f0.y * f0.y, n1 = f1.x * f1.x + f1.y * f1.y;
+        n0 += __shfl_xor_sync(0xffffffffu, n0, 1);
+        n0 += __shfl_xor_sync(0xffffffffu, n0, 2);
+        n1 += __shfl_xor_sync(0xffffffffu, n1, 1);
+        n1 += __shfl_xor_sync(0xffffffffu, n1, 2);
+        if (t == 0) {
+            sm.nn[m0] = n0;
+            sm.nn[m1] = n1;
+        }
+    }
+    __syncthreads();
+
+    // ---- lane constants: the x part of the spatial weight for the lane's
+    //      neighbour pair (2t, 2t + 1) of each row segment, pixel column g % 4
+    const int pxl = g & 3;
+    u64 lswx[3];
+    uint32_t swx[3];
+#pragma unroll
+    for (int s = 0; s < 3; s++) {
+        float l[2], w[2];
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const int dx = 8 * s + 2 * t + e - pxl - 10;
+            const bool in = dx >= -10 && dx <= 10;
+            w[e] = in ? spatial_weight(dx, 0) : 0.f;
+            l[e] = in ? -log2f(w[e]) : __int_as_float(0x7f800000);
+        }
+        lswx[s] = pk2(l[0], l[1]);
+        swx[s] = cvt_h2(w[0], w[1]);
+    }
+    const uint32_t ONE2 = 0x3c003c00u;  // half2 (1, 1)
+    const __half* ysrc = sm.y;  // the luma B column (lanes g == 0)
+
+    // ---- 4 x 4 pixel groups: 64 per tile, warp w takes groups w, w + 8, ...
+    for (int grp = warp; grp < (BM_T / 4) * (BM_T / 4); grp += BM_THREADS / 32) {
+        const int gx = (grp % (BM_T / 4)) * 4, gy = (grp / (BM_T / 4)) * 4;  // tile coordinates
+        // the lane's two pixels: rows g and g + 8 of the group = (g % 4, g / 4) and (g % 4, g / 4 + 2)
+        BmRow R[2];
+        uint32_t ap[2];  // A fragments: -2 p', components 2t, 2t + 1
+        int py[2];
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            py[r] = (g >> 2) + 2 * r;
+            const int sx = gx + pxl + 10, sy = gy + py[r] + 10;  // staged position of the pixel
+            const int pos = sy * BM_W + sx;
+            const float in_y = __half2float(sm.y[pos]), in_cb = __half2float(sm.cb[pos]), in_cr = __half2float(sm.cr[pos]);
+            const int ix = min(x0 + gx + pxl, img.w - 1), iy = min(y0 + gy + py[r], img.h - 1);
+            const BmConst k = bm_const<__half>(a, grad, img.w, img.h, ix, iy, in_y, in_cb, in_cr);
+            const float kl = fmaxf(-2.f * kLog2e * k.s * k.s, -1e30f);
+            const float base = fmaf(kl, sm.nn[pos], 0.5f * log2f(lk));
+            const float sq = sqrtf(lk);
+            const float c1 = sq * k.c1, c2 = sq * k.c2;
+            R[r].kl = pk2(kl, kl);
+            R[r].base = pk2(base, base);
+            R[r].c1 = pk2(c1, c1);
+            R[r].c2 = pk2(c2, c2);
+            R[r].no1 = pk2(-c1 * in_cb, -c1 * in_cb);
+            R[r].no2 = pk2(-c2 * in_cr, -c2 * in_cr);
+            ap[r] = hmul2_u(q32[pos * 4 + t], 0xc000c000u);  // p' components 2t, 2t + 1, times -2 (exact)
+        }
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        // union rows ny = 0..23 (staged rows gy + ny), segments s = 0..2
+        // (staged columns gx + 8 s .. + 7): tiles in row-major order, two per k-step
+        uint32_t pwy[2], pwc[2], pby, pbc;  // the pending (first) tile of a k-step
+#pragma unroll 1
+        for (int ny = 0; ny < 24; ny += 2) {
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+                const int row = ny + j / 3, s = j % 3;
+                const int base_pos = (gy + row) * BM_W + gx + 8 * s;
+                // B of S: neighbour g's coefficients 2t, 2t + 1
+                const uint32_t bq = q32[(base_pos + g) * 4 + t];
+                const float2 nnp = *reinterpret_cast<const float2*>(&sm.nn[base_pos + 2 * t]);
+                float S[4];
+                mma1688(S, ap[0], ap[1], bq, nnp.x, nnp.y, nnp.x, nnp.y);
+                const uint32_t cbh = *reinterpret_cast<const uint32_t*>(&sm.cb[base_pos + 2 * t]);
+                const uint32_t crh = *reinterpret_cast<const uint32_t*>(&sm.cr[base_pos + 2 * t]);
+                const uint32_t yh = *reinterpret_cast<const uint32_t*>(&ysrc[base_pos + 2 * t]);
+                const u64 cbf = h2_to_f2(cbh), crf = h2_to_f2(crh);
+                uint32_t wy[2], wc[2];
+#pragma unroll
+                for (int r = 0; r < 2; r++) {
+                    const int dyi = row - py[r] - 10 + 13;  // 0..26
+                    const float ly = sm.lswy[dyi];
+                    const __half sy = sm.swy[dyi];
+                    const u64 lsw = add2(lswx[s], pk2(ly, ly));
+                    const uint32_t swp = hmul2_u(swx[s], h2u(__halves2half2(sy, sy)));
+                    bm_weights(R[r], S[2 * r], S[2 * r + 1], cbf, crf, lsw, swp, wy[r], wc[r]);
+                }
+                // B columns of the sums: luma (Y, 0, 0, 1, 0..), chroma (0, Cb, Cr, 0, 1, 0..)
+                const uint32_t by = g == 0 ? yh : (g == 3 ? ONE2 : 0u);
+                const uint32_t bc = g == 1 ? cbh : (g == 2 ? crh : (g == 4 ? ONE2 : 0u));
+                if ((j & 1) == 0) {
+                    pwy[0] = wy[0]; pwy[1] = wy[1]; pwc[0] = wc[0]; pwc[1] = wc[1]; pby = by; pbc = bc;
+                } else {
+                    mma16816_acc(acc, pwy[0], pwy[1], wy[0], wy[1], pby, by);
+                    mma16816_acc(acc, pwc[0], pwc[1], wc[0], wc[1], pbc, bc);
+                }
+            }
+        }
+        // acc: rows g, g + 8; columns 2t, 2t + 1. Column 0 sum wy Y, 1 sum wc Cb,
+        // 2 sum wc Cr, 3 sum wy, 4 sum wc: gather to lane t = 0
+        const float a2 = __shfl_down_sync(0xffffffffu, acc[0], 1), a3 = __shfl_down_sync(0xffffffffu, acc[1], 1);
+        const float a4 = __shfl_down_sync(0xffffffffu, acc[0], 2);
+        const float b2 = __shfl_down_sync(0xffffffffu, acc[2], 1), b3 = __shfl_down_sync(0xffffffffu, acc[3], 1);
+        const float b4 = __shfl_down_sync(0xffffffffu, acc[2], 2);
+        if (t == 0) {
+            const int ox = x0 + gx + pxl;
+            if (ox < out.w) {
+                const int oy0 = y0 + gy + py[0], oy1 = y0 + gy + py[1];
+                if (oy0 < out.h) st4<__half>(out.px(ox, oy0), f4{acc[0] / a3, acc[1] / a4, a2 / a4, a3});
+                if (oy1 < out.h) st4<__half>(out.px(ox, oy1), f4{acc[2] / b3, acc[3] / b4, b2 / b4, b3});
+            }
+        }
+    }
+}
+
+static void launch_mma(Plane<__half, 4> img, Plane<__half, 2> grad, const float* basis, Plane<__half, 4> out,
+                       const BlockMatchArgs& a, cudaStream_t s) {
+    ensure_dynamic_smem(reinterpret_cast<const void*>(k_block_match_mma), int(sizeof(BmMmaSmem)));
+    dim3 g((img.w + BM_T - 1) / BM_T, (img.h + BM_T - 1) / BM_T);
+    k_block_match_mma<<<g, BM_THREADS, sizeof(BmMmaSmem), s>>>(img, grad, basis, out, a);
+}
+
 // Tile-height autotuner of the FP16 block matcher. Both heights compute
 // identical results (the same per-pixel arithmetic and the same centring),
 // so the choice only changes speed: 32 x 32 tiles amortise the staged halo
@@ -530,6 +826,14 @@ template <class S>
 void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, const float* basis, Plane<S, 4> out,
                         const BlockMatchArgs& a, cudaStream_t s) {
     if constexpr (is_half<S>::value) {
+        static const bool pair_kernel = [] {
+            const char* e = std::getenv("GLS_BM_KERNEL");
+            return e && std::strcmp(e, "pair") == 0;
+        }();
+        if (!pair_kernel) {
+            launch_mma(img, grad, basis, out, a, s);
+            return;
+        }
         const int ty = bm_tile_height(img.w, img.h, [&](int t) {
             if (t == 8) launch_pair<8>(img, grad, basis, out, a, s);
             else launch_pair<4>(img, grad, basis, out, a, s);

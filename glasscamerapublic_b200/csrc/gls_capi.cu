@@ -4,6 +4,7 @@
 // (pyramid_processor.cpp:96-172); the kernels are in gls_front.cu and
 // gls_pyramid.cu.
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -34,6 +35,15 @@ gls_status set_error(gls_status code, const char* fmt, ...) {
 }
 void clear_error() { g_last_error.clear(); }
 
+static std::atomic<long long> g_dev_bytes{0}, g_dev_peak{0};
+
+void devbuf_account(long long delta) {
+    const long long now = g_dev_bytes.fetch_add(delta) + delta;
+    long long pk = g_dev_peak.load();
+    while (now > pk && !g_dev_peak.compare_exchange_weak(pk, now)) {
+    }
+}
+
 cudaError_t ensure_dynamic_smem(const void* func, int bytes) {
     static std::mutex mu;
     static std::set<std::pair<const void*, int>> done;
@@ -60,7 +70,11 @@ struct Pipeline {
     DevBuf raw, scaled, grad, quad, A, B, pca, acc, basis, status;
     DevBuf scaled0;  // the Bayer plane before the raw branch, kept only for the adjoint
     DevBuf post_hist, post_stats, post_perm, post_gtab, post_ab;  // display post-processing scratch
-    DevBuf img[GLS_MAX_LEVELS], gradp[GLS_MAX_LEVELS], sub[GLS_MAX_LEVELS], den[GLS_MAX_LEVELS];
+    // the pyramid: each level's image and gradient (level 0 in B / grad) and
+    // denoised output; one reconstructed layer buffer serves every level
+    // (a level's layer is read only by that level's PCA and block matching;
+    // the adjoint recomputes it in its reverse sweep)
+    DevBuf img[GLS_MAX_LEVELS], gradp[GLS_MAX_LEVELS], den[GLS_MAX_LEVELS], layer;
     DevBuf nc[GLS_MAX_LEVELS];  // chroma norms, kept only for the adjoint
     DevBuf out_f32, out_f16, stage_in, stage_grad;
     std::vector<double> host_acc;
@@ -75,6 +89,7 @@ struct Pipeline {
         GLS_TRY(A.ensure(n * 4 * sizeof(S)));
         GLS_TRY(B.ensure(n * 4 * sizeof(S)));
         GLS_TRY(pca.ensure(n * 8 * sizeof(S)));
+        GLS_TRY(layer.ensure(n * 4 * sizeof(S)));
         GLS_TRY(acc.ensure(sizeof(double) * kPcaAcc * kPcaMaxBlocks * GLS_MAX_LEVELS));
         GLS_TRY(basis.ensure(sizeof(float) * 200 * GLS_MAX_LEVELS));
         GLS_TRY(status.ensure(sizeof(int) * GLS_MAX_LEVELS));
@@ -84,7 +99,6 @@ struct Pipeline {
                 GLS_TRY(img[i].ensure(ni * 4 * sizeof(S)));
                 GLS_TRY(gradp[i].ensure(ni * 2 * sizeof(S)));
             }
-            GLS_TRY(sub[i].ensure(ni * 4 * sizeof(S)));
             GLS_TRY(den[i].ensure(ni * 4 * sizeof(S)));
         }
         W = w;
@@ -93,13 +107,12 @@ struct Pipeline {
         return GLS_OK;
     }
     void release() {
-        for (DevBuf* b : {&raw, &scaled, &scaled0, &grad, &quad, &A, &B, &pca, &acc, &basis, &status, &out_f32,
+        for (DevBuf* b : {&raw, &scaled, &scaled0, &grad, &quad, &A, &B, &pca, &layer, &acc, &basis, &status, &out_f32,
                           &out_f16, &stage_in, &stage_grad, &post_hist, &post_stats, &post_perm, &post_gtab, &post_ab})
             b->release();
         for (int i = 0; i < GLS_MAX_LEVELS; i++) {
             img[i].release();
             gradp[i].release();
-            sub[i].release();
             den[i].release();
             nc[i].release();
         }
@@ -380,7 +393,7 @@ static gls_status pyramid_run(gls_converter* cv, Pipeline<S>& P, Plane<S, 4> img
             sa.sharpening = dp.sharpening;
             sa.nlf_a = p->pyramid_nlf[i].a[0] * dp.luma;
             sa.nlf_b = p->pyramid_nlf[i].b[0] * dp.luma;
-            layer = plane<S, 4>(P.sub[i], wi, hi);
+            layer = plane<S, 4>(P.layer, wi, hi);
             KScope k(cv->prof, KC_SUBTRACT, s);
             launch_subtract_noise<S>(img[i], img[i + 1], plane<S, 4>(P.den[i + 1], W >> (i + 1), H >> (i + 1)), grd[i],
                                      layer, sa, s);
@@ -801,9 +814,25 @@ static gls_status adjoint_run(gls_converter* cv, const gls_demosaic_params* p, c
         const int wi = W >> i, hi = H >> i;
         const gls_denoise_params& dp = p->denoise[i];
         const float* img_i = static_cast<const float*>(i == 0 ? P.B.p : P.img[i].p);
-        const float* layer = i < L - 1 ? static_cast<const float*>(P.sub[i].p) : img_i;
         const float* grd = static_cast<const float*>(i == 0 ? P.grad.p : P.gradp[i].p);
         const float* basis = static_cast<const float*>(P.basis.p) + i * 200;
+        // the level's reconstructed layer, recomputed from the retained
+        // pyramid (the forward keeps one layer buffer for all levels): the
+        // same kernel on the same inputs, so the same bits
+        const float* layer = img_i;
+        if (i < L - 1) {
+            SubtractArgs ra;
+            ra.luma_weight = 1.f;
+            ra.sharpening = dp.sharpening;
+            ra.nlf_a = p->pyramid_nlf[i].a[0] * dp.luma;
+            ra.nlf_b = p->pyramid_nlf[i].b[0] * dp.luma;
+            const int cw = W >> (i + 1), ch = H >> (i + 1);
+            launch_subtract_noise<float>(Plane<float, 4>{const_cast<float*>(img_i), wi, hi, size_t(wi) * 4},
+                                         plane<float, 4>(P.img[i + 1], cw, ch), plane<float, 4>(P.den[i + 1], cw, ch),
+                                         Plane<float, 2>{const_cast<float*>(grd), wi, hi, size_t(wi) * 2},
+                                         plane<float, 4>(P.layer, wi, hi), ra, s);
+            layer = static_cast<const float*>(P.layer.p);
+        }
         launch_pca_project<float>(Plane<float, 4>{const_cast<float*>(layer), wi, hi, size_t(wi) * 4}, basis,
                                   plane<float, 8>(P.pca, wi, hi), s);
         AdjointLevelArgs la{};
@@ -1016,6 +1045,15 @@ const char* gls_last_error_message(void) { return g_last_error.c_str(); }
 
 const char* gls_version(void) {
     return "glscam 0.1 (sm_100a; demosaic, pyramid PCA block-matching denoise)";
+}
+
+gls_status gls_device_memory(uint64_t* current_bytes, uint64_t* peak_bytes, int32_t reset_peak) {
+    clear_error();
+    const long long now = g_dev_bytes.load();
+    if (current_bytes) *current_bytes = uint64_t(now);
+    if (peak_bytes) *peak_bytes = uint64_t(g_dev_peak.load());
+    if (reset_peak) g_dev_peak.store(now);
+    return GLS_OK;
 }
 
 gls_status gls_converter_create(int32_t device, const uint8_t* icc, size_t icc_len, int32_t calibrate_from_image,
@@ -1342,6 +1380,9 @@ gls_status gls_demosaic_denoise_vjp(gls_converter* conv, const uint16_t* raw, in
     const size_t trow = size_t(width) * target->channels * 4;
     const size_t tstride_b = target->stride_bytes ? target->stride_bytes : trow;
     if (tstride_b < trow || tstride_b % 4) return set_error(GLS_ERR_INVALID_ARG, "bad target stride");
+    if (conv->calibrate)
+        return set_error(GLS_ERR_UNSUPPORTED, "the gradient is taken with respect to the given noise models; "
+                                              "a calibrating converter replaces them with measured ones");
     GLS_CUDA(cudaSetDevice(conv->device));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     gls_image_view out{};  // converter-owned FP32 output
@@ -1385,6 +1426,9 @@ gls_status gls_pyramid_denoise_vjp(gls_converter* conv, const gls_image_view* yc
         if (!g_ycc->data) return set_error(GLS_ERR_INVALID_ARG, "g_ycc has no data");
         GLS_TRY(check3(g_ycc, "g_ycc"));
     }
+    if (conv->calibrate)
+        return set_error(GLS_ERR_UNSUPPORTED, "the gradient is taken with respect to the given noise models; "
+                                              "a calibrating converter replaces them with measured ones");
     GLS_CUDA(cudaSetDevice(conv->device));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const bool host_io = flags & GLS_HOST_IO;

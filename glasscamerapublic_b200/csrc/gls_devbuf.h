@@ -22,12 +22,20 @@ namespace gls {
         if (s_ != GLS_OK) return s_;     \
     } while (0)
 
+// Bytes of device memory the library holds (all of it is DevBuf), summed
+// over devices, and the largest value since the last reset
+// (gls_device_memory).
+void devbuf_account(long long delta);
+
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
     gls_status ensure(size_t b) {
         if (b <= bytes) return GLS_OK;
-        if (p) cudaFree(p);
+        if (p) {
+            cudaFree(p);
+            devbuf_account(-static_cast<long long>(bytes));
+        }
         p = nullptr;
         bytes = 0;
         cudaError_t e = cudaMalloc(&p, b);
@@ -36,6 +44,7 @@ struct DevBuf {
             return set_error(GLS_ERR_OOM, "cudaMalloc(%zu) failed: %s", b, cudaGetErrorString(e));
         }
         bytes = b;
+        devbuf_account(static_cast<long long>(b));
         return GLS_OK;
     }
     // ensure(), and a newly allocated buffer is zeroed on stream s (a
@@ -49,7 +58,10 @@ struct DevBuf {
         return GLS_OK;
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            cudaFree(p);
+            devbuf_account(-static_cast<long long>(bytes));
+        }
         p = nullptr;
         bytes = 0;
     }

@@ -164,6 +164,14 @@ const char* gls_last_error_message(void);
 /* Library build string (kernels, architecture). */
 const char* gls_version(void);
 
+/* Device memory the library holds (no reference counterpart; the reference
+ * allocates Metal buffers per RawConverter, raw_converter.cpp:20-45): the
+ * bytes of every converter, pyramid, detector and scratch buffer of this
+ * process, summed over devices, and the largest such sum since the last
+ * reset. reset_peak != 0 sets the peak to the current value afterwards.
+ * Buffers grow to the largest frame seen and are kept until destroy. */
+gls_status gls_device_memory(uint64_t* current_bytes, uint64_t* peak_bytes, int32_t reset_peak);
+
 /* RawConverter(device, icc, calibrateFromImage), raw_converter.hpp:128-156.
  * icc may be NULL (xyz_sRGB). With calibrate_from_image the converter
  * measures the noise model of every frame it converts, as the reference

@@ -5,7 +5,10 @@ in float64 on the CPU, so that torch.autograd gives a reference gradient of
 the MSE loss with respect to the per-level parameters. Test infrastructure
 only: the product's adjoint is hand-written CUDA (gls_adjoint.cu).
 
-The PCA bases are inputs (held fixed), as in the adjoint.
+The PCA bases are inputs (held fixed), as in the adjoint. Every function
+runs on the device of its inputs; with checkpoint=True the block matching
+keeps only one window row's intermediates for the backward pass (it
+recomputes them), so a 2048x1536 frame fits on one GPU.
 """
 from __future__ import annotations
 
@@ -50,8 +53,8 @@ def bilin(img: torch.Tensor, u: torch.Tensor, v: torch.Tensor) -> torch.Tensor:
 def downsample(img: torch.Tensor, ow: int, oh: int) -> torch.Tensor:
     h, w = img.shape[:2]
     rx, ry = w / ow, h / oh
-    x = torch.arange(ow, dtype=torch.float64)
-    y = torch.arange(oh, dtype=torch.float64)
+    x = torch.arange(ow, dtype=torch.float64, device=img.device)
+    y = torch.arange(oh, dtype=torch.float64, device=img.device)
     u0, u1 = x * rx - 0.5, (x + 1) * rx - 0.5
     v0, v1 = y * ry - 0.5, (y + 1) * ry - 0.5
     return 0.25 * (bilin(img, u0, v0) + bilin(img, u1, v0) + bilin(img, u0, v1) + bilin(img, u1, v1))
@@ -66,8 +69,8 @@ def subtract_noise(inp, coarse, coarse_den, grad, sharpening, na, nb):
     h, w = inp.shape[:2]
     ch, cw = coarse.shape[:2]
     rx, ry = cw / w, ch / h
-    u = (torch.arange(w, dtype=torch.float64) + 0.5) * rx - 0.5
-    v = (torch.arange(h, dtype=torch.float64) + 0.5) * ry - 0.5
+    u = (torch.arange(w, dtype=torch.float64, device=inp.device) + 0.5) * rx - 0.5
+    v = (torch.arange(h, dtype=torch.float64, device=inp.device) + 0.5) * ry - 0.5
     p1 = bilin(coarse[..., :3], u, v)
     pd = bilin(coarse_den[..., :3], u, v)
     dn = inp[..., :3] - (p1 - pd)  # lumaDenoiseWeight = 1
@@ -87,9 +90,9 @@ def subtract_noise(inp, coarse, coarse_den, grad, sharpening, na, nb):
 def pca_project(layer, basis):
     h, w = layer.shape[:2]
     lum = layer[..., 0]
-    ys = torch.arange(h)
-    xs = torch.arange(w)
-    acc = torch.zeros(h, w, 8, dtype=torch.float64)
+    ys = torch.arange(h, device=layer.device)
+    xs = torch.arange(w, device=layer.device)
+    acc = torch.zeros(h, w, 8, dtype=torch.float64, device=layer.device)
     row = 0
     for j in range(-2, 3):
         for i in range(-2, 3):
@@ -99,9 +102,34 @@ def pca_project(layer, basis):
     return acc
 
 
-def block_match(layer, grad, pca, a, b, tm, dp):
-    """a, b: (3,) tensors of the level's NLF; tm: (luma, chroma, chroma)."""
+def _window_row(j, layer, pca, L, K1, K2):
+    """The five window sums of block_match over the taps of window row j."""
     h, w = layer.shape[:2]
+    ys, xs = torch.arange(h, device=layer.device), torch.arange(w, device=layer.device)
+    yi = (ys + j).clamp(0, h - 1)
+    fy = torch.zeros(h, w, dtype=torch.float64, device=layer.device)
+    fcb, fcr, ny, nc = torch.zeros_like(fy), torch.zeros_like(fy), torch.zeros_like(fy), torch.zeros_like(fy)
+    for i in range(-10, 11):
+        xi = (xs + i).clamp(0, w - 1)
+        s = layer[yi][:, xi]
+        sp = pca[yi][:, xi]
+        d2 = ((sp - pca) ** 2).sum(-1)
+        lw = torch.exp(-2.0 * d2 * L * L)
+        c1 = (s[..., 1] - layer[..., 1]) * K1
+        c2 = (s[..., 2] - layer[..., 2]) * K2
+        cw = torch.exp(-2.0 * (lw * lw + c1 * c1 + c2 * c2))
+        d = 0.1 * math.sqrt(i * i + j * j)
+        sw = math.exp(-2.0 * d * d)
+        fy = fy + sw * lw * s[..., 0]
+        fcb = fcb + sw * cw * s[..., 1]
+        fcr = fcr + sw * cw * s[..., 2]
+        ny = ny + sw * lw
+        nc = nc + sw * cw
+    return fy, fcb, fcr, ny, nc
+
+
+def block_match(layer, grad, pca, a, b, tm, dp, checkpoint: bool = False):
+    """a, b: (3,) tensors of the level's NLF; tm: (luma, chroma, chroma)."""
     y = layer[..., 0]
     dm = [1.0 / (tm[c] * torch.sqrt(a[c] + b[c] * y)) for c in range(3)]
     mag = torch.sqrt(grad[..., 0] ** 2 + grad[..., 1] ** 2)
@@ -109,31 +137,19 @@ def block_match(layer, grad, pca, a, b, tm, dp):
     edge = smoothstep(2.0, 16.0, dp.gradient_threshold * mag / sig0)
     L = dm[0] / (1.0 + dp.gradient_boost * edge)
     K1, K2 = dm[1] / dp.chroma_boost, dm[2] / dp.chroma_boost
-    ys, xs = torch.arange(h), torch.arange(w)
-    fy = torch.zeros(h, w, dtype=torch.float64)
-    fcb, fcr, ny, nc = torch.zeros_like(fy), torch.zeros_like(fy), torch.zeros_like(fy), torch.zeros_like(fy)
+    sums = None
     for j in range(-10, 11):
-        yi = (ys + j).clamp(0, h - 1)
-        for i in range(-10, 11):
-            xi = (xs + i).clamp(0, w - 1)
-            s = layer[yi][:, xi]
-            sp = pca[yi][:, xi]
-            d2 = ((sp - pca) ** 2).sum(-1)
-            lw = torch.exp(-2.0 * d2 * L * L)
-            c1 = (s[..., 1] - layer[..., 1]) * K1
-            c2 = (s[..., 2] - layer[..., 2]) * K2
-            cw = torch.exp(-2.0 * (lw * lw + c1 * c1 + c2 * c2))
-            d = 0.1 * math.sqrt(i * i + j * j)
-            sw = math.exp(-2.0 * d * d)
-            fy = fy + sw * lw * s[..., 0]
-            fcb = fcb + sw * cw * s[..., 1]
-            fcr = fcr + sw * cw * s[..., 2]
-            ny = ny + sw * lw
-            nc = nc + sw * cw
+        if checkpoint:
+            from torch.utils.checkpoint import checkpoint as ckpt
+            part = ckpt(_window_row, j, layer, pca, L, K1, K2, use_reentrant=False)
+        else:
+            part = _window_row(j, layer, pca, L, K1, K2)
+        sums = part if sums is None else tuple(u + v for u, v in zip(sums, part))
+    fy, fcb, fcr, ny, nc = sums
     return torch.stack([fy / ny, fcb / nc, fcr / nc, ny], -1)
 
 
-def pyramid_rgb(ds, grad, theta, params, bases, y2c):
+def pyramid_rgb(ds, grad, theta, params, bases, y2c, checkpoint: bool = False):
     """Denoised linear camera RGB (h, w, 3) of the despeckled YCbCr image ds
     (h, w, 4) and its gradient (h, w, 2)."""
     L = params.levels
@@ -158,25 +174,27 @@ def pyramid_rgb(ds, grad, theta, params, bases, y2c):
         else:
             layer = img[i]
         pca = pca_project(layer, bases[i])
-        den[i] = block_match(layer, grd[i], pca, a, b, (luma, chroma, chroma), dp)
+        den[i] = block_match(layer, grd[i], pca, a, b, (luma, chroma, chroma), dp, checkpoint)
     return den[0][..., :3] @ y2c.T
 
 
-def loss_and_grad(ds, grad, params, bases, y2c, target, with_ds: bool = False):
+def loss_and_grad(ds, grad, params, bases, y2c, target, with_ds: bool = False, device: str = "cpu",
+                  checkpoint: bool = False):
     """MSE loss and its gradient with respect to the first 30 parameters
     (NaN for the two raw-green entries, which act before ds); with with_ds,
-    also dL/d(ds) (h, w, 3)."""
-    theta = theta_from_params(params, params.levels).requires_grad_(True)
-    dst = torch.as_tensor(ds, dtype=torch.float64).clone().requires_grad_(with_ds)
-    rgb = pyramid_rgb(dst, torch.as_tensor(grad, dtype=torch.float64), theta, params,
-                      torch.as_tensor(bases, dtype=torch.float64), torch.as_tensor(y2c, dtype=torch.float64))
-    loss = ((rgb - torch.as_tensor(target, dtype=torch.float64)[..., :3]) ** 2).mean()
+    also dL/d(ds) (h, w, 3). device: where the float64 evaluation runs."""
+    f64 = dict(dtype=torch.float64, device=device)
+    theta = theta_from_params(params, params.levels).to(device).requires_grad_(True)
+    dst = torch.as_tensor(ds, **f64).clone().requires_grad_(with_ds)
+    rgb = pyramid_rgb(dst, torch.as_tensor(grad, **f64), theta, params, torch.as_tensor(bases, **f64),
+                      torch.as_tensor(y2c, **f64), checkpoint)
+    loss = ((rgb - torch.as_tensor(target, **f64)[..., :3]) ** 2).mean()
     loss.backward()
-    g = theta.grad.detach().clone()
+    g = theta.grad.detach().cpu().clone()
     g[30:] = float("nan")
-    res = (float(loss.detach()), g.numpy(), rgb.detach().numpy())
+    res = (float(loss.detach()), g.numpy(), rgb.detach().cpu().numpy())
     if with_ds:
-        res = res + (dst.grad.detach()[..., :3].numpy(),)
+        res = res + (dst.grad.detach()[..., :3].cpu().numpy(),)
     return res
 
 

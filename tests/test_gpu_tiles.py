@@ -1,8 +1,9 @@
-"""The FP16 block matcher's tile-height autotuner: 32 x 32 and 32 x 16 pixel
-tiles compute the same bits (same per-pixel arithmetic, same centring
-vector), so forcing either height through GLS_BM_TILE, or letting the
-autotuner choose, gives identical frames. Each setting runs in its own
-process because the height is read once per process."""
+"""The FFMA2 pair form of the FP16 block matcher (GLS_BM_KERNEL=pair) and
+its tile-height autotuner: 32 x 32 and 32 x 16 pixel tiles compute the same
+bits (same per-pixel arithmetic, same centring vector), so forcing either
+height through GLS_BM_TILE, or letting the autotuner choose, gives
+identical frames. Each setting runs in its own process because the kernel
+choice and the height are read once per process."""
 import json
 import os
 import subprocess
@@ -44,6 +45,7 @@ c.close()
 def _run(tmp_path, tag, tile):
     env = dict(os.environ)
     env.pop("GLS_BM_TILE", None)
+    env["GLS_BM_KERNEL"] = "pair"
     if tile:
         env["GLS_BM_TILE"] = str(tile)
     base = str(tmp_path / tag)
