@@ -212,6 +212,144 @@ struct DemosaicSmem {
 };
 
 
+// The three interpolation passes evaluate the reference's formulas at two
+// kinds of site: the Bayer sites of the pass's own colour copy a value, the
+// others run the full stencil. Within a Bayer row the two kinds alternate,
+// so a lane takes a horizontal pair of sites (one of each) and no warp
+// runs both branches. Tiles whose staged region reaches past the image
+// edge (clamped, repeated positions) take the sites one by one instead.
+// The per-site arithmetic is the same in both orders.
+struct DmSites {
+    int rx, ry, bx, by;
+    __device__ __forceinline__ bool red(int px, int py) const { return (rx & 1) == (px & 1) && (ry & 1) == (py & 1); }
+    __device__ __forceinline__ bool blue(int px, int py) const { return (bx & 1) == (px & 1) && (by & 1) == (py & 1); }
+};
+
+// interpolateGreen (demosaic.metal:215-316) at raw-tile index (lx, ly) of a
+// red or blue site; gg = |gradient| there.
+__device__ __forceinline__ float dm_green(const DemosaicSmem& sm, int lx, int ly, float2 gg, const DemosaicArgs& a,
+                                          float lowNoise) {
+    const float kPi = 3.14159265358979323846f;
+    auto R = [&](int di, int dj) { return sm.raw[ly + dj][lx + di]; };
+    const float gl = R(-1, 0), gr = R(1, 0), gu = R(0, -1), gd = R(0, 1);
+    const float cxy = R(0, 0);
+    const float cl = R(-2, 0), cr = R(2, 0), cu = R(0, -2), cd = R(0, 2);
+    const float c2ave = (R(-1, -1) + R(1, -1) + R(-1, 1) + R(1, 1)) / 4.f;
+    const float gave = (gl + gr + gu + gd) / 4.f;
+    const float glfx = (gl + gr) / 2.f, glfy = (gu + gd) / 2.f;
+    const float ghfx = ((cl + cr) - 2.f * cxy) / 4.f, ghfy = ((cu + cd) - 2.f * cxy) / 4.f;
+    const float sd = sqrtf(a.gv0 + a.gv1 * gave);
+    const float glen = sqrtf(gg.x * gg.x + gg.y * gg.y);
+    const float gthr = smoothstepf(sd, 4.f * sd, glen);
+    const float lowthr = 1.f - smoothstepf(2.f * sd, 8.f * sd, glen);
+    const float sharp = (0.5f + 0.5f * lowNoise) * gthr * (1.f + lowNoise * lowthr);
+    const float hl = 1.f - smoothstepf(0.25f, 1.f, fmaxf(cxy, fmaxf(fmaxf(cl, cr), fmaxf(cu, cd))));
+    float dir = 2.f * atan2f(gg.y, gg.x) / kPi;
+    if (a.gv1 < 1e-3f) {
+        dir = dir < 0.5f ? mixf(dir, 0.f, 1.f - smoothstepf(0.3f, 0.45f, dir))
+                         : mixf(dir, 1.f, smoothstepf(1.f - 0.45f, 1.f - 0.3f, dir));
+    }
+    const float cmin = fminf(cxy, fminf(gave, c2ave)), cmax = fmaxf(cxy, fmaxf(gave, c2ave));
+    const float white = cmin / cmax;
+    const float k = hl * white * sharp;
+    const float gex = glfx - k * ghfx, gey = glfy - k * ghfy;
+    float g = mixf(gey, gex, dir);
+    const float maxo = mixf(1.f, 1.5f, white), mino = mixf(1.f, 0.5f, white);
+    const float gmax = fmaxf(fmaxf(gl, gr), fmaxf(gu, gd));
+    const float gmin = fminf(fminf(gl, gr), fminf(gu, gd));
+    return clampf(g, mino * gmin, maxo * gmax);
+}
+
+// interpolateRedBlue (demosaic.metal:318-416) at a red or blue site: the
+// other colour; green-tile index (gx, gy), raw-tile index (lx, ly).
+__device__ __forceinline__ float dm_redblue(const DemosaicSmem& sm, int gx, int gy, int lx, int ly, bool red,
+                                            const DemosaicArgs& a) {
+    const float kPi = 3.14159265358979323846f;
+    auto R = [&](int di, int dj) { return sm.raw[ly + dj][lx + di]; };
+    auto G = [&](int di, int dj) { return sm.green[gy + dj][gx + di]; };
+    const float g0 = G(0, 0), c1 = R(0, 0);
+    const float c2tl = R(-1, -1), c2tr = R(1, -1), c2bl = R(-1, 1), c2br = R(1, 1);
+    const float c2ave = (c2tl + c2tr + c2bl + c2br) / 4.f;
+    const float gctl = G(-1, -1) - c2tl, gctr = G(1, -1) - c2tr, gcbl = G(-1, 1) - c2bl, gcbr = G(1, 1) - c2br;
+    const float gtl2 = G(-2, -2), gtr2 = G(2, -2), gbl2 = G(-2, 2), gbr2 = G(2, 2);
+    const float gctl2 = gtl2 - R(-2, -2), gctr2 = gtr2 - R(2, -2), gcbl2 = gbl2 - R(-2, 2), gcbr2 = gbr2 - R(2, 2);
+    const float v0 = red ? a.rv0 : a.bv0, v1 = red ? a.rv1 : a.bv1;
+    const float sd = sqrtf(v0 + v1 * c2ave);
+    const float2 gg = sm.grad[gy][gx];
+    const float dir = 1.f - 2.f * atan2f(gg.y, gg.x) / kPi;
+    const float gthr = smoothstepf(sd, 4.f * sd, sqrtf(gg.x * gg.x + gg.y * gg.y));
+    const float alpha = mixf(0.5f, dir, gthr);
+    const float hl = 1.f - smoothstepf(0.25f, 1.f, fmaxf(g0, fmaxf(fmaxf(gtr2, gbl2), fmaxf(gtl2, gbr2))));
+    const float gc = g0 - c1;
+    const float aa = (gctr + gcbl) / 2.f + hl * (gctr2 + gcbl2 - 2.f * gc) / 8.f;
+    const float bb = (gctl + gcbr) / 2.f + hl * (gctl2 + gcbr2 - 2.f * gc) / 8.f;
+    const float c2 = g0 - mixf(aa, bb, alpha);
+    const float c2max = fmaxf(fmaxf(c2tl, c2tr), fmaxf(c2bl, c2br));
+    const float c2min = fminf(fminf(c2tl, c2tr), fminf(c2bl, c2br));
+    return clampf(c2, c2min, c2max);
+}
+
+// interpolateRedBlueAtGreen (demosaic.metal:418-521) at a green site:
+// tmp-tile index (cx, cy), green-tile index of the gradient (gx, gy).
+__device__ __forceinline__ void dm_rb_at_green(const DemosaicSmem& sm, int cx, int cy, float2 gg, const DemosaicArgs& a,
+                                               float rgb[3]) {
+    const float kPi = 3.14159265358979323846f;
+    auto P = [&](int di, int dj, int c) { return sm.tmp[c][cy + dj][cx + di]; };
+    const float g0 = P(0, 0, 1);
+    const float lr = P(-1, 0, 0), lg = P(-1, 0, 1), lb = P(-1, 0, 2);
+    const float rr = P(1, 0, 0), rg = P(1, 0, 1), rb = P(1, 0, 2);
+    const float ur = P(0, -1, 0), ug = P(0, -1, 1), ub = P(0, -1, 2);
+    const float dr = P(0, 1, 0), dg = P(0, 1, 1), db = P(0, 1, 2);
+    const float red_ave = (lr + rr + ur + dr) / 4.f, blue_ave = (lb + rb + ub + db) / 4.f;
+    const float grl = lg - lr, grr = rg - rr, gru = ug - ur, grd = dg - dr;
+    const float gbl = lg - lb, gbr = rg - rb, gbu = ug - ub, gbd = dg - db;
+    const float grl3 = P(-3, 0, 1) - P(-3, 0, 0), grr3 = P(3, 0, 1) - P(3, 0, 0);
+    const float gru3 = P(0, -3, 1) - P(0, -3, 0), grd3 = P(0, 3, 1) - P(0, 3, 0);
+    const float gbl3 = P(-3, 0, 1) - P(-3, 0, 2), gbr3 = P(3, 0, 1) - P(3, 0, 2);
+    const float gbu3 = P(0, -3, 1) - P(0, -3, 2), gbd3 = P(0, 3, 1) - P(0, 3, 2);
+    const float dir = 2.f * atan2f(gg.y, gg.x) / kPi;
+    const float glen = sqrtf(gg.x * gg.x + gg.y * gg.y);
+    const float rsd = sqrtf(a.rv0 + a.rv1 * red_ave), bsd = sqrtf(a.bv0 + a.bv1 * blue_ave);
+    const float ralpha = mixf(0.5f, dir, smoothstepf(rsd, 4.f * rsd, glen));
+    const float balpha = mixf(0.5f, dir, smoothstepf(bsd, 4.f * bsd, glen));
+    const float hl = 1.f - smoothstepf(0.25f, 1.f, fmaxf(g0, fmaxf(fmaxf(rg, lg), fmaxf(dg, ug))));
+    const float red_v = g0 - mixf((gru + grd) / 2.f - hl * ((grd3 - gru) - (grd - gru3)) / 8.f,
+                                  (grl + grr) / 2.f - hl * ((grr3 - grl) - (grr - grl3)) / 8.f, ralpha);
+    const float blue_v = g0 - mixf((gbu + gbd) / 2.f - hl * ((gbd3 - gbu) - (gbd - gbu3)) / 8.f,
+                                   (gbl + gbr) / 2.f - hl * ((gbr3 - gbl) - (gbr - gbl3)) / 8.f, balpha);
+    rgb[0] = clampf(red_v, fminf(fminf(lr, rr), fminf(ur, dr)), fmaxf(fmaxf(lr, rr), fmaxf(ur, dr)));
+    rgb[1] = g0;
+    rgb[2] = clampf(blue_v, fminf(fminf(lb, rb), fminf(ub, db)), fmaxf(fmaxf(lb, rb), fmaxf(ub, db)));
+}
+
+// blendHighlightsImage (clip = 1) and the optional colour transform.
+__device__ __forceinline__ f4 dm_finish(float rgb[3], const DemosaicArgs& a) {
+    const float clip = 1.f;
+    if (rgb[0] > clip || rgb[1] > clip || rgb[2] > clip) {
+        const float s3 = 1.7320508f;
+        const float c0[3] = {rgb[0], rgb[1], rgb[2]};
+        const float c1[3] = {fminf(rgb[0], clip), fminf(rgb[1], clip), fminf(rgb[2], clip)};
+        const float l0x = c0[0] + c0[1] + c0[2], l0y = s3 * c0[0] - s3 * c0[1], l0z = -c0[0] - c0[1] + 2.f * c0[2];
+        const float l1y = s3 * c1[0] - s3 * c1[1], l1z = -c1[0] - c1[1] + 2.f * c1[2];
+        const float sum0 = l0y * l0y + l0z * l0z, sum1 = l1y * l1y + l1z * l1z;
+        const float chr = sum0 > 0.f ? sqrtf(sum1 / sum0) : 1.f;
+        const float ly = l0y * chr, lz = l0z * chr;
+        rgb[0] = (l0x + (s3 / 2.f) * ly - 0.5f * lz) / 3.f;
+        rgb[1] = (l0x - (s3 / 2.f) * ly - 0.5f * lz) / 3.f;
+        rgb[2] = (l0x + lz) / 3.f;
+    }
+    f4 o;
+    if (a.transform) {
+        o.x = a.m[0] * rgb[0] + a.m[1] * rgb[1] + a.m[2] * rgb[2];
+        o.y = a.m[3] * rgb[0] + a.m[4] * rgb[1] + a.m[5] * rgb[2];
+        o.z = a.m[6] * rgb[0] + a.m[7] * rgb[1] + a.m[8] * rgb[2];
+    } else {
+        o.x = rgb[0]; o.y = rgb[1]; o.z = rgb[2];
+    }
+    o.w = 0.f;
+    return o;
+}
+
 template <class S>
 __global__ void __launch_bounds__(256) k_demosaic(Plane<S, 1> raw, Plane<S, 2> grad, Plane<S, 4> out, DemosaicArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -219,9 +357,12 @@ __global__ void __launch_bounds__(256) k_demosaic(Plane<S, 1> raw, Plane<S, 2> g
     const int x0 = blockIdx.x * DM_TW, y0 = blockIdx.y * DM_TH;
     const int tid = threadIdx.y * blockDim.x + threadIdx.x, nth = blockDim.x * blockDim.y;
     const int W = raw.w, H = raw.h;
-    const int rx = kBayer[a.pattern][0][0], ry = kBayer[a.pattern][0][1];
-    const int bx = kBayer[a.pattern][2][0], by = kBayer[a.pattern][2][1];
-    const float kPi = 3.14159265358979323846f;
+    const DmSites st{kBayer[a.pattern][0][0], kBayer[a.pattern][0][1], kBayer[a.pattern][2][0], kBayer[a.pattern][2][1]};
+    // the staged region (raw tile, origin -7) lies inside the image: positions
+    // are not clamped, and sites alternate along every row
+    const bool inner = x0 >= 7 && y0 >= 7 && x0 + DM_RW - 7 <= W && y0 + DM_RH - 7 <= H;
+    // a site (px, py) is red or blue iff the parity of px ^ py is this
+    const int rb_par = (st.rx ^ st.ry) & 1;
 
     for (int i = tid; i < DM_RW * DM_RH; i += nth) {
         const int ty = i / DM_RW, tx = i % DM_RW;
@@ -236,165 +377,95 @@ __global__ void __launch_bounds__(256) k_demosaic(Plane<S, 1> raw, Plane<S, 2> g
 
     // ---- green at the clamped position of every green-tile entry
     const float lowNoise = 1.f - smoothstepf(3.5e-4f, 2e-3f, a.gv1);
-    for (int i = tid; i < DM_GW * DM_GH; i += nth) {
-        const int ty = i / DM_GW, tx = i % DM_GW;
-        const int px = clampi(x0 - 5 + tx, 0, W - 1), py = clampi(y0 - 5 + ty, 0, H - 1);
-        const int lx = px - (x0 - 7), ly = py - (y0 - 7);  // raw-tile index of the clamped position
-        auto R = [&](int di, int dj) { return sm.raw[ly + dj][lx + di]; };
-        const bool red = (rx & 1) == (px & 1) && (ry & 1) == (py & 1);
-        const bool blue = (bx & 1) == (px & 1) && (by & 1) == (py & 1);
-        float g;
-        if (!(red || blue)) {
-            g = R(0, 0);
-        } else {
-            const float gl = R(-1, 0), gr = R(1, 0), gu = R(0, -1), gd = R(0, 1);
-            const float cxy = R(0, 0);
-            const float cl = R(-2, 0), cr = R(2, 0), cu = R(0, -2), cd = R(0, 2);
-            const float c2ave = (R(-1, -1) + R(1, -1) + R(-1, 1) + R(1, 1)) / 4.f;
-            const float gave = (gl + gr + gu + gd) / 4.f;
-            const float2 gg = sm.grad[ty][tx];
-            const float glfx = (gl + gr) / 2.f, glfy = (gu + gd) / 2.f;
-            const float ghfx = ((cl + cr) - 2.f * cxy) / 4.f, ghfy = ((cu + cd) - 2.f * cxy) / 4.f;
-            const float sd = sqrtf(a.gv0 + a.gv1 * gave);
-            const float glen = sqrtf(gg.x * gg.x + gg.y * gg.y);
-            const float gthr = smoothstepf(sd, 4.f * sd, glen);
-            const float lowthr = 1.f - smoothstepf(2.f * sd, 8.f * sd, glen);
-            const float sharp = (0.5f + 0.5f * lowNoise) * gthr * (1.f + lowNoise * lowthr);
-            const float hl = 1.f - smoothstepf(0.25f, 1.f, fmaxf(cxy, fmaxf(fmaxf(cl, cr), fmaxf(cu, cd))));
-            float dir = 2.f * atan2f(gg.y, gg.x) / kPi;
-            if (a.gv1 < 1e-3f) {
-                dir = dir < 0.5f ? mixf(dir, 0.f, 1.f - smoothstepf(0.3f, 0.45f, dir))
-                                 : mixf(dir, 1.f, smoothstepf(1.f - 0.45f, 1.f - 0.3f, dir));
-            }
-            const float cmin = fminf(cxy, fminf(gave, c2ave)), cmax = fmaxf(cxy, fmaxf(gave, c2ave));
-            const float white = cmin / cmax;
-            const float k = hl * white * sharp;
-            const float gex = glfx - k * ghfx, gey = glfy - k * ghfy;
-            g = mixf(gey, gex, dir);
-            const float maxo = mixf(1.f, 1.5f, white), mino = mixf(1.f, 0.5f, white);
-            const float gmax = fmaxf(fmaxf(gl, gr), fmaxf(gu, gd));
-            const float gmin = fminf(fminf(gl, gr), fminf(gu, gd));
-            g = clampf(g, mino * gmin, maxo * gmax);
+    if (inner) {
+        // entry pairs (2k, 2k + 1) of a row: one red/blue site, one green site
+        for (int i = tid; i < (DM_GW / 2) * DM_GH; i += nth) {
+            const int ty = i / (DM_GW / 2), tx0 = 2 * (i % (DM_GW / 2));
+            const int py = y0 - 5 + ty;
+            const int trb = tx0 + (((x0 - 5 + tx0) ^ py ^ rb_par) & 1);  // the pair's red/blue entry
+            const int tg = tx0 + tx0 + 1 - trb;
+            sm.green[ty][tg] = sm.raw[ty + 2][tg + 2];
+            sm.green[ty][trb] = dm_green(sm, trb + 2, ty + 2, sm.grad[ty][trb], a, lowNoise);
         }
-        sm.green[ty][tx] = g;
+    } else {
+        for (int i = tid; i < DM_GW * DM_GH; i += nth) {
+            const int ty = i / DM_GW, tx = i % DM_GW;
+            const int px = clampi(x0 - 5 + tx, 0, W - 1), py = clampi(y0 - 5 + ty, 0, H - 1);
+            const int lx = px - (x0 - 7), ly = py - (y0 - 7);  // raw-tile index of the clamped position
+            sm.green[ty][tx] = (st.red(px, py) || st.blue(px, py)) ? dm_green(sm, lx, ly, sm.grad[ty][tx], a, lowNoise)
+                                                                   : sm.raw[ly][lx];
+        }
     }
     __syncthreads();
 
     // ---- red/blue temporary at the clamped position of every tmp-tile entry
-    for (int i = tid; i < DM_CW * DM_CH; i += nth) {
-        const int ty = i / DM_CW, tx = i % DM_CW;
-        const int px = clampi(x0 - 3 + tx, 0, W - 1), py = clampi(y0 - 3 + ty, 0, H - 1);
-        const int gx = px - (x0 - 5), gy = py - (y0 - 5);  // green-tile index
-        const int lx = px - (x0 - 7), ly = py - (y0 - 7);  // raw-tile index
-        const bool red = (rx & 1) == (px & 1) && (ry & 1) == (py & 1);
-        const bool blue = (bx & 1) == (px & 1) && (by & 1) == (py & 1);
-        float o0, o1, o2;
-        if (!(red || blue)) {
-            o0 = 0.f;
-            o1 = sm.green[gy][gx];
-            o2 = 0.f;
-        } else {
-            auto R = [&](int di, int dj) { return sm.raw[ly + dj][lx + di]; };
-            auto G = [&](int di, int dj) { return sm.green[gy + dj][gx + di]; };
-            const float g0 = G(0, 0), c1 = R(0, 0);
-            const float c2tl = R(-1, -1), c2tr = R(1, -1), c2bl = R(-1, 1), c2br = R(1, 1);
-            const float c2ave = (c2tl + c2tr + c2bl + c2br) / 4.f;
-            const float gctl = G(-1, -1) - c2tl, gctr = G(1, -1) - c2tr, gcbl = G(-1, 1) - c2bl, gcbr = G(1, 1) - c2br;
-            const float gtl2 = G(-2, -2), gtr2 = G(2, -2), gbl2 = G(-2, 2), gbr2 = G(2, 2);
-            const float gctl2 = gtl2 - R(-2, -2), gctr2 = gtr2 - R(2, -2), gcbl2 = gbl2 - R(-2, 2),
-                        gcbr2 = gbr2 - R(2, 2);
-            const float v0 = red ? a.rv0 : a.bv0, v1 = red ? a.rv1 : a.bv1;
-            const float sd = sqrtf(v0 + v1 * c2ave);
-            const float2 gg = sm.grad[gy][gx];
-            const float dir = 1.f - 2.f * atan2f(gg.y, gg.x) / kPi;
-            const float gthr = smoothstepf(sd, 4.f * sd, sqrtf(gg.x * gg.x + gg.y * gg.y));
-            const float alpha = mixf(0.5f, dir, gthr);
-            const float hl = 1.f - smoothstepf(0.25f, 1.f, fmaxf(g0, fmaxf(fmaxf(gtr2, gbl2), fmaxf(gtl2, gbr2))));
-            const float gc = g0 - c1;
-            const float aa = (gctr + gcbl) / 2.f + hl * (gctr2 + gcbl2 - 2.f * gc) / 8.f;
-            const float bb = (gctl + gcbr) / 2.f + hl * (gctl2 + gcbr2 - 2.f * gc) / 8.f;
-            float c2 = g0 - mixf(aa, bb, alpha);
-            const float c2max = fmaxf(fmaxf(c2tl, c2tr), fmaxf(c2bl, c2br));
-            const float c2min = fminf(fminf(c2tl, c2tr), fminf(c2bl, c2br));
-            c2 = clampf(c2, c2min, c2max);
-            if (red) {
-                o0 = c1; o1 = g0; o2 = c2;
-            } else {
-                o0 = c2; o1 = g0; o2 = c1;
-            }
+    if (inner) {
+        for (int i = tid; i < (DM_CW / 2) * DM_CH; i += nth) {
+            const int ty = i / (DM_CW / 2), tx0 = 2 * (i % (DM_CW / 2));
+            const int px0 = x0 - 3 + tx0, py = y0 - 3 + ty;
+            const int trb = tx0 + ((px0 ^ py ^ rb_par) & 1);
+            const int tg = tx0 + tx0 + 1 - trb;
+            const int prb = x0 - 3 + trb;
+            const bool red = st.red(prb, py);
+            sm.tmp[0][ty][tg] = 0.f;
+            sm.tmp[1][ty][tg] = sm.green[ty + 2][tg + 2];
+            sm.tmp[2][ty][tg] = 0.f;
+            const float c2 = dm_redblue(sm, trb + 2, ty + 2, trb + 4, ty + 4, red, a);
+            const float c1 = sm.raw[ty + 4][trb + 4];
+            sm.tmp[0][ty][trb] = red ? c1 : c2;
+            sm.tmp[1][ty][trb] = sm.green[ty + 2][trb + 2];
+            sm.tmp[2][ty][trb] = red ? c2 : c1;
         }
-        sm.tmp[0][ty][tx] = o0;
-        sm.tmp[1][ty][tx] = o1;
-        sm.tmp[2][ty][tx] = o2;
+    } else {
+        for (int i = tid; i < DM_CW * DM_CH; i += nth) {
+            const int ty = i / DM_CW, tx = i % DM_CW;
+            const int px = clampi(x0 - 3 + tx, 0, W - 1), py = clampi(y0 - 3 + ty, 0, H - 1);
+            const int gx = px - (x0 - 5), gy = py - (y0 - 5);  // green-tile index
+            const int lx = px - (x0 - 7), ly = py - (y0 - 7);  // raw-tile index
+            const bool red = st.red(px, py), blue = st.blue(px, py);
+            float o0, o1, o2;
+            if (!(red || blue)) {
+                o0 = 0.f;
+                o1 = sm.green[gy][gx];
+                o2 = 0.f;
+            } else {
+                const float c2 = dm_redblue(sm, gx, gy, lx, ly, red, a);
+                const float c1 = sm.raw[ly][lx];
+                o0 = red ? c1 : c2;
+                o1 = sm.green[gy][gx];
+                o2 = red ? c2 : c1;
+            }
+            sm.tmp[0][ty][tx] = o0;
+            sm.tmp[1][ty][tx] = o1;
+            sm.tmp[2][ty][tx] = o2;
+        }
     }
     __syncthreads();
 
-    // ---- red/blue at green sites, highlights, colour transform
-    for (int r = threadIdx.y; r < DM_TH; r += blockDim.y) {
-        const int x = x0 + threadIdx.x, y = y0 + r;
-        if (x >= W || y >= H) continue;
-        const int cx = threadIdx.x + 3, cy = r + 3;  // tmp-tile index of (x, y)
-        const bool red = (rx & 1) == (x & 1) && (ry & 1) == (y & 1);
-        const bool blue = (bx & 1) == (x & 1) && (by & 1) == (y & 1);
-        float rgb[3];
-        if (red || blue) {
-            rgb[0] = sm.tmp[0][cy][cx];
-            rgb[1] = sm.tmp[1][cy][cx];
-            rgb[2] = sm.tmp[2][cy][cx];
-        } else {
-            auto P = [&](int di, int dj, int c) { return sm.tmp[c][cy + dj][cx + di]; };
-            const float g0 = P(0, 0, 1);
-            const float lr = P(-1, 0, 0), lg = P(-1, 0, 1), lb = P(-1, 0, 2);
-            const float rr = P(1, 0, 0), rg = P(1, 0, 1), rb = P(1, 0, 2);
-            const float ur = P(0, -1, 0), ug = P(0, -1, 1), ub = P(0, -1, 2);
-            const float dr = P(0, 1, 0), dg = P(0, 1, 1), db = P(0, 1, 2);
-            const float red_ave = (lr + rr + ur + dr) / 4.f, blue_ave = (lb + rb + ub + db) / 4.f;
-            const float grl = lg - lr, grr = rg - rr, gru = ug - ur, grd = dg - dr;
-            const float gbl = lg - lb, gbr = rg - rb, gbu = ug - ub, gbd = dg - db;
-            const float grl3 = P(-3, 0, 1) - P(-3, 0, 0), grr3 = P(3, 0, 1) - P(3, 0, 0);
-            const float gru3 = P(0, -3, 1) - P(0, -3, 0), grd3 = P(0, 3, 1) - P(0, 3, 0);
-            const float gbl3 = P(-3, 0, 1) - P(-3, 0, 2), gbr3 = P(3, 0, 1) - P(3, 0, 2);
-            const float gbu3 = P(0, -3, 1) - P(0, -3, 2), gbd3 = P(0, 3, 1) - P(0, 3, 2);
-            const float2 gg = sm.grad[r + 5][threadIdx.x + 5];
-            const float dir = 2.f * atan2f(gg.y, gg.x) / kPi;
-            const float glen = sqrtf(gg.x * gg.x + gg.y * gg.y);
-            const float rsd = sqrtf(a.rv0 + a.rv1 * red_ave), bsd = sqrtf(a.bv0 + a.bv1 * blue_ave);
-            const float ralpha = mixf(0.5f, dir, smoothstepf(rsd, 4.f * rsd, glen));
-            const float balpha = mixf(0.5f, dir, smoothstepf(bsd, 4.f * bsd, glen));
-            const float hl = 1.f - smoothstepf(0.25f, 1.f, fmaxf(g0, fmaxf(fmaxf(rg, lg), fmaxf(dg, ug))));
-            const float red_v = g0 - mixf((gru + grd) / 2.f - hl * ((grd3 - gru) - (grd - gru3)) / 8.f,
-                                          (grl + grr) / 2.f - hl * ((grr3 - grl) - (grr - grl3)) / 8.f, ralpha);
-            const float blue_v = g0 - mixf((gbu + gbd) / 2.f - hl * ((gbd3 - gbu) - (gbd - gbu3)) / 8.f,
-                                           (gbl + gbr) / 2.f - hl * ((gbr3 - gbl) - (gbr - gbl3)) / 8.f, balpha);
-            rgb[0] = clampf(red_v, fminf(fminf(lr, rr), fminf(ur, dr)), fmaxf(fmaxf(lr, rr), fmaxf(ur, dr)));
-            rgb[1] = g0;
-            rgb[2] = clampf(blue_v, fminf(fminf(lb, rb), fminf(ub, db)), fmaxf(fmaxf(lb, rb), fmaxf(ub, db)));
+    // ---- red/blue at green sites, highlights, colour transform: a lane
+    //      takes the pixel pair (2k, 2k + 1) of a tile row
+    for (int i = tid; i < (DM_TW / 2) * DM_TH; i += nth) {
+        const int r = i / (DM_TW / 2), c0 = 2 * (i % (DM_TW / 2));
+        const int y = y0 + r;
+        if (y >= H) continue;
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            // the pair's green site first, so both lanes of a warp branch alike
+            const int cg = c0 + (((x0 + c0) ^ y ^ rb_par ^ 1) & 1);
+            const int c = e == 0 ? cg : c0 + c0 + 1 - cg;
+            const int x = x0 + c;
+            if (x >= W) continue;
+            const int cx = c + 3, cy = r + 3;  // tmp-tile index of (x, y)
+            float rgb[3];
+            if (st.red(x, y) || st.blue(x, y)) {
+                rgb[0] = sm.tmp[0][cy][cx];
+                rgb[1] = sm.tmp[1][cy][cx];
+                rgb[2] = sm.tmp[2][cy][cx];
+            } else {
+                dm_rb_at_green(sm, cx, cy, sm.grad[r + 5][c + 5], a, rgb);
+            }
+            st4<S>(out.px(x, y), dm_finish(rgb, a));
         }
-        // blendHighlightsImage, clip = 1
-        const float clip = 1.f;
-        if (rgb[0] > clip || rgb[1] > clip || rgb[2] > clip) {
-            const float s3 = 1.7320508f;
-            const float c0[3] = {rgb[0], rgb[1], rgb[2]};
-            const float c1[3] = {fminf(rgb[0], clip), fminf(rgb[1], clip), fminf(rgb[2], clip)};
-            const float l0x = c0[0] + c0[1] + c0[2], l0y = s3 * c0[0] - s3 * c0[1], l0z = -c0[0] - c0[1] + 2.f * c0[2];
-            const float l1y = s3 * c1[0] - s3 * c1[1], l1z = -c1[0] - c1[1] + 2.f * c1[2];
-            const float sum0 = l0y * l0y + l0z * l0z, sum1 = l1y * l1y + l1z * l1z;
-            const float chr = sum0 > 0.f ? sqrtf(sum1 / sum0) : 1.f;
-            const float ly = l0y * chr, lz = l0z * chr;
-            rgb[0] = (l0x + (s3 / 2.f) * ly - 0.5f * lz) / 3.f;
-            rgb[1] = (l0x - (s3 / 2.f) * ly - 0.5f * lz) / 3.f;
-            rgb[2] = (l0x + lz) / 3.f;
-        }
-        f4 o;
-        if (a.transform) {
-            o.x = a.m[0] * rgb[0] + a.m[1] * rgb[1] + a.m[2] * rgb[2];
-            o.y = a.m[3] * rgb[0] + a.m[4] * rgb[1] + a.m[5] * rgb[2];
-            o.z = a.m[6] * rgb[0] + a.m[7] * rgb[1] + a.m[8] * rgb[2];
-        } else {
-            o.x = rgb[0]; o.y = rgb[1]; o.z = rgb[2];
-        }
-        o.w = 0.f;
-        st4<S>(out.px(x, y), o);
     }
 }
 
