@@ -36,6 +36,7 @@ HOST_IO = 1 << 3
 SYNC = 1 << 4
 GRAPH = 1 << 6
 SURF_CORRECTED = 1 << 7
+PERSISTENT = 1 << 8
 HOST_PCA = 1 << 5
 
 PLANE_SCALED_RAW = 0
@@ -169,6 +170,7 @@ _SIGNATURES = {
     "gls_last_error_message": (C.c_char_p, []),
     "gls_version": (C.c_char_p, []),
     "gls_device_memory": (C.c_int, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_int32]),
+    "gls_persistent_selftest": (C.c_int, [C.c_int32, C.c_int64, C.POINTER(C.c_int32)]),
     "gls_converter_create": (C.c_int, [C.c_int32, C.c_void_p, C.c_size_t, C.c_int32, C.POINTER(C.c_void_p)]),
     "gls_converter_destroy": (C.c_int, [C.c_void_p]),
     "gls_demosaic": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_size_t,

@@ -22,6 +22,7 @@
 
 #include "gls_common.cuh"
 #include "gls_kernels.h"
+#include "gls_pyramid_dev.cuh"
 
 namespace gls {
 
@@ -503,6 +504,8 @@ struct BmMmaSmem {
     float lswy[32];              // -log2 of the spatial weight's y part, dy = -13..13 (+inf outside +-10)
     __half swy[32];              // its y part / sqrt(lk) (0 outside)
     __half luma[BM_LW * BM_LW];  // the luma tile of the projection patches, origin (x0 - 12, y0 - 12)
+    float cen[8];                // the centring vector
+    float bsm[25][8];            // the level's basis
 };
 
 __device__ __forceinline__ uint32_t cvt_h2(float lo, float hi) {
@@ -569,14 +572,12 @@ __device__ __forceinline__ void bm_weights(const BmRow& R, float s0, float s1, u
     wy = hmul2_u(lws, swp);                           // sw lw
 }
 
-__global__ void __launch_bounds__(BM_THREADS, 2)
-    k_block_match_mma(Plane<__half, 4> img, Plane<__half, 2> grad, const float* __restrict__ basis,
-                      Plane<__half, 4> out, BlockMatchArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    BmMmaSmem& sm = *reinterpret_cast<BmMmaSmem*>(smem_raw);
-    __shared__ float cen[8];
-    __shared__ float bsm[25][8];
-    const int x0 = blockIdx.x * BM_T, y0 = blockIdx.y * BM_T;
+// One 32 x 32 tile (origin x0, y0) by a block of BM_THREADS threads.
+__device__ __forceinline__ void bm_mma_tile(int x0, int y0, const Plane<__half, 4>& img, const Plane<__half, 2>& grad,
+                                            const float* __restrict__ basis, const Plane<__half, 4>& out,
+                                            const BlockMatchArgs& a, BmMmaSmem& sm) {
+    float* cen = sm.cen;
+    float (*bsm)[8] = sm.bsm;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
     const float kLog2e = 1.4426950408889634f, lk = 2.f * kLog2e, isq = rsqrtf(lk);
     // ---- staging: spatial y table, basis, luma tile, Y/Cb/Cr of the window region
@@ -757,11 +758,162 @@ __global__ void __launch_bounds__(BM_THREADS, 2)
     }
 }
 
+__global__ void __launch_bounds__(BM_THREADS, 2)
+    k_block_match_mma(Plane<__half, 4> img, Plane<__half, 2> grad, const float* __restrict__ basis,
+                      Plane<__half, 4> out, BlockMatchArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    bm_mma_tile(blockIdx.x * BM_T, blockIdx.y * BM_T, img, grad, basis, out, a,
+                *reinterpret_cast<BmMmaSmem*>(smem_raw));
+}
+
 static void launch_mma(Plane<__half, 4> img, Plane<__half, 2> grad, const float* basis, Plane<__half, 4> out,
                        const BlockMatchArgs& a, cudaStream_t s) {
     ensure_dynamic_smem(reinterpret_cast<const void*>(k_block_match_mma), int(sizeof(BmMmaSmem)));
     dim3 g((img.w + BM_T - 1) / BM_T, (img.h + BM_T - 1) / BM_T);
     k_block_match_mma<<<g, BM_THREADS, sizeof(BmMmaSmem), s>>>(img, grad, basis, out, a);
+}
+
+// ============================================================ persistent batch kernel
+// PyramidProcessor::denoise (pyramid_processor.cpp:96-172) for every frame
+// of a batch in one launch. The host lists the work of every (frame,
+// level) as tasks: reconstruct tiles (SN, 32 x 32 pixels), covariance
+// partial rows (COV), the eigen-solve (EIG) and block-matching tiles (BM,
+// 32 x 32), level by level from the coarsest, all frames' SN / COV / EIG of
+// a level before their BM tiles. A block takes the next task from a
+// counter, waits until the task's inputs are complete, runs it with the
+// same device code as the stream kernels (so the results are
+// bit-identical), and counts it done:
+//   SN (f, l)  waits for every BM tile of (f, l + 1)  (the coarse denoised image)
+//   COV (f, l) waits for every SN tile of (f, l)      (the layer)
+//   EIG (f, l) waits for every COV row of (f, l)
+//   BM (f, l)  waits for EIG (f, l)                   (the basis; the layer before it)
+// Every task a block waits for comes earlier in the list and was taken by a
+// running block, so the earliest unfinished task can always run: the order
+// cannot deadlock, and the blocks need not be co-resident. A wait is
+// bounded: past limit_ns (global timer) the block records the task type
+// in *err and every block stops taking tasks; the host reads the word and
+// returns GLS_ERR_TIMEOUT.
+struct PSmem {
+    union {
+        BmMmaSmem bm;
+        EigenSmem eig;
+        CovSmem cov;
+    };
+};
+
+__device__ __forceinline__ long long global_ns() {
+    long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// the rarely taken eigen-solve as a call of its own, so that its registers
+// do not weigh on the block-matching path
+__device__ __noinline__ void persistent_eigen(const PLevel& L, EigenSmem& sm) {
+    pca_eigen_block(L.part, L.n_cov, (L.layer.w / 8) * (L.layer.h / 8), L.basis, L.status, sm);
+}
+
+__global__ void __launch_bounds__(BM_THREADS, 2)
+    k_pyramid_persistent(const PTask* __restrict__ tasks, int n_tasks, const PLevel* __restrict__ lv,
+                         PCounters* __restrict__ cnt, int* __restrict__ next, int* __restrict__ err, long long limit_ns) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    PSmem& sm = *reinterpret_cast<PSmem*>(smem_raw);
+    __shared__ int s_task, s_ok;
+    for (;;) {
+        if (threadIdx.x == 0) s_task = ld_acquire(err) ? n_tasks : atomicAdd(next, 1);
+        __syncthreads();
+        const int ti = s_task;
+        if (ti >= n_tasks) break;
+        const PTask tk = tasks[ti];
+        const uint32_t type = tk.item >> 30, item = tk.item & kPTaskItemMask;
+        const PLevel& L = lv[tk.lev];
+        if (threadIdx.x == 0) {
+            // the counter this task waits on and its target (none: -1)
+            const int* c = nullptr;
+            int target = 0;
+            if (type == PT_SN) {
+                c = &cnt[L.coarser].bm;
+                target = lv[L.coarser].n_bm;
+            } else if (type == PT_COV) {
+                if (L.n_sn > 0) {
+                    c = &cnt[tk.lev].sn;
+                    target = L.n_sn;
+                }
+            } else if (type == PT_EIG) {
+                c = &cnt[tk.lev].cov;
+                target = L.n_cov;
+            } else {
+                c = &cnt[tk.lev].eig;
+                target = 1;
+            }
+            int ok = 1;
+            if (c && ld_acquire(c) < target) {
+                const long long t0 = global_ns();
+                unsigned ns = 32;
+                while (ld_acquire(c) < target) {
+                    if (ld_acquire(err) || global_ns() - t0 > limit_ns) {
+                        atomicCAS(err, 0, int(1 + type));
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(ns);
+                    ns = ns < 2048 ? 2 * ns : ns;
+                }
+            }
+            __threadfence();
+            s_ok = ok;
+        }
+        __syncthreads();
+        if (!s_ok) break;
+        int* done;
+        if (type == PT_SN) {
+            const int tx = item % L.tiles_x, ty = item / L.tiles_x;
+            for (int k = threadIdx.x; k < BM_T * BM_T; k += BM_THREADS) {
+                const int x = tx * BM_T + k % BM_T, y = ty * BM_T + k / BM_T;
+                if (x < L.img.w && y < L.img.h)
+                    subtract_noise_px<__half>(L.img, L.coarse, L.coarse_den, L.grad, L.layer, L.sa, L.rx, L.ry, x, y);
+            }
+            done = &cnt[tk.lev].sn;
+        } else if (type == PT_COV) {
+            const int c0 = int(item) * kPcaCovGroup;
+            pca_cov_row<__half>(L.layer, L.part + size_t(item) * kPcaAcc, c0, min(c0 + kPcaCovGroup, L.chunks), sm.cov);
+            done = &cnt[tk.lev].cov;
+        } else if (type == PT_EIG) {
+            persistent_eigen(L, sm.eig);
+            done = &cnt[tk.lev].eig;
+        } else {
+            const int tx = item % L.tiles_x, ty = item / L.tiles_x;
+            bm_mma_tile(tx * BM_T, ty * BM_T, L.layer, L.grad, L.basis, L.den, L.ba, sm.bm);
+            done = &cnt[tk.lev].bm;
+        }
+        __syncthreads();  // the task's writes, and its shared memory, are finished
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(done, 1);
+        }
+    }
+}
+
+int persistent_grid(int device) {
+    ensure_dynamic_smem(reinterpret_cast<const void*>(k_pyramid_persistent), int(sizeof(PSmem)));
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pyramid_persistent, BM_THREADS, sizeof(PSmem)) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+        return 0;
+    return per_sm * sms;
+}
+
+void launch_pyramid_persistent(const PTask* tasks, int n, const PLevel* lv, PCounters* cnt, int* next, int* err,
+                               long long limit_ns, int grid, cudaStream_t s) {
+    ensure_dynamic_smem(reinterpret_cast<const void*>(k_pyramid_persistent), int(sizeof(PSmem)));
+    k_pyramid_persistent<<<grid, BM_THREADS, sizeof(PSmem), s>>>(tasks, n, lv, cnt, next, err, limit_ns);
 }
 
 // Tile-height autotuner of the FP16 block matcher. Both heights compute

@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <set>
 #include <string>
@@ -77,6 +78,7 @@ struct Pipeline {
     DevBuf img[GLS_MAX_LEVELS], gradp[GLS_MAX_LEVELS], den[GLS_MAX_LEVELS], layer;
     DevBuf nc[GLS_MAX_LEVELS];  // chroma norms, kept only for the adjoint
     DevBuf out_f32, out_f16, stage_in, stage_grad;
+    size_t acc_off[GLS_MAX_LEVELS] = {};  // per level: the first covariance partial (doubles into acc)
     std::vector<double> host_acc;
     std::vector<float> host_basis;
 
@@ -90,7 +92,12 @@ struct Pipeline {
         GLS_TRY(B.ensure(n * 4 * sizeof(S)));
         GLS_TRY(pca.ensure(n * 8 * sizeof(S)));
         GLS_TRY(layer.ensure(n * 4 * sizeof(S)));
-        GLS_TRY(acc.ensure(sizeof(double) * kPcaAcc * kPcaMaxBlocks * GLS_MAX_LEVELS));
+        size_t rows = 0;
+        for (int i = 0; i < levels; i++) {
+            acc_off[i] = rows * kPcaAcc;
+            rows += size_t(pca_cov_rows(w >> i, h >> i));
+        }
+        GLS_TRY(acc.ensure(sizeof(double) * kPcaAcc * std::max<size_t>(rows, 1)));
         GLS_TRY(basis.ensure(sizeof(float) * 200 * GLS_MAX_LEVELS));
         GLS_TRY(status.ensure(sizeof(int) * GLS_MAX_LEVELS));
         for (int i = 0; i < levels; i++) {
@@ -127,11 +134,13 @@ namespace gls {
 // kernel classes for launch accounting
 enum KernelClass {
     KC_SCALE, KC_SOBEL_BLUR, KC_RAW_DENOISE, KC_DEMOSAIC, KC_DESPECKLE, KC_DOWNSAMPLE, KC_SUBTRACT,
-    KC_PCA_COV, KC_PCA_EIGEN, KC_PCA_PROJECT, KC_BLOCK_MATCH, KC_OUTPUT, KC_VIEW_IN, KC_POST, KC_NLF, KC_COUNT
+    KC_PCA_COV, KC_PCA_EIGEN, KC_PCA_PROJECT, KC_BLOCK_MATCH, KC_OUTPUT, KC_VIEW_IN, KC_POST, KC_NLF,
+    KC_PERSISTENT, KC_COUNT
 };
 static const char* const kKcNames[KC_COUNT] = {
     "scale_raw", "sobel_blur", "raw_quad_denoise", "demosaic", "despeckle", "downsample", "subtract_noise",
-    "pca_cov", "pca_eigen", "pca_project", "block_match", "output_transform", "view_in", "post_process", "noise_model"};
+    "pca_cov", "pca_eigen", "pca_project", "block_match", "output_transform", "view_in", "post_process", "noise_model",
+    "pyramid_persistent"};
 
 struct Prof {
     bool on = false;
@@ -220,6 +229,13 @@ struct gls_converter {
     // the last GLS_GRAPH batch: its signature and executable graph
     std::vector<uint64_t> graph_key;
     cudaGraphExec_t graph_exec = nullptr;
+    bool graph_persistent = false;  // the recorded batch reads the persistent kernel's error word
+    // GLS_PERSISTENT batches: a pyramid per frame, the work list of the last
+    // batch (its signature, descriptors, tasks) and the kernel's counters
+    std::vector<std::unique_ptr<Pipeline<__half>>> pframes;
+    std::vector<uint64_t> plan_key;
+    int plan_tasks = 0, plan_levels = 0, plan_grid = 0;
+    DevBuf plan_task_buf, plan_level_buf, plan_cnt, plan_ctl;  // ctl: next, err
     // adjoint scratch (gls_demosaic_denoise_vjp)
     DevBuf adj_gden[2], adj_rec, adj_glayer, adj_gpca, adj_gup, adj_part, adj_loss, adj_target;
     DevBuf adj_gimg, adj_gp1, adj_jvp, adj_jvp_part;  // dL/d(input pyramid), front-end tangents
@@ -356,7 +372,7 @@ static gls_status measure_ycc_nlf(gls_converter* cv, Plane<S, 4> img, float expo
 
 template <class S>
 static gls_status pyramid_run(gls_converter* cv, Pipeline<S>& P, Plane<S, 4> img0, Plane<S, 2> grad0,
-                              const gls_demosaic_params* p, uint32_t flags, cudaStream_t s) {
+                              const gls_demosaic_params* p, uint32_t flags, cudaStream_t s, bool build_only = false) {
     const int L = p->levels;
     const int W = img0.w, H = img0.h;
     Plane<S, 4> img[GLS_MAX_LEVELS];
@@ -370,6 +386,7 @@ static gls_status pyramid_run(gls_converter* cv, Pipeline<S>& P, Plane<S, 4> img
         launch_downsample<S, 4>(img[i - 1], img[i], s);
         launch_downsample<S, 2>(grd[i - 1], grd[i], s);
     }
+    if (build_only) return GLS_OK;  // the levels run in the persistent batch kernel
     gls_demosaic_params measured;
     if (cv->calibrate) {  // each level's model, measured before the denoise (pyramid_processor.cpp:113-117)
         measured = *p;
@@ -399,8 +416,8 @@ static gls_status pyramid_run(gls_converter* cv, Pipeline<S>& P, Plane<S, 4> img
                                      layer, sa, s);
         }
         const int n_patches = (wi / 8) * (hi / 8);
-        const int n_blocks = pca_cov_blocks(wi, hi);
-        double* part = acc + size_t(i) * kPcaAcc * kPcaMaxBlocks;
+        const int n_blocks = pca_cov_rows(wi, hi);
+        double* part = acc + P.acc_off[i];
         {
             KScope k(cv->prof, KC_PCA_COV, s, n_blocks > 0 ? 1 : 0);
             launch_pca_cov<S>(layer, part, s);
@@ -547,15 +564,35 @@ static DemosaicArgs demosaic_args(const gls_demosaic_params* p, bool transform) 
     return da;
 }
 
+// Stages of a frame: the whole frame, or (persistent batches) the front end
+// and the pyramid's images only, or the output only (after the levels).
+enum { STAGE_ALL = 0, STAGE_FRONT = 1, STAGE_OUTPUT = 2 };
+
 template <class S>
 static gls_status demosaic_run(gls_converter* cv, const uint16_t* raw, int w, int h, size_t stride_bytes,
                                const gls_demosaic_params* p, uint32_t flags, gls_image_view* out, cudaStream_t s,
-                               int slot = 0, const SlotCopies* cp = nullptr) {
-    Pipeline<S>& P =
-        *reinterpret_cast<Pipeline<S>*>(is_half<S>::value ? (void*)&cv->p16s[slot] : (void*)&cv->p32s[slot]);
+                               int slot = 0, const SlotCopies* cp = nullptr, int stage = STAGE_ALL,
+                               Pipeline<S>* use = nullptr) {
+    Pipeline<S>& P = use ? *use
+                         : *reinterpret_cast<Pipeline<S>*>(is_half<S>::value ? (void*)&cv->p16s[slot]
+                                                                            : (void*)&cv->p32s[slot]);
     const bool host_io = flags & GLS_HOST_IO;
     const bool denoise = flags & GLS_DENOISE;
     GLS_TRY(P.ensure(w, h, p->levels));
+    if (stage == STAGE_OUTPUT) {  // the levels are done: transformImage(YCbCr -> cam) of level 0
+        float c2y[9], y2c[9];
+        cam_ycbcr(p->rgb_cam, p->xyz_rgb, c2y, y2c);
+        const Plane<S, 4> den0 = plane<S, 4>(P.den[0], w, h);
+        if (out->dtype == GLS_F16) {
+            OutTarget<__half> t;
+            GLS_TRY(make_target<S, __half>(P, out, w, h, host_io, t));
+            return finish_output<S, __half>(cv, den0, true, y2c, t, s, cp, nullptr);
+        }
+        out->dtype = GLS_F32;
+        OutTarget<float> t;
+        GLS_TRY(make_target<S, float>(P, out, w, h, host_io, t));
+        return finish_output<S, float>(cv, den0, true, y2c, t, s, cp, nullptr);
+    }
 
     // raw input
     const uint16_t* rawp = raw;
@@ -663,7 +700,8 @@ static gls_status demosaic_run(gls_converter* cv, const uint16_t* raw, int w, in
             KScope k(cv->prof, KC_DESPECKLE, s);
             launch_despeckle<S>(A, B, p->pyramid_nlf[0].a[0], p->pyramid_nlf[0].b[0], s);
         }
-        GLS_TRY(pyramid_run<S>(cv, P, B, grad, p, flags, s));
+        GLS_TRY(pyramid_run<S>(cv, P, B, grad, p, flags, s, stage == STAGE_FRONT));
+        if (stage == STAGE_FRONT) return GLS_OK;
         final_src = plane<S, 4>(P.den[0], w, h);
         if (cv->calibrate)  // the post-processing reads the measured level-0 model
             for (int i = 0; i < p->levels; i++) calibrated.pyramid_nlf[i] = cv->nlf_pyr[i];
@@ -986,9 +1024,172 @@ static std::vector<uint64_t> batch_key(const gls_frame_desc* frames, int n, uint
     return k;
 }
 
+// The work list of a persistent batch: a descriptor per (frame, level) and
+// the tasks, level by level from the coarsest, all frames' reconstruct /
+// covariance / eigen-solve tasks of a level before their block-matching
+// tiles (the order the kernel's dependency waits rely on).
+static gls_status persistent_plan(gls_converter* conv, const gls_frame_desc* frames, int n) {
+    std::vector<PLevel> lv;
+    std::vector<int> first(n);  // descriptor index of each frame's level 0
+    int max_levels = 0;
+    for (int f = 0; f < n; f++) {
+        const gls_demosaic_params* p = frames[f].params;
+        Pipeline<__half>& P = *conv->pframes[f];
+        const int W = frames[f].width, H = frames[f].height, L = p->levels;
+        max_levels = std::max(max_levels, L);
+        first[f] = int(lv.size());
+        for (int i = 0; i < L; i++) {
+            const int wi = W >> i, hi = H >> i;
+            PLevel d{};
+            d.img = i == 0 ? plane<__half, 4>(P.B, W, H) : plane<__half, 4>(P.img[i], wi, hi);
+            d.grad = i == 0 ? plane<__half, 2>(P.grad, W, H) : plane<__half, 2>(P.gradp[i], wi, hi);
+            d.layer = i < L - 1 ? plane<__half, 4>(P.layer, wi, hi) : d.img;
+            d.den = plane<__half, 4>(P.den[i], wi, hi);
+            if (i < L - 1) {
+                const int cw = W >> (i + 1), ch = H >> (i + 1);
+                d.coarse = plane<__half, 4>(P.img[i + 1], cw, ch);
+                d.coarse_den = plane<__half, 4>(P.den[i + 1], cw, ch);
+                d.rx = float(cw) / float(wi);
+                d.ry = float(ch) / float(hi);
+            }
+            const gls_denoise_params& dp = p->denoise[i];
+            d.sa.luma_weight = 1.f;  // lumaDenoiseWeight, pyramid_processor.cpp:93
+            d.sa.sharpening = dp.sharpening;
+            d.sa.nlf_a = p->pyramid_nlf[i].a[0] * dp.luma;
+            d.sa.nlf_b = p->pyramid_nlf[i].b[0] * dp.luma;
+            for (int c = 0; c < 3; c++) {
+                d.ba.var_a[c] = p->pyramid_nlf[i].a[c];
+                d.ba.var_b[c] = p->pyramid_nlf[i].b[c];
+            }
+            d.ba.tm[0] = dp.luma;
+            d.ba.tm[1] = dp.chroma;
+            d.ba.tm[2] = dp.chroma;
+            d.ba.chroma_boost = dp.chroma_boost;
+            d.ba.gradient_boost = dp.gradient_boost;
+            d.ba.gradient_threshold = dp.gradient_threshold;
+            d.ba.lsc = p->lens_shading_correction;
+            d.ba.nc_out = nullptr;
+            d.part = static_cast<double*>(P.acc.p) + P.acc_off[i];
+            d.basis = static_cast<float*>(P.basis.p) + i * 200;
+            d.status = static_cast<int*>(P.status.p) + i;
+            d.tiles_x = (wi + 31) / 32;
+            const int tiles = d.tiles_x * ((hi + 31) / 32);
+            d.n_bm = tiles;
+            d.n_sn = i < L - 1 ? tiles : 0;
+            d.n_cov = pca_cov_rows(wi, hi);
+            d.chunks = pca_cov_chunks(wi, hi);
+            d.coarser = i < L - 1 ? first[f] + i + 1 : -1;
+            lv.push_back(d);
+        }
+    }
+    std::vector<PTask> tasks;
+    auto put = [&](int lev, uint32_t type, int count) {
+        for (int k = 0; k < count; k++) tasks.push_back({uint32_t(lev), (type << 30) | uint32_t(k)});
+    };
+    for (int i = max_levels - 1; i >= 0; i--) {
+        for (int f = 0; f < n; f++) {
+            if (i >= frames[f].params->levels) continue;
+            const int lev = first[f] + i;
+            put(lev, PT_SN, lv[lev].n_sn);
+            put(lev, PT_COV, lv[lev].n_cov);
+            put(lev, PT_EIG, 1);
+        }
+        for (int f = 0; f < n; f++)
+            if (i < frames[f].params->levels) put(first[f] + i, PT_BM, lv[first[f] + i].n_bm);
+    }
+    GLS_TRY(conv->plan_task_buf.ensure(tasks.size() * sizeof(PTask)));
+    GLS_TRY(conv->plan_level_buf.ensure(lv.size() * sizeof(PLevel)));
+    GLS_TRY(conv->plan_cnt.ensure(lv.size() * sizeof(PCounters)));
+    GLS_TRY(conv->plan_ctl.ensure(2 * sizeof(int)));
+    GLS_CUDA(cudaMemcpy(conv->plan_task_buf.p, tasks.data(), tasks.size() * sizeof(PTask), cudaMemcpyHostToDevice));
+    GLS_CUDA(cudaMemcpy(conv->plan_level_buf.p, lv.data(), lv.size() * sizeof(PLevel), cudaMemcpyHostToDevice));
+    conv->plan_tasks = int(tasks.size());
+    conv->plan_levels = int(lv.size());
+    return GLS_OK;
+}
+
+// Wait limit of the persistent kernel's dependency waits: far above any
+// level's duration (a dependency is at most one level of the batch away).
+constexpr long long kPersistentWaitNs = 2000000000ll;
+
+// A persistent batch: every frame's front end and pyramid images on the
+// slot streams (frames LPT-assigned as in enqueue_batch, each into a
+// pyramid of its own), then one launch for every level of every frame,
+// then every frame's output transform.
+static gls_status persistent_batch(gls_converter* conv, gls_frame_desc* frames, int n, uint32_t flags, cudaStream_t s,
+                                   const std::vector<int>& order, const std::vector<int>& slot_of, int nslots,
+                                   bool capturing) {
+    while (int(conv->pframes.size()) < n) conv->pframes.push_back(std::make_unique<Pipeline<__half>>());
+    GLS_CUDA(cudaEventRecord(conv->fork_ev, s));
+    for (int k = 0; k < nslots; k++) GLS_CUDA(cudaStreamWaitEvent(conv->slot_stream[k], conv->fork_ev, 0));
+    gls_status result = GLS_OK;
+    for (int oi = 0; oi < n && result == GLS_OK; oi++) {
+        const int i = order[oi];
+        gls_frame_desc& f = frames[i];
+        result = demosaic_run<__half>(conv, f.raw, f.width, f.height, f.raw_stride_bytes, f.params, flags, &f.out,
+                                      conv->slot_stream[slot_of[i]], slot_of[i], nullptr, STAGE_FRONT,
+                                      conv->pframes[i].get());
+    }
+    for (int k = 0; k < nslots; k++) {
+        GLS_CUDA(cudaEventRecord(conv->join_ev[k], conv->slot_stream[k]));
+        GLS_CUDA(cudaStreamWaitEvent(s, conv->join_ev[k], 0));
+    }
+    GLS_TRY(result);
+    // the work list: rebuilt when the batch changes (never while capturing:
+    // a recording runs right after an identical run)
+    std::vector<uint64_t> key = batch_key(frames, n, flags);
+    if (key.empty() || key != conv->plan_key) {
+        if (capturing) return set_error(GLS_ERR_INVALID_ARG, "persistent batch plan changed during capture");
+        GLS_TRY(persistent_plan(conv, frames, n));
+        conv->plan_key = key;
+        conv->plan_grid = persistent_grid(conv->device);
+        if (conv->plan_grid <= 0) return set_error(GLS_ERR_CUDA, "persistent kernel occupancy query failed");
+    }
+    GLS_CUDA(cudaMemsetAsync(conv->plan_cnt.p, 0, size_t(conv->plan_levels) * sizeof(PCounters), s));
+    GLS_CUDA(cudaMemsetAsync(conv->plan_ctl.p, 0, 2 * sizeof(int), s));
+    {
+        KScope k(conv->prof, KC_PERSISTENT, s);
+        int* ctl = static_cast<int*>(conv->plan_ctl.p);
+        launch_pyramid_persistent(static_cast<const PTask*>(conv->plan_task_buf.p), conv->plan_tasks,
+                                  static_cast<const PLevel*>(conv->plan_level_buf.p),
+                                  static_cast<PCounters*>(conv->plan_cnt.p), ctl, ctl + 1, kPersistentWaitNs,
+                                  conv->plan_grid, s);
+    }
+    GLS_CUDA(cudaGetLastError());
+    // outputs on the slot streams again
+    GLS_CUDA(cudaEventRecord(conv->fork_ev, s));
+    for (int k = 0; k < nslots; k++) GLS_CUDA(cudaStreamWaitEvent(conv->slot_stream[k], conv->fork_ev, 0));
+    for (int oi = 0; oi < n && result == GLS_OK; oi++) {
+        const int i = order[oi];
+        gls_frame_desc& f = frames[i];
+        result = demosaic_run<__half>(conv, f.raw, f.width, f.height, f.raw_stride_bytes, f.params, flags, &f.out,
+                                      conv->slot_stream[slot_of[i]], slot_of[i], nullptr, STAGE_OUTPUT,
+                                      conv->pframes[i].get());
+    }
+    for (int k = 0; k < nslots; k++) {
+        GLS_CUDA(cudaEventRecord(conv->join_ev[k], conv->slot_stream[k]));
+        GLS_CUDA(cudaStreamWaitEvent(s, conv->join_ev[k], 0));
+    }
+    return result;
+}
+
+// The persistent kernel's error word after its batch (synchronises s).
+static gls_status persistent_status(gls_converter* conv, cudaStream_t s) {
+    int ctl[2] = {0, 0};
+    GLS_CUDA(cudaMemcpyAsync(ctl, conv->plan_ctl.p, sizeof(ctl), cudaMemcpyDeviceToHost, s));
+    GLS_CUDA(cudaStreamSynchronize(s));
+    if (ctl[1]) {
+        static const char* const kTypes[4] = {"reconstruct", "covariance", "eigen-solve", "block-matching"};
+        return set_error(GLS_ERR_TIMEOUT, "persistent batch: a %s task waited past the limit for its inputs",
+                         kTypes[(ctl[1] - 1) & 3]);
+    }
+    return GLS_OK;
+}
+
 // Frames to slot streams, largest first onto the least-loaded slot (the
 // longest-processing-time rule), then the fork / per-slot runs / join on s.
-static gls_status enqueue_batch(gls_converter* conv, gls_frame_desc* frames, int n, uint32_t flags, cudaStream_t s) {
+static gls_status enqueue_batch(gls_converter* conv, gls_frame_desc* frames, int n, uint32_t flags, cudaStream_t s,
+                                bool capturing = false) {
     const int nslots = n < kSlots ? n : kSlots;
     std::vector<int> order(n), slot_of(n);
     for (int i = 0; i < n; i++) order[i] = i;
@@ -1003,6 +1204,7 @@ static gls_status enqueue_batch(gls_converter* conv, gls_frame_desc* frames, int
         slot_of[i] = k;
         load[k] += size_t(frames[i].width) * frames[i].height;
     }
+    if (flags & GLS_PERSISTENT) return persistent_batch(conv, frames, n, flags, s, order, slot_of, nslots, capturing);
     const bool host_io = flags & GLS_HOST_IO;
     std::vector<SlotCopies> cps(nslots);
     GLS_CUDA(cudaEventRecord(conv->fork_ev, s));
@@ -1045,6 +1247,45 @@ const char* gls_last_error_message(void) { return g_last_error.c_str(); }
 
 const char* gls_version(void) {
     return "glscam 0.1 (sm_100a; demosaic, pyramid PCA block-matching denoise)";
+}
+
+gls_status gls_persistent_selftest(int32_t device, int64_t limit_ns, int32_t* err_word) {
+    clear_error();
+    if (limit_ns <= 0 || limit_ns > 10000000000ll) return set_error(GLS_ERR_INVALID_ARG, "limit_ns out of range");
+    GLS_CUDA(cudaSetDevice(device));
+    // one eigen-solve task of a level that lists one covariance row but
+    // no covariance task: its count never arrives
+    PLevel lv{};
+    lv.n_cov = 1;
+    lv.coarser = -1;
+    const PTask task{0u, uint32_t(PT_EIG) << 30};
+    DevBuf b_lv, b_task, b_cnt, b_ctl;
+    gls_status st = b_lv.ensure(sizeof(PLevel));
+    if (st == GLS_OK) st = b_task.ensure(sizeof(PTask));
+    if (st == GLS_OK) st = b_cnt.ensure(sizeof(PCounters));
+    if (st == GLS_OK) st = b_ctl.ensure(2 * sizeof(int));
+    int ctl[2] = {0, 0};
+    cudaError_t e = cudaSuccess;
+    if (st == GLS_OK) {
+        e = cudaMemcpy(b_lv.p, &lv, sizeof(lv), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(b_task.p, &task, sizeof(task), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemset(b_cnt.p, 0, sizeof(PCounters));
+        if (e == cudaSuccess) e = cudaMemset(b_ctl.p, 0, 2 * sizeof(int));
+        if (e == cudaSuccess) {
+            int* c = static_cast<int*>(b_ctl.p);
+            launch_pyramid_persistent(static_cast<const PTask*>(b_task.p), 1, static_cast<const PLevel*>(b_lv.p),
+                                      static_cast<PCounters*>(b_cnt.p), c, c + 1, limit_ns, 1, nullptr);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaMemcpy(ctl, b_ctl.p, sizeof(ctl), cudaMemcpyDeviceToHost);
+    }
+    for (DevBuf* b : {&b_lv, &b_task, &b_cnt, &b_ctl}) b->release();
+    if (st != GLS_OK) return st;
+    if (e != cudaSuccess) return set_error(GLS_ERR_CUDA, "persistent self-test: %s", cudaGetErrorString(e));
+    if (err_word) *err_word = ctl[1];
+    if (ctl[1]) return set_error(GLS_ERR_TIMEOUT, "persistent self-test: the wait ran out (error word %d)", ctl[1]);
+    return GLS_OK;
 }
 
 gls_status gls_device_memory(uint64_t* current_bytes, uint64_t* peak_bytes, int32_t reset_peak) {
@@ -1091,6 +1332,8 @@ gls_status gls_converter_destroy(gls_converter* conv) {
     }
     if (conv->fork_ev) cudaEventDestroy(conv->fork_ev);
     if (conv->graph_exec) cudaGraphExecDestroy(conv->graph_exec);
+    for (auto& pf : conv->pframes) pf->release();
+    for (DevBuf* b : {&conv->plan_task_buf, &conv->plan_level_buf, &conv->plan_cnt, &conv->plan_ctl}) b->release();
     for (DevBuf* b : {&conv->adj_gden[0], &conv->adj_gden[1], &conv->adj_rec, &conv->adj_glayer, &conv->adj_gpca,
                       &conv->adj_gup, &conv->adj_part, &conv->adj_loss, &conv->adj_target, &conv->adj_gimg,
                       &conv->adj_gp1, &conv->adj_jvp, &conv->adj_jvp_part, &conv->adj_gout, &conv->nlf_scratch,
@@ -1132,9 +1375,21 @@ gls_status gls_demosaic_batch(gls_converter* conv, gls_frame_desc* frames, int32
         if (f.out.dtype != GLS_F32 && f.out.dtype != GLS_F16)
             return set_error(GLS_ERR_INVALID_ARG, "frame %d: output dtype must be F32 or F16", i);
     }
+    const bool persistent = flags & GLS_PERSISTENT;
+    if (persistent) {
+        if (!(flags & GLS_FP16_STORAGE) || !(flags & GLS_DENOISE))
+            return set_error(GLS_ERR_INVALID_ARG, "GLS_PERSISTENT runs the FP16-storage path with noise reduction");
+        if (flags & (GLS_HOST_IO | GLS_POSTPROCESS | GLS_HOST_PCA))
+            return set_error(GLS_ERR_UNSUPPORTED, "GLS_PERSISTENT takes device buffers, without post-processing "
+                                                  "or host PCA");
+        if (conv->calibrate) return set_error(GLS_ERR_UNSUPPORTED, "GLS_PERSISTENT cannot run a calibrating converter");
+        for (int i = 0; i < n_frames; i++)
+            if (!frames[i].out.data)
+                return set_error(GLS_ERR_INVALID_ARG, "GLS_PERSISTENT needs caller-owned outputs (frame %d)", i);
+    }
     GLS_CUDA(cudaSetDevice(conv->device));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if ((flags & GLS_HOST_PCA) || n_frames == 1) {
+    if (!persistent && ((flags & GLS_HOST_PCA) || n_frames == 1)) {
         // per-level host synchronisation serialises anyway: one frame after the other
         for (int i = 0; i < n_frames; i++) {
             gls_frame_desc& f = frames[i];
@@ -1177,17 +1432,19 @@ gls_status gls_demosaic_batch(gls_converter* conv, gls_frame_desc* frames, int32
         key = batch_key(frames, n_frames, flags);
         if (!key.empty() && conv->graph_exec && key == conv->graph_key) {  // replay
             GLS_CUDA(cudaGraphLaunch(conv->graph_exec, s));
+            if (conv->graph_persistent) return persistent_status(conv, s);
             if (flags & (GLS_SYNC | GLS_HOST_IO)) GLS_CUDA(cudaStreamSynchronize(s));
             return GLS_OK;
         }
         if (key.empty()) return set_error(GLS_ERR_INVALID_ARG, "GLS_GRAPH needs caller-owned outputs");
     }
     gls_status result = enqueue_batch(conv, frames, n_frames, flags & ~(GLS_SYNC | GLS_GRAPH), s);
+    if (result == GLS_OK && persistent) result = persistent_status(conv, s);
     if (result == GLS_OK && graph) {
         // record the same launch sequence (allocations and one-time set-up
         // are done by the run above) for replays of this batch
         GLS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
-        const gls_status cap = enqueue_batch(conv, frames, n_frames, flags & ~(GLS_SYNC | GLS_GRAPH), s);
+        const gls_status cap = enqueue_batch(conv, frames, n_frames, flags & ~(GLS_SYNC | GLS_GRAPH), s, true);
         cudaGraph_t g = nullptr;
         const cudaError_t e = cudaStreamEndCapture(s, &g);
         if (cap != GLS_OK) {
@@ -1205,6 +1462,7 @@ gls_status gls_demosaic_batch(gls_converter* conv, gls_frame_desc* frames, int32
             return set_error(GLS_ERR_CUDA, "batch graph instantiation: %s", cudaGetErrorString(ie));
         }
         conv->graph_key = key;
+        conv->graph_persistent = persistent;
     }
     if (result != GLS_OK) return result;
     if (flags & (GLS_SYNC | GLS_HOST_IO)) GLS_CUDA(cudaStreamSynchronize(s));

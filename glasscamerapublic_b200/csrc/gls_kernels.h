@@ -89,8 +89,9 @@ struct SubtractArgs {
 // patches (325, row-major) followed by sum p (25), FP64.
 constexpr int kPcaAcc = 25 + 325;
 constexpr int kPcaDim = 25, kPcaComp = 8;
-constexpr int kPcaMaxBlocks = 296;  // covariance blocks (2 per SM); partials: kPcaMaxBlocks x kPcaAcc FP64
-int pca_cov_blocks(int w, int h);
+constexpr int kPcaCovGroup = 16;  // 64-patch chunks per covariance partial row
+int pca_cov_chunks(int w, int h);  // 64-patch chunks of a level
+int pca_cov_rows(int w, int h);    // partial rows of a level: chunks / kPcaCovGroup, rounded up
 
 template <class S, int C>
 void launch_downsample(Plane<S, C> in, Plane<S, C> out, cudaStream_t s);
@@ -99,7 +100,7 @@ void launch_subtract_noise(Plane<S, 4> in, Plane<S, 4> coarse, Plane<S, 4> coars
                            Plane<S, 4> out, const SubtractArgs& a, cudaStream_t s);
 template <class S>
 void launch_pca_cov(Plane<S, 4> img, double* part, cudaStream_t s);
-// one block per 64-patch chunk: `rows` = ceil(patches / 64) partial rows
+// one block and partial row per 64-patch chunk: `rows` = ceil(patches / 64)
 template <class S>
 void launch_pca_cov_rows(Plane<S, 4> img, double* part, int rows, cudaStream_t s);
 constexpr int kPcaChunk = 64;
@@ -116,6 +117,41 @@ void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, cons
 // the FP16 block matcher's tile-height autotuner decisions: (w, h, height)
 // triples of the level sizes seen so far; returns their count
 int bm_tile_list(int* whty, int max);
+
+// ---- the persistent batch kernel: every pyramid level of every frame of a
+//      batch (reconstruct, covariance, eigen-solve, block matching) in one
+//      launch over a device work list, levels ordered by dependency counters
+enum PTaskType : uint32_t { PT_SN = 0, PT_COV = 1, PT_EIG = 2, PT_BM = 3 };
+struct PTask {
+    uint32_t lev;   // index of the (frame, level) descriptor
+    uint32_t item;  // type in the top 2 bits; tile / row index below
+};
+constexpr uint32_t kPTaskItemMask = 0x3fffffffu;
+struct PLevel {
+    Plane<__half, 4> img, layer, den;  // the level's image, reconstructed layer, denoised output
+    Plane<__half, 2> grad;
+    Plane<__half, 4> coarse, coarse_den;  // the next coarser level (reconstruct inputs)
+    double* part;                         // covariance partial rows
+    float* basis;                         // 25 x 8
+    int* status;                          // eigen-solve status
+    SubtractArgs sa;
+    float rx, ry;                         // coarse / fine size ratios
+    BlockMatchArgs ba;
+    int n_sn, n_cov, n_bm;                // task counts of the level
+    int tiles_x;                          // 32-pixel tiles across the level
+    int chunks;                           // 64-patch covariance chunks
+    int coarser;                          // descriptor of the next coarser level, -1 at the coarsest
+};
+struct PCounters {
+    int sn, cov, eig, bm;  // tasks of the level finished, per type
+};
+// blocks the kernel runs as (resident on the device at once)
+int persistent_grid(int device);
+// tasks[n]; lv, cnt: one per descriptor (cnt zeroed); next: the work
+// counter (zeroed); err: 0, or set to 1 + the type of the task whose wait
+// ran past limit_ns (the kernel then stops taking tasks)
+void launch_pyramid_persistent(const PTask* tasks, int n, const PLevel* lv, PCounters* cnt, int* next, int* err,
+                               long long limit_ns, int grid, cudaStream_t s);
 
 // ---- display post-processing (gls_post.cu)
 // histogram_data's statistics (demosaic.metal:1360-1369)

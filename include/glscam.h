@@ -139,7 +139,9 @@ enum {
     GLS_HOST_PCA = 1u << 5,      /* per-level PCA eigen-solve on the host, as the reference does */
     GLS_GRAPH = 1u << 6,         /* gls_demosaic_batch: record the batch as one CUDA graph and replay it while
                                     the batch (pointers, sizes, strides, parameter bytes) stays the same */
-    GLS_SURF_CORRECTED = 1u << 7 /* gls_surf_detect_and_compute: the corrected detector (see there) */
+    GLS_SURF_CORRECTED = 1u << 7, /* gls_surf_detect_and_compute: the corrected detector (see there) */
+    GLS_PERSISTENT = 1u << 8     /* gls_demosaic_batch: every pyramid level of every frame in one persistent
+                                    launch (see there) */
 };
 
 /* Planes a converter exposes after gls_demosaic, for stage checks. */
@@ -171,6 +173,14 @@ const char* gls_version(void);
  * reset. reset_peak != 0 sets the peak to the current value afterwards.
  * Buffers grow to the largest frame seen and are kept until destroy. */
 gls_status gls_device_memory(uint64_t* current_bytes, uint64_t* peak_bytes, int32_t reset_peak);
+
+/* Failure detection of the persistent batch kernel (GLS_PERSISTENT; no
+ * reference counterpart): runs the kernel on `device` with one eigen-solve
+ * task whose covariance input no task produces, so its bounded wait runs
+ * out after limit_ns. Returns GLS_ERR_TIMEOUT with the kernel's error word
+ * (1 + the task type, 3 for the eigen-solve) in *err_word, the device still
+ * usable; GLS_OK would mean the wait did not run out. */
+gls_status gls_persistent_selftest(int32_t device, int64_t limit_ns, int32_t* err_word);
 
 /* RawConverter(device, icc, calibrateFromImage), raw_converter.hpp:128-156.
  * icc may be NULL (xyz_sRGB). With calibrate_from_image the converter
@@ -220,7 +230,19 @@ typedef struct gls_frame_desc {
  * non-default stream, at least 2 frames) the first call runs the batch and
  * records its launch sequence, copies included, as a CUDA graph; later
  * calls with the same frames, buffers and parameter values replay that
- * graph in one launch. */
+ * graph in one launch.
+ * With GLS_PERSISTENT (FP16 storage, noise reduction, device buffers,
+ * caller-owned outputs, device PCA, no post-processing, not a calibrating
+ * converter) the frames' front ends and pyramid images run on the slot
+ * streams into a pyramid per frame, then ONE launch of a persistent
+ * kernel runs every level of every frame (reconstruct, covariance,
+ * eigen-solve and block matching, PyramidProcessor::denoise,
+ * pyramid_processor.cpp:96-172) from a device work list whose tasks wait
+ * on per-level counters, then the output transforms run; the results are
+ * bit-identical to the stream-launched batch. The call returns after the
+ * kernel, with GLS_ERR_TIMEOUT if a task's wait for its inputs ran past
+ * its limit (2 s). Combined with GLS_GRAPH the whole sequence is recorded
+ * and replayed. */
 gls_status gls_demosaic_batch(gls_converter* conv, gls_frame_desc* frames, int32_t n_frames,
                               uint32_t flags, void* stream);
 
