@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--no-full-frame", action="store_true", help="reference arm: skip the one whole-frame check")
     ap.add_argument("--workload", default=WORKLOAD, help="workload name (cfg2_4032x3024 or cfg1_1024x768)")
     ap.add_argument("--quick", action="store_true", help="timed FP16 loop only (for profiler captures)")
+    ap.add_argument("--frames", type=int, default=N_ROTATE, help="frames per step (batch size)")
     ap.add_argument("--no-burst", action="store_true", help="skip the burst registration + fusion leg")
     ap.add_argument("--burst-frames", type=int, default=8)
     ap.add_argument("--burst-only", action="store_true", help="run only the burst leg (for profiler captures)")
@@ -511,6 +512,22 @@ def mixed_leg(args, rank, local, conv, stream):
         e1.record(stream)
         stream.synchronize()
         ms_stream = e0.elapsed_time(e1) / reps
+        # the persistent batch: the front ends on the slot streams, then one
+        # launch for every pyramid level of every frame, recorded as a graph
+        conv.demosaic_batch(raws, params, outs, stream=stream, persistent=True)  # builds the work list
+        stream.synchronize()
+        l0 = launches()
+        conv.demosaic_batch(raws, params, outs, stream=stream, persistent=True)
+        per_batch_persistent = launches() - l0
+        conv.demosaic_batch(raws, params, outs, stream=stream, persistent=True, graph=True)  # runs and records
+        ms_p = []
+        for _ in range(reps):
+            e0.record(stream)
+            conv.demosaic_batch(raws, params, outs, stream=stream, persistent=True, graph=True)  # replays
+            e1.record(stream)
+            stream.synchronize()
+            ms_p.append(e0.elapsed_time(e1))
+        ms_persistent = float(np.median(ms_p))
         # strong scaling: the one 16-frame batch split over the ranks by
         # pixel count (shard.assign_frames); this rank's share as its own graph
         from glasscamerapublic_b200.shard import assign_frames
@@ -537,6 +554,11 @@ def mixed_leg(args, rank, local, conv, stream):
         "ms_per_batch_graph": ms_graph,
         "ms_per_batch_stream_launched": ms_stream,
         "gpu_launches_per_batch": per_batch,
+        "persistent": {"ms_per_batch_graph": ms_persistent, "value": mpix / (ms_persistent / 1e3), "unit": "MP/s",
+                       "gpu_launches_per_batch": per_batch_persistent,
+                       "note": "GLS_PERSISTENT + GLS_GRAPH: per frame the front end and the pyramid images, then "
+                               "one persistent launch running every level of every frame (reconstruct, covariance, "
+                               "eigen-solve, block matching) from a device work list, then the output transforms"},
         "strong": {"frames_this_rank": mine, "ms_share": ms_share,
                    "note": "the one batch split over the ranks by pixel count (longest-processing-time); "
                            "value = batch MP / the slowest rank's share time"},
@@ -819,12 +841,12 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
-def main_config(wl, world):
+def main_config(wl, world, frames=N_ROTATE):
     """The workload description shared by both arms' lines."""
     return {"workload": wl.name, "frame": f"{wl.width}x{wl.height} RGGB 12-bit", "levels": wl.levels,
-            "iso": wl.iso, "frames_per_step": N_ROTATE,
+            "iso": wl.iso, "frames_per_step": frames,
             "l2": "each step reads 6 distinct frames; inputs + planes >> 126 MB L2",
-            "parallelism": f"frames sharded over {world} rank(s), {N_ROTATE}-frame batch per rank on 3 streams"}
+            "parallelism": f"frames sharded over {world} rank(s), {frames}-frame batch per rank on 3 streams"}
 
 
 def main():
@@ -865,7 +887,7 @@ def main():
             dist.destroy_process_group()
         return
     H, W = wl.height, wl.width
-    B = N_ROTATE  # frames per step (one batch)
+    B = args.frames  # frames per step (one batch)
 
     # resident inputs: distinct frames per rank (weak scaling)
     made = [scene.make_raw(wl, frame=rank * B + f) for f in range(B)]
@@ -992,7 +1014,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f16-storage/f32-math", "data": "synthetic",
-        "config": main_config(wl, world),
+        "config": main_config(wl, world, B),
         "e2e": {"value": world * B / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": B * W * H * 2,
                 "d2h_bytes_per_step": B * W * H * 8,
                 "stream_launched_value": world * B / (e2e_stream_ms / 1e3),

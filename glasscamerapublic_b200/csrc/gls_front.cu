@@ -120,6 +120,154 @@ __global__ void __launch_bounds__(256) k_sobel_blur(Plane<S, 1> raw, Plane<S, 2>
     }
 }
 
+// The FP16-storage path's form of the same stencil. The wide blur's 25
+// bilinear taps sit on a 5 x 5 grid whose x offsets depend on the column
+// only and y offsets on the row only, and whose weights are the Gaussian's
+// 2 x 2 block sums, a product of a row and a column factor: the blur is
+// separable. It runs as a horizontal pass (5 taps, two texels each) into
+// shared memory and a vertical pass over it, a third of the operations of
+// the 25 bilinear taps. The one tap off the grid is the corner, which the
+// folding puts at (width/2, width/2) = (4.5, 4.5) (demosaic_utils.cpp:984)
+// instead of (4, 4): it is moved there by one correction term. The factors
+// come from the tap table (row and column sums of the weights), so the
+// result is the 25-tap blur up to FP32 rounding of the factorisation.
+struct SepSmem {
+    float sraw[SB_RH][SB_RW];
+    float2 ssob[SB_SH][SB_SW];
+    float4 hsum[SB_SH][SB_TW];  // horizontal pass: (gx, gy, |gx|, |gy|) per sobel-tile row, output column
+    float u[5], v[5];
+    int ix[5], iy[5];
+    float fx[5], fy[5];
+    float total, wc, cdx, cdy;  // corner tap: weight, offset
+};
+
+__device__ __forceinline__ float4 bil4(const float2 (*ssob)[SB_SW], int ix, int iy, float ax, float ay) {
+    const float2 p00 = ssob[iy][ix], p01 = ssob[iy][ix + 1];
+    const float2 p10 = ssob[iy + 1][ix], p11 = ssob[iy + 1][ix + 1];
+    auto bil = [&](float v00, float v01, float v10, float v11) {
+        const float top = v00 + (v01 - v00) * ax;
+        const float bot = v10 + (v11 - v10) * ax;
+        return top + (bot - top) * ay;
+    };
+    return make_float4(bil(p00.x, p01.x, p10.x, p11.x), bil(p00.y, p01.y, p10.y, p11.y),
+                       bil(fabsf(p00.x), fabsf(p01.x), fabsf(p10.x), fabsf(p11.x)),
+                       bil(fabsf(p00.y), fabsf(p01.y), fabsf(p10.y), fabsf(p11.y)));
+}
+
+template <class S>
+__global__ void __launch_bounds__(256) k_sobel_blur_sep(Plane<S, 1> raw, Plane<S, 2> out, BlurArgs a) {
+    __shared__ SepSmem sm;
+    const int x0 = blockIdx.x * SB_TW, y0 = blockIdx.y * SB_TH;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int nth = blockDim.x * blockDim.y;
+    if (tid == 0) {  // the wide taps' grid: row / column offsets and weight factors
+        const int b = a.n1;
+        float total = 0.f, rs[5] = {0, 0, 0, 0, 0}, cs[5] = {0, 0, 0, 0, 0};
+        for (int r = 0; r < 5; r++)
+            for (int c = 0; c < 5; c++) {
+                const float w = a.w[b + r * 5 + c];
+                rs[r] += w;
+                cs[c] += w;
+                total += w;
+            }
+        for (int k = 0; k < 5; k++) {
+            sm.u[k] = rs[k] / total;  // u_r v_c = W_rc for a separable table
+            sm.v[k] = cs[k];
+            sm.ix[k] = a.ix[b + k];
+            sm.fx[k] = a.fx[b + k];
+            sm.iy[k] = a.iy[b + k * 5];
+            sm.fy[k] = a.fy[b + k * 5];
+        }
+        sm.total = total;
+        sm.wc = a.w[b + 24];
+        sm.cdx = float(a.ix[b + 24]) + a.fx[b + 24];
+        sm.cdy = float(a.iy[b + 24]) + a.fy[b + 24];
+    }
+    for (int i = tid; i < SB_RW * SB_RH; i += nth) {
+        const int ty = i / SB_RW, tx = i % SB_RW;
+        sm.sraw[ty][tx] = to_f(*raw.pxc(x0 - 5 + tx, y0 - 5 + ty));
+    }
+    __syncthreads();
+    const float inv = a.inv_sqrt45;
+    for (int i = tid; i < SB_SW * SB_SH; i += nth) {
+        const int ty = i / SB_SW, tx = i % SB_SW;
+        const int qx = clampi(x0 - 4 + tx, 0, raw.w - 1) - (x0 - 5);
+        const int qy = clampi(y0 - 4 + ty, 0, raw.h - 1) - (y0 - 5);
+        const float tl = sm.sraw[qy - 1][qx - 1], tc = sm.sraw[qy - 1][qx], tr = sm.sraw[qy - 1][qx + 1];
+        const float ml = sm.sraw[qy][qx - 1], mr = sm.sraw[qy][qx + 1];
+        const float bl = sm.sraw[qy + 1][qx - 1], bc = sm.sraw[qy + 1][qx], br = sm.sraw[qy + 1][qx + 1];
+        const float gx = ((tl - tr) + 2.f * (ml - mr) + (bl - br)) * inv;
+        const float gy = ((tl - bl) + 2.f * (tc - bc) + (tr - br)) * inv;
+        sm.ssob[ty][tx] = make_float2(gx, gy);
+    }
+    __syncthreads();
+    // horizontal pass: every sobel-tile row, every output column
+    for (int i = tid; i < SB_SH * SB_TW; i += nth) {
+        const int ry = i / SB_TW, cx = i % SB_TW;
+        float4 h = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int c = 0; c < 5; c++) {
+            const int xx = cx + 4 + sm.ix[c];
+            const float ax = sm.fx[c], vc = sm.v[c];
+            const float2 p0 = sm.ssob[ry][xx], p1 = sm.ssob[ry][xx + 1];
+            h.x += vc * (p0.x + (p1.x - p0.x) * ax);
+            h.y += vc * (p0.y + (p1.y - p0.y) * ax);
+            h.z += vc * (fabsf(p0.x) + (fabsf(p1.x) - fabsf(p0.x)) * ax);
+            h.w += vc * (fabsf(p0.y) + (fabsf(p1.y) - fabsf(p0.y)) * ax);
+        }
+        sm.hsum[ry][cx] = h;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < SB_TH; r += blockDim.y) {
+        const int x = x0 + threadIdx.x, y = y0 + r;
+        if (x >= out.w || y >= out.h) continue;
+        const int lx = threadIdx.x + 4, ly = r + 4;  // sobel tile index of (x, y)
+        float res[4];
+        {  // narrow blur: its few taps directly
+            float s0 = 0, s1 = 0, s2 = 0, s3 = 0, norm = 0;
+            for (int t = 0; t < a.n1; t++) {
+                const float w = a.w[t];
+                const float4 b = bil4(sm.ssob, lx + a.ix[t], ly + a.iy[t], a.fx[t], a.fy[t]);
+                s0 += w * b.x;
+                s1 += w * b.y;
+                s2 += w * b.z;
+                s3 += w * b.w;
+                norm += w;
+            }
+            res[0] = s0 / norm;
+            res[1] = s1 / norm;
+            res[2] = s2 / norm;
+            res[3] = s3 / norm;
+        }
+        const float sigma = sqrtf(a.var0 + a.var1 * sm.sraw[r + 5][threadIdx.x + 5]);
+        if (sqrtf(res[0] * res[0] + res[1] * res[1]) < 4.f * sigma) {
+            // vertical pass over the horizontal sums, then the corner tap moved
+            float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                const int yy = ly + sm.iy[k];
+                const float ay = sm.fy[k], ur = sm.u[k];
+                const float4 h0 = sm.hsum[yy][threadIdx.x], h1 = sm.hsum[yy + 1][threadIdx.x];
+                acc.x += ur * (h0.x + (h1.x - h0.x) * ay);
+                acc.y += ur * (h0.y + (h1.y - h0.y) * ay);
+                acc.z += ur * (h0.z + (h1.z - h0.z) * ay);
+                acc.w += ur * (h0.w + (h1.w - h0.w) * ay);
+            }
+            const float gxo = float(sm.ix[4]) + sm.fx[4], gyo = float(sm.iy[4]) + sm.fy[4];  // the grid corner
+            const float4 on = bil4(sm.ssob, lx + int(floorf(gxo)), ly + int(floorf(gyo)), gxo - floorf(gxo),
+                                   gyo - floorf(gyo));
+            const float4 at = bil4(sm.ssob, lx + int(floorf(sm.cdx)), ly + int(floorf(sm.cdy)),
+                                   sm.cdx - floorf(sm.cdx), sm.cdy - floorf(sm.cdy));
+            const float it = 1.f / sm.total;
+            res[0] = (acc.x + sm.wc * (at.x - on.x)) * it;
+            res[1] = (acc.y + sm.wc * (at.y - on.y)) * it;
+            res[2] = (acc.z + sm.wc * (at.z - on.z)) * it;
+            res[3] = (acc.w + sm.wc * (at.w - on.w)) * it;
+        }
+        st2<S>(out.px(x, y), f2{copysignf(res[2], res[0]), copysignf(res[3], res[1])});
+    }
+}
+
 // --------------------------------------------------------------------------
 // High-noise raw branch, raw_converter.cpp:195-202: bayerToRawRGBA ->
 // despeckleRawRGBAImage -> crossDenoiseRawRGBAImage -> rawRGBAToBayer.
@@ -554,7 +702,10 @@ template <class S>
 void launch_sobel_blur(Plane<S, 1> raw, Plane<S, 2> out, const BlurArgs& a, cudaStream_t s) {
     dim3 b(32, 8);
     dim3 g((raw.w + SB_TW - 1) / SB_TW, (raw.h + SB_TH - 1) / SB_TH);
-    k_sobel_blur<S><<<g, b, 0, s>>>(raw, out, a);
+    // the FP16-storage path takes the separable form of the 5 x 5 wide blur;
+    // the FP32 plain path evaluates the reference's 25 bilinear taps
+    if (is_half<S>::value && a.n2 == 25) k_sobel_blur_sep<S><<<g, b, 0, s>>>(raw, out, a);
+    else k_sobel_blur<S><<<g, b, 0, s>>>(raw, out, a);
 }
 
 template <class S>
