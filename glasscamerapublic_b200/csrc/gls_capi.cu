@@ -382,9 +382,8 @@ static gls_status pyramid_run(gls_converter* cv, Pipeline<S>& P, Plane<S, 4> img
     for (int i = 1; i < L; i++) {  // Gaussian pyramid, pyramid_processor.cpp:103-120
         img[i] = plane<S, 4>(P.img[i], W >> i, H >> i);
         grd[i] = plane<S, 2>(P.gradp[i], W >> i, H >> i);
-        KScope k(cv->prof, KC_DOWNSAMPLE, s, 2);
-        launch_downsample<S, 4>(img[i - 1], img[i], s);
-        launch_downsample<S, 2>(grd[i - 1], grd[i], s);
+        KScope k(cv->prof, KC_DOWNSAMPLE, s);
+        launch_downsample_pair<S>(img[i - 1], img[i], grd[i - 1], grd[i], s);
     }
     if (build_only) return GLS_OK;  // the levels run in the persistent batch kernel
     gls_demosaic_params measured;

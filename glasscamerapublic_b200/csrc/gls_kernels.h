@@ -95,6 +95,10 @@ int pca_cov_rows(int w, int h);    // partial rows of a level: chunks / kPcaCovG
 
 template <class S, int C>
 void launch_downsample(Plane<S, C> in, Plane<S, C> out, cudaStream_t s);
+// a level's image and gradient in one launch (equal sizes)
+template <class S>
+void launch_downsample_pair(Plane<S, 4> img, Plane<S, 4> img_out, Plane<S, 2> grad, Plane<S, 2> grad_out,
+                            cudaStream_t s);
 template <class S>
 void launch_subtract_noise(Plane<S, 4> in, Plane<S, 4> coarse, Plane<S, 4> coarse_den, Plane<S, 2> grad,
                            Plane<S, 4> out, const SubtractArgs& a, cudaStream_t s);

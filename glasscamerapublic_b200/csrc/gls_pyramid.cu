@@ -19,9 +19,8 @@ namespace gls {
 // r = in/out size (a 4x4 box for an exact halving). Positions are formed
 // with explicit FP32 roundings, matching the oracle's FP32 run.
 template <class S, int C>
-__global__ void __launch_bounds__(256) k_downsample(Plane<S, C> in, Plane<S, C> out, float rx, float ry) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= out.w || y >= out.h) return;
+__device__ __forceinline__ void downsample_px(const Plane<S, C>& in, const Plane<S, C>& out, float rx, float ry,
+                                              int x, int y) {
     const float u[2] = {__fsub_rn(__fmul_rn(float(x), rx), 0.5f), __fsub_rn(__fmul_rn(float(x + 1), rx), 0.5f)};
     const float v[2] = {__fsub_rn(__fmul_rn(float(y), ry), 0.5f), __fsub_rn(__fmul_rn(float(y + 1), ry), 0.5f)};
     float acc[C > 2 ? 3 : 2] = {};
@@ -60,6 +59,25 @@ __global__ void __launch_bounds__(256) k_downsample(Plane<S, C> in, Plane<S, C> 
     } else {
         st2<S>(out.px(x, y), f2{0.25f * acc[0], 0.25f * acc[1]});
     }
+}
+
+template <class S, int C>
+__global__ void __launch_bounds__(256) k_downsample(Plane<S, C> in, Plane<S, C> out, float rx, float ry) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= out.w || y >= out.h) return;
+    downsample_px<S, C>(in, out, rx, ry, x, y);
+}
+
+// The image and the gradient of a pyramid level in one launch (same sizes,
+// same sample positions): PyramidProcessor::denoise's two downsamples
+// (pyramid_processor.cpp:109-110).
+template <class S>
+__global__ void __launch_bounds__(256) k_downsample_pair(Plane<S, 4> img, Plane<S, 4> img_out, Plane<S, 2> grad,
+                                                         Plane<S, 2> grad_out, float rx, float ry) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= img_out.w || y >= img_out.h) return;
+    downsample_px<S, 4>(img, img_out, rx, ry, x, y);
+    downsample_px<S, 2>(grad, grad_out, rx, ry, x, y);
 }
 
 template <class S>
@@ -133,6 +151,14 @@ void launch_downsample(Plane<S, C> in, Plane<S, C> out, cudaStream_t s) {
     dim3 b(32, 8);
     k_downsample<S, C><<<grid2(out.w, out.h, b), b, 0, s>>>(in, out, float(in.w) / float(out.w),
                                                             float(in.h) / float(out.h));
+}
+
+template <class S>
+void launch_downsample_pair(Plane<S, 4> img, Plane<S, 4> img_out, Plane<S, 2> grad, Plane<S, 2> grad_out,
+                            cudaStream_t s) {
+    dim3 b(32, 8);
+    k_downsample_pair<S><<<grid2(img_out.w, img_out.h, b), b, 0, s>>>(
+        img, img_out, grad, grad_out, float(img.w) / float(img_out.w), float(img.h) / float(img_out.h));
 }
 
 template <class S>
@@ -250,6 +276,7 @@ void host_pca_basis(const double* part, int n_blocks, int n_patches, float* basi
 #define GLS_INST(S)                                                                                              \
     template void launch_downsample<S, 4>(Plane<S, 4>, Plane<S, 4>, cudaStream_t);                              \
     template void launch_downsample<S, 2>(Plane<S, 2>, Plane<S, 2>, cudaStream_t);                              \
+    template void launch_downsample_pair<S>(Plane<S, 4>, Plane<S, 4>, Plane<S, 2>, Plane<S, 2>, cudaStream_t);  \
     template void launch_subtract_noise<S>(Plane<S, 4>, Plane<S, 4>, Plane<S, 4>, Plane<S, 2>, Plane<S, 4>,     \
                                            const SubtractArgs&, cudaStream_t);                                   \
     template void launch_pca_cov<S>(Plane<S, 4>, double*, cudaStream_t);                                         \
