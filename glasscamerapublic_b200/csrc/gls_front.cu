@@ -682,18 +682,18 @@ __device__ __forceinline__ float median9(float v[9]) {
     return v[4];
 }
 
-template <class S>
-__global__ void __launch_bounds__(256) k_despeckle(Plane<S, 4> in, Plane<S, 4> out, float va, float vb) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= in.w || y >= in.h) return;
+// One output pixel from its 3 x 3 neighbourhood, rows r0..r2 of 3 loaded
+// pixels each, taken in the reference's order (j = -1..1, i = -1..1).
+__device__ __forceinline__ f4 despeckle_px(const f4 (&r0)[3], const f4 (&r1)[3], const f4 (&r2)[3], float va,
+                                           float vb) {
     float cb[9], cr[9];
     float fmx = 0.f, smx = 0.f, fmn = INFINITY, smn = INFINITY, sample = 0.f;
-    int k = 0;
+    const f4* rows[3] = {r0, r1, r2};
 #pragma unroll
-    for (int j = -1; j <= 1; j++)
+    for (int j = 0; j < 3; j++)
 #pragma unroll
-        for (int i = -1; i <= 1; i++, k++) {
-            const f4 p = ld4<S>(in.pxc(x + i, y + j));
+        for (int i = 0; i < 3; i++) {
+            const f4 p = rows[j][i];
             const float v = p.x;
             smx = (v <= fmx && v > smx) ? v : smx;
             smx = v > fmx ? fmx : smx;
@@ -701,14 +701,29 @@ __global__ void __launch_bounds__(256) k_despeckle(Plane<S, 4> in, Plane<S, 4> o
             smn = (v >= fmn && v < smn) ? v : smn;
             smn = v < fmn ? fmn : smn;
             fmn = v < fmn ? v : fmn;
-            if (i == 0 && j == 0) sample = v;
-            cb[k] = p.y;
-            cr[k] = p.z;
+            if (i == 1 && j == 1) sample = v;
+            cb[3 * j + i] = p.y;
+            cr[3 * j + i] = p.z;
         }
     const float sigma = sqrtf(va + vb * sample);
     const float mn = mixf(smn, fmn, smoothstepf(sigma, 4.f * sigma, smn - fmn));
     const float mx = mixf(smx, fmx, smoothstepf(sigma, 4.f * sigma, fmx - smx));
-    st4<S>(out.px(x, y), f4{clampf(sample, mn, mx), median9(cb), median9(cr), 0.f});
+    return f4{clampf(sample, mn, mx), median9(cb), median9(cr), 0.f};
+}
+
+// Two vertically adjacent pixels per thread: they share two of their three
+// neighbourhood rows (12 loads instead of 18).
+template <class S>
+__global__ void __launch_bounds__(256) k_despeckle(Plane<S, 4> in, Plane<S, 4> out, float va, float vb) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = 2 * (blockIdx.y * blockDim.y + threadIdx.y);
+    if (x >= in.w || y >= in.h) return;
+    f4 r[4][3];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int i = 0; i < 3; i++) r[j][i] = ld4<S>(in.pxc(x + i - 1, y + j - 1));
+    st4<S>(out.px(x, y), despeckle_px(r[0], r[1], r[2], va, vb));
+    if (y + 1 < in.h) st4<S>(out.px(x, y + 1), despeckle_px(r[1], r[2], r[3], va, vb));
 }
 
 // transformImage, demosaic.metal:649-662, from plane S4 to an output of
@@ -781,7 +796,7 @@ void launch_demosaic(Plane<S, 1> raw, Plane<S, 2> grad, Plane<S, 4> out, const D
 template <class S>
 void launch_despeckle(Plane<S, 4> in, Plane<S, 4> out, float va, float vb, cudaStream_t s) {
     dim3 b(32, 8);
-    k_despeckle<S><<<grid2(in.w, in.h, b), b, 0, s>>>(in, out, va, vb);
+    k_despeckle<S><<<grid2(in.w, (in.h + 1) / 2, b), b, 0, s>>>(in, out, va, vb);
 }
 
 template <class S, class O>

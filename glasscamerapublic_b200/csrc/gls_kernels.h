@@ -89,7 +89,7 @@ struct SubtractArgs {
 // patches (325, row-major) followed by sum p (25), FP64.
 constexpr int kPcaAcc = 25 + 325;
 constexpr int kPcaDim = 25, kPcaComp = 8;
-constexpr int kPcaCovGroup = 16;  // 64-patch chunks per covariance partial row
+constexpr int kPcaCovGroup = 4;  // 64-patch chunks per covariance partial row
 int pca_cov_chunks(int w, int h);  // 64-patch chunks of a level
 int pca_cov_rows(int w, int h);    // partial rows of a level: chunks / kPcaCovGroup, rounded up
 

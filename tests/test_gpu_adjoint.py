@@ -4,10 +4,14 @@ gradient: torch.autograd of the float64 re-expression of the pyramid
 FP64 oracle), fed the CUDA forward's own despeckled image, gradient plane and
 PCA bases. The adjoint runs in FP32; tolerances:
   * loss: 1e-4 relative;
-  * each gradient entry: 2e-3 of its magnitude plus 1e-3 of the largest
-    entry of the same parameter kind (per-level luma, chroma, A_Y, B_Y,
-    A_C, B_C), which absorbs FP32 rounding on near-zero entries;
+  * each gradient entry of at least 1e-2 of the largest entry of its
+    parameter kind (per-level luma, chroma, A_Y, B_Y, A_C, B_C): 1e-3
+    relative; every entry: 1e-3 of its magnitude plus 1e-5 of the largest
+    entry of its kind, which absorbs FP32 rounding on near-zero entries
+    (the coarsest levels' entries can be 1e-12 of the finest's);
   * dL/d(despeckled image), per pixel: 1e-3 of its largest entry.
+The full-size case (one 2048x1536 frame of the calibration workload) runs
+the float64 reference on the GPU, its window rows checkpointed.
 The raw-green entries (30, 31) act through the front end: they are checked
 against central differences of the loss, the front end run by the FP64
 oracle's stages and the pyramid by the oracle's FP64 pyramid with the same
@@ -25,12 +29,12 @@ from glasscamerapublic_b200 import scene
 pytestmark = pytest.mark.gpu
 
 
-def _reference(converter, p, target, levels):
+def _reference(converter, p, target, levels, device="cpu", checkpoint=False):
     ds = converter.plane(g.PLANE_DESPECKLED)
     grad = converter.plane(g.PLANE_GRADIENT)
     bases = np.stack([converter.pca_basis(l) for l in range(levels)]).astype(np.float64)
     _, inv = O.cam_ycbcr(np.eye(3), scene.XYZ_SRGB)
-    return TP.loss_and_grad(ds, grad, p, bases, inv, target)
+    return TP.loss_and_grad(ds, grad, p, bases, inv, target, device=device, checkpoint=checkpoint)
 
 
 def _check(loss, grad, loss_t, g_t, levels):
@@ -39,8 +43,11 @@ def _check(loss, grad, loss_t, g_t, levels):
     for kind in range(6):
         sl = slice(5 * kind, 5 * kind + levels)
         ref = g_t[sl]
-        tol = 2e-3 * np.abs(ref) + 1e-3 * np.abs(ref).max() + 1e-30
-        assert np.all(np.abs(grad[sl] - ref) <= tol), (kind, grad[sl], ref)
+        got = grad[sl].astype(np.float64)
+        big = np.abs(ref) >= 1e-2 * np.abs(ref).max()
+        assert np.all(np.abs(got - ref)[big] <= 1e-3 * np.abs(ref)[big]), (kind, got, ref)
+        tol = 1e-3 * np.abs(ref) + 1e-5 * np.abs(ref).max() + 1e-30
+        assert np.all(np.abs(got - ref) <= tol), (kind, got, ref)
         assert np.all(grad[5 * kind + levels:5 * kind + 5] == 0)
 
 
@@ -54,6 +61,18 @@ def test_adjoint_matches_autograd(converter, levels, iso, size):
     loss, grad = A.loss_and_grad(converter, raw, p, target)
     loss_t, g_t, _ = _reference(converter, p, target, levels)
     _check(loss, grad, loss_t, g_t, levels)
+
+
+def test_adjoint_full_size_calibration_frame(converter):
+    # one frame of the 8 x 2048x1536 calibration workload, 5 levels
+    wl = scene.Workload("cfg5_2048x1536", 2048, 1536, levels=5, gain=1.0, read=4.0, iso=800, seed=5000)
+    raw, clean = scene.make_raw(wl)
+    p = scene.make_params(wl)
+    target = scene.target_rgb(clean).astype(np.float32)
+    loss, grad = A.loss_and_grad(converter, raw, p, target)
+    loss_t, g_t, _ = _reference(converter, p, target, 5, device="cuda", checkpoint=True)
+    torch.cuda.empty_cache()
+    _check(loss, grad, loss_t, g_t, 5)
 
 
 def test_adjoint_input_gradient_matches_autograd(converter):
@@ -153,6 +172,6 @@ def test_pyramid_denoise_vjp_matches_autograd(converter):
     for kind in range(6):
         sl = slice(5 * kind, 5 * kind + 3)
         ref = g_ref[sl]
-        tol = 2e-3 * np.abs(ref) + 1e-3 * np.abs(ref).max() + 1e-30
-        assert np.all(np.abs(gt[sl] - ref) <= tol), (kind, gt[sl], ref)
+        tol = 1e-3 * np.abs(ref) + 1e-4 * np.abs(ref).max() + 1e-30  # a random cotangent: sums that cancel
+        assert np.all(np.abs(gt[sl].astype(np.float64) - ref) <= tol), (kind, gt[sl], ref)
     assert np.abs(g_ycc - gds_ref).max() <= 1e-3 * np.abs(gds_ref).max()
