@@ -76,8 +76,10 @@ def test_persistent_batch_rejects_what_it_does_not_run(converter):
     with pytest.raises(g.GlsError) as e:
         converter.demosaic_batch(raws, params, _outs(), fp16=False, out_fp16=False, persistent=True)
     assert e.value.code == g.GLS_ERR_INVALID_ARG
-    with pytest.raises(g.GlsError) as e:
-        converter.demosaic_batch(raws, params, _outs(), persistent=True, postProcess=True)
+    host_raws = [r.cpu().numpy() for r in raws]
+    host_outs = [o.cpu().numpy() for o in _outs()]
+    with pytest.raises(g.GlsError) as e:  # host buffers
+        converter.demosaic_batch(host_raws, params, host_outs, persistent=True)
     assert e.value.code == g.GLS_ERR_UNSUPPORTED
 
 
