@@ -143,7 +143,7 @@ __device__ __forceinline__ void pca_cov_row(Plane<S, 4> img, double* __restrict_
 //   2. the 8 largest eigenvalues of T by Sturm-sequence multisection:
 //      warp w brackets eigenvalue 24 - w (ascending order); its 32 lanes
 //      count the eigenvalues below 32 points of the bracket, which shrinks
-//      33-fold per round (11 rounds reach FP64 resolution);
+//      33-fold per round (7 rounds: 2.4e-11 of the spectrum width);
 //   3. each eigenvector of T by inverse iteration: the tridiagonal
 //      T - lambda I is factored once with partial pivoting (lane 0 of the
 //      eigenvalue's warp) and solved three times from a start vector of its
@@ -158,7 +158,11 @@ __device__ __forceinline__ void pca_cov_row(Plane<S, 4> img, double* __restrict_
 // basis. Every reduction has a fixed order, so the result is deterministic.
 // status receives the number of inverse-iteration solves per vector (3), or
 // -1 when a vector came out non-finite (the basis is then still written).
-constexpr int EJ_N = 25, EJ_TOP = 8, EJ_INV_ITERS = 3, EJ_MSEC_ROUNDS = 11;
+// 7 multisection rounds bracket each eigenvalue to 33^-7 (2.4e-11) of the
+// spectrum's width: inverse iteration from such a shift converges in its
+// three solves (the error shrinks by shift error / gap per solve), and the
+// eigenvalue itself only orders the vectors and sets the rank threshold
+constexpr int EJ_N = 25, EJ_TOP = 8, EJ_INV_ITERS = 3, EJ_MSEC_ROUNDS = 7;
 
 // 1 / x to FP64 accuracy: the hardware approximation refined by two
 // Newton-Raphson steps r <- r + r (1 - x r), each doubling the correct bits.
@@ -223,7 +227,7 @@ __device__ inline void pca_eigen_block(const double* __restrict__ part, int n_bl
         return;
     }
     // ---- partial rows summed in a fixed order: two halves of the row range
-    //      per accumulator, eight loads in flight each, then added
+    //      per accumulator, sixteen loads in flight each, then added
     {
         const int half = (n_blocks + 1) / 2;
         for (int q = t; q < 2 * kPcaAcc; q += nth) {
@@ -231,12 +235,12 @@ __device__ inline void pca_eigen_block(const double* __restrict__ part, int n_bl
             const int b0 = h == 0 ? 0 : half, b1 = h == 0 ? half : n_blocks;
             double v = 0.0;
             int b = b0;
-            for (; b + 8 <= b1; b += 8) {
-                double x[8];
+            for (; b + 16 <= b1; b += 16) {  // sixteen loads in flight
+                double x[16];
 #pragma unroll
-                for (int k = 0; k < 8; k++) x[k] = part[size_t(b + k) * kPcaAcc + a];
+                for (int k = 0; k < 16; k++) x[k] = part[size_t(b + k) * kPcaAcc + a];
 #pragma unroll
-                for (int k = 0; k < 8; k++) v += x[k];
+                for (int k = 0; k < 16; k++) v += x[k];
             }
             for (; b < b1; b++) v += part[size_t(b) * kPcaAcc + a];
             (h == 0 ? sm.part1 : sm.part2)[a] = v;
