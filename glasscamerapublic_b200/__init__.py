@@ -37,6 +37,7 @@ SYNC = 1 << 4
 GRAPH = 1 << 6
 SURF_CORRECTED = 1 << 7
 PERSISTENT = 1 << 8
+BM_TENSOR = 1 << 9
 HOST_PCA = 1 << 5
 
 PLANE_SCALED_RAW = 0

@@ -13,7 +13,8 @@ import ctypes as C
 
 import numpy as np
 
-from . import (DENOISE, F16, F32, FP16_STORAGE, GRAPH, HOST_IO, HOST_PCA, PERSISTENT, POSTPROCESS, SYNC,
+from . import (BM_TENSOR, DENOISE, F16, F32, FP16_STORAGE, GRAPH, HOST_IO, HOST_PCA, PERSISTENT, POSTPROCESS,
+               SYNC,
                CAMERA_IPHONE14_WIDE,
                DemosaicParams, ImageView, FrameDesc, RawNLF, YCbCrNLF, check, lib)
 
@@ -133,11 +134,14 @@ class RawConverter:
 
     def demosaic_batch(self, raws, params_list, outs, fp16: bool = True, noiseReduction: bool = True,
                        out_fp16: bool = True, stream=None, sync: bool = False, host_pca: bool = False,
-                       graph: bool = False, postProcess: bool = False, persistent: bool = False):
+                       graph: bool = False, postProcess: bool = False, persistent: bool = False,
+                       tensor_bm: bool = False):
         """Batched RawConverter::demosaic over frames of uneven sizes.
 
         ``raws``/``outs``: torch CUDA tensors (device I/O), or host buffers
         (numpy arrays or pinned torch CPU tensors; copied inside the call).
+        ``tensor_bm``: the tensor-core block matcher (GLS_BM_TENSOR), the one
+        the persistent batch runs.
         """
         n = len(raws)
         frames = (FrameDesc * n)()
@@ -154,6 +158,7 @@ class RawConverter:
         flags = (DENOISE if noiseReduction else 0) | (FP16_STORAGE if fp16 else 0) | (SYNC if sync else 0)
         flags |= (HOST_IO if host else 0) | (HOST_PCA if host_pca else 0) | (GRAPH if graph else 0)
         flags |= (POSTPROCESS if postProcess else 0) | (PERSISTENT if persistent else 0)
+        flags |= BM_TENSOR if tensor_bm else 0
         check(lib().gls_demosaic_batch(self._h, frames, n, flags, _stream_handle(stream)))
         return outs
 

@@ -978,11 +978,13 @@ template <class S>
 void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, const float* basis, Plane<S, 4> out,
                         const BlockMatchArgs& a, cudaStream_t s) {
     if constexpr (is_half<S>::value) {
-        static const bool pair_kernel = [] {
+        // the packed-FP32 matcher unless the call asks for the tensor-core one
+        // (GLS_BM_TENSOR) or GLS_BM_KERNEL=mma selects it for the process
+        static const bool mma_env = [] {
             const char* e = std::getenv("GLS_BM_KERNEL");
-            return e && std::strcmp(e, "pair") == 0;
+            return e && std::strcmp(e, "mma") == 0;
         }();
-        if (!pair_kernel) {
+        if (a.tensor || mma_env) {
             launch_mma(img, grad, basis, out, a, s);
             return;
         }

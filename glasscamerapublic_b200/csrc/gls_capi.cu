@@ -453,6 +453,7 @@ static gls_status pyramid_run(gls_converter* cv, Pipeline<S>& P, Plane<S, 4> img
         ba.gradient_boost = dp.gradient_boost;
         ba.gradient_threshold = dp.gradient_threshold;
         ba.lsc = p->lens_shading_correction;
+        ba.tensor = flags & GLS_BM_TENSOR;
         if (!is_half<S>::value && cv->keep_nc) {
             GLS_TRY(P.nc[i].ensure(size_t(wi) * hi * sizeof(float)));
             ba.nc_out = static_cast<float*>(P.nc[i].p);

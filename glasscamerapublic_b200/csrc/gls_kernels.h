@@ -79,6 +79,7 @@ struct BlockMatchArgs {
     float chroma_boost, gradient_boost, gradient_threshold;
     float lsc;                    // lens shading correction (0 = off)
     float* nc_out = nullptr;      // FP32 path: the chroma kernel norm per pixel, kept for the adjoint
+    bool tensor = false;          // FP16 path: the tensor-core matcher (GLS_BM_TENSOR)
 };
 
 struct SubtractArgs {

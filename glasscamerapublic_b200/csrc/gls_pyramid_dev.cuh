@@ -72,15 +72,16 @@ __device__ __forceinline__ void subtract_noise_px(const Plane<S, 4>& in, const P
 // chunks of 64. Partial row r holds the FP64 sums over chunks
 // [g r, g (r + 1)) (g chunks per row): the upper triangle of sum p p^T
 // (325, indexed by pca_tri_index) then sum p (25). A block stages a chunk
-// in shared memory; its threads own the 350 accumulators (thread t the
-// ones t, t + blockDim, ...), each summed chunk by chunk, patch by patch,
-// so a row's bits do not depend on the block size. The rows are summed in
-// order by the eigen-solve, so the result does not depend on scheduling
-// (no atomics).
+// in shared memory, converted to FP64 once per value (a conversion per
+// product would cost more than the products); its threads own the 350
+// accumulators (thread t the ones t, t + blockDim, ...), each summed chunk
+// by chunk, patch by patch, so a row's bits do not depend on the block
+// size. The rows are summed in order by the eigen-solve, so the result
+// does not depend on scheduling (no atomics).
 constexpr int PC_CHUNK = kPcaChunk;
 
 struct CovSmem {
-    float sp[PC_CHUNK][kPcaDim + 1];
+    double sp[PC_CHUNK][kPcaDim + 1];
 };
 
 template <class S>
@@ -106,7 +107,7 @@ __device__ __forceinline__ void pca_cov_row(Plane<S, 4> img, double* __restrict_
             const int k = i / kPcaDim, e = i % kPcaDim;
             const int pidx = base + k;
             const int px = (pidx % gw) * 8 + (e % 5) - 2, py = (pidx / gw) * 8 + (e / 5) - 2;
-            sm.sp[k][e] = to_f(*img.pxc(px, py));
+            sm.sp[k][e] = double(to_f(*img.pxc(px, py)));
         }
         __syncthreads();
 #pragma unroll
@@ -114,10 +115,10 @@ __device__ __forceinline__ void pca_cov_row(Plane<S, 4> img, double* __restrict_
             const int a = t + j * nth;
             if (a < kPcaTri) {
 #pragma unroll 4
-                for (int k = 0; k < cnt; k++) sum[j][k & 3] += double(sm.sp[k][r[j]]) * double(sm.sp[k][c[j]]);
+                for (int k = 0; k < cnt; k++) sum[j][k & 3] += sm.sp[k][r[j]] * sm.sp[k][c[j]];
             } else if (a < kPcaAcc) {
 #pragma unroll 4
-                for (int k = 0; k < cnt; k++) sum[j][k & 3] += double(sm.sp[k][r[j]]);
+                for (int k = 0; k < cnt; k++) sum[j][k & 3] += sm.sp[k][r[j]];
             }
         }
         __syncthreads();

@@ -140,8 +140,12 @@ enum {
     GLS_GRAPH = 1u << 6,         /* gls_demosaic_batch: record the batch as one CUDA graph and replay it while
                                     the batch (pointers, sizes, strides, parameter bytes) stays the same */
     GLS_SURF_CORRECTED = 1u << 7, /* gls_surf_detect_and_compute: the corrected detector (see there) */
-    GLS_PERSISTENT = 1u << 8     /* gls_demosaic_batch: every pyramid level of every frame in one persistent
+    GLS_PERSISTENT = 1u << 8,    /* gls_demosaic_batch: every pyramid level of every frame in one persistent
                                     launch (see there) */
+    GLS_BM_TENSOR = 1u << 9      /* FP16 storage: block matching with the patch distances and the weighted
+                                    sums on the tensor cores and the weights in half precision (the matcher
+                                    the persistent batch runs); without it the FP16 matcher computes every
+                                    weight in packed FP32 */
 };
 
 /* Planes a converter exposes after gls_demosaic, for stage checks. */

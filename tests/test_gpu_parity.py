@@ -26,6 +26,14 @@ def _run(conv, raw, p, denoise=True, fp16=False, host_pca=False):
     return conv.demosaic(raw, p, noiseReduction=denoise, fp16=fp16, host_pca=host_pca)
 
 
+def _run_tensor_bm(conv, raw, p):
+    """The FP16-storage path with the tensor-core block matcher
+    (GLS_BM_TENSOR; half-precision weights), host buffers in and out."""
+    out = np.empty(raw.shape + (4,), np.float16)
+    conv.demosaic_batch([raw], [p], [out], tensor_bm=True, sync=True)
+    return out.astype(np.float32)
+
+
 def _p999(a, b):
     d = np.abs(np.asarray(a, np.float64) - np.asarray(b, np.float64))
     return float(np.quantile(d, 0.999)), float(d.max())
@@ -109,12 +117,14 @@ def test_full_pipeline_cfg1_fp32_and_fp16(converter):
     out32 = _run(converter, raw, p)
     q, m = _p999(out32[..., :3], ref32[..., :3])
     assert q <= 1e-4, (q, m)
-    out16 = _run(converter, raw, p, fp16=True)
     tgt = scene.target_rgb(clean)
-    ps16 = scene.psnr(out16[..., :3], tgt)
     ps64 = scene.psnr(ref64[..., :3], tgt)
-    assert abs(ps16 - ps64) <= 0.05, (ps16, ps64)
-    assert scene.psnr(out16[..., :3], ref64[..., :3]) >= 50.0
+    # both FP16 block matchers: packed FP32 weights (default) and the
+    # tensor-core one with half-precision weights
+    for out16 in (_run(converter, raw, p, fp16=True), _run_tensor_bm(converter, raw, p)):
+        ps16 = scene.psnr(out16[..., :3], tgt)
+        assert abs(ps16 - ps64) <= 0.05, (ps16, ps64)
+        assert scene.psnr(out16[..., :3], ref64[..., :3]) >= 50.0
 
 
 def test_full_pipeline_cfg2_headline(converter):
@@ -123,8 +133,9 @@ def test_full_pipeline_cfg2_headline(converter):
     pyramid, through RawConverter::demosaic's sequence
     (raw_converter.cpp:148-248, pyramid_processor.cpp:96-172):
       * FP32 path vs the oracle's FP32 run: 99.9th pct |diff| <= 1e-4;
-      * FP16-storage path vs the oracle's FP64 run: PSNR >= 50 dB, and its
-        PSNR against the clean scene within 0.05 dB of the FP64 oracle's."""
+      * FP16-storage path, with either block matcher, vs the oracle's FP64
+        run: PSNR >= 50 dB, and its PSNR against the clean scene within
+        0.05 dB of the FP64 oracle's."""
     wl = scene.WORKLOADS["cfg2_4032x3024"]
     raw, clean = scene.make_raw(wl)
     p = scene.make_params(wl)
@@ -135,12 +146,14 @@ def test_full_pipeline_cfg2_headline(converter):
     assert q <= 1e-4, (q, m)
     del ref32, out32
     ref64 = O.raw_pipeline(raw, p, denoise=True, f64=True)["out"]
-    out16 = _run(converter, raw, p, fp16=True)
     tgt = scene.target_rgb(clean)
-    ps16 = scene.psnr(out16[..., :3], tgt)
     ps64 = scene.psnr(ref64[..., :3], tgt)
-    assert abs(ps16 - ps64) <= 0.05, (ps16, ps64)
-    assert scene.psnr(out16[..., :3], ref64[..., :3]) >= 50.0
+    # both FP16 block matchers: packed FP32 weights (default) and the
+    # tensor-core one with half-precision weights
+    for out16 in (_run(converter, raw, p, fp16=True), _run_tensor_bm(converter, raw, p)):
+        ps16 = scene.psnr(out16[..., :3], tgt)
+        assert abs(ps16 - ps64) <= 0.05, (ps16, ps64)
+        assert scene.psnr(out16[..., :3], ref64[..., :3]) >= 50.0
 
 
 def test_host_pca_and_device_pca_agree(converter):

@@ -1,4 +1,4 @@
-"""The FFMA2 pair form of the FP16 block matcher (GLS_BM_KERNEL=pair) and
+"""The FFMA2 pair form of the FP16 block matcher (the default one) and
 its tile-height autotuner: 32 x 32 and 32 x 16 pixel tiles compute the same
 bits (same per-pixel arithmetic, same centring vector), so forcing either
 height through GLS_BM_TILE, or letting the autotuner choose, gives
@@ -45,7 +45,7 @@ c.close()
 def _run(tmp_path, tag, tile):
     env = dict(os.environ)
     env.pop("GLS_BM_TILE", None)
-    env["GLS_BM_KERNEL"] = "pair"
+    env.pop("GLS_BM_KERNEL", None)
     if tile:
         env["GLS_BM_TILE"] = str(tile)
     base = str(tmp_path / tag)
