@@ -71,17 +71,21 @@ __device__ __forceinline__ void subtract_noise_px(const Plane<S, 4>& in, const P
 // the 5x5 luma neighbourhoods of (8x, 8y), x < W/8, y < H/8, taken in
 // chunks of 64. Partial row r holds the FP64 sums over chunks
 // [g r, g (r + 1)) (g chunks per row): the upper triangle of sum p p^T
-// (325, indexed by pca_tri_index) then sum p (25). A block stages a chunk
-// in shared memory, converted to FP64 once per value (a conversion per
-// product would cost more than the products); its threads own the 350
-// accumulators (thread t the ones t, t + blockDim, ...), each summed chunk
-// by chunk, patch by patch, so a row's bits do not depend on the block
-// size. The rows are summed in order by the eigen-solve, so the result
+// (325, indexed by pca_tri_index) then sum p (25). A block stages two
+// chunks at a time in shared memory, converted to FP64 once per value; a
+// thread issues all of its loads of a round before it stores any (the
+// rounds are latency-bound: a few loads per thread, from L2). Its threads
+// own the 350 accumulators (thread t the ones t, t + blockDim, ...), each
+// summed patch by patch in four partial sums (patch k of the row into sum
+// k mod 4), so a row's bits do not depend on the block size or the
+// staging. The rows are summed in order by the eigen-solve, so the result
 // does not depend on scheduling (no atomics).
 constexpr int PC_CHUNK = kPcaChunk;
+constexpr int PC_STAGE = 2 * PC_CHUNK;                       // patches staged per round
+constexpr int PC_LOADS = (PC_STAGE * kPcaDim + 255) / 256;   // loads in flight per thread (256+ threads)
 
 struct CovSmem {
-    double sp[PC_CHUNK][kPcaDim + 1];
+    double sp[PC_STAGE][kPcaDim + 1];
 };
 
 template <class S>
@@ -100,25 +104,56 @@ __device__ __forceinline__ void pca_cov_row(Plane<S, 4> img, double* __restrict_
         if (a < kPcaTri) pca_pair(a, r[j], c[j]);
         else if (a < kPcaAcc) r[j] = a - kPcaTri;
     }
-    for (int ch = chunk0; ch < chunk1; ch++) {
-        const int base = ch * PC_CHUNK;
-        const int cnt = min(PC_CHUNK, n - base);
-        for (int i = t; i < cnt * kPcaDim; i += nth) {
-            const int k = i / kPcaDim, e = i % kPcaDim;
-            const int pidx = base + k;
-            const int px = (pidx % gw) * 8 + (e % 5) - 2, py = (pidx / gw) * 8 + (e / 5) - 2;
-            sm.sp[k][e] = double(to_f(*img.pxc(px, py)));
+    const int p_end = min(chunk1 * PC_CHUNK, n);
+    for (int base = chunk0 * PC_CHUNK; base < p_end; base += PC_STAGE) {
+        const int cnt = min(PC_STAGE, p_end - base);
+        const int nv = cnt * kPcaDim;
+        for (int i0 = 0; i0 < nv; i0 += PC_LOADS * nth) {
+            float v[PC_LOADS];
+#pragma unroll
+            for (int u = 0; u < PC_LOADS; u++) {
+                const int i = i0 + t + u * nth;
+                v[u] = 0.f;
+                if (i < nv) {
+                    const int k = i / kPcaDim, e = i % kPcaDim;
+                    const int pidx = base + k;
+                    const int px = (pidx % gw) * 8 + (e % 5) - 2, py = (pidx / gw) * 8 + (e / 5) - 2;
+                    v[u] = to_f(*img.pxc(px, py));
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < PC_LOADS; u++) {
+                const int i = i0 + t + u * nth;
+                if (i < nv) sm.sp[i / kPcaDim][i % kPcaDim] = double(v[u]);
+            }
         }
         __syncthreads();
+        // patch k into partial sum k mod 4 (base is a multiple of 4, and cnt
+        // is but in the last round of the level): products by FMA, the 25
+        // component sums by additions
 #pragma unroll
         for (int j = 0; j < 2; j++) {
             const int a = t + j * nth;
+            if (a >= kPcaAcc) continue;
+            const int rr = r[j], cc = c[j];
+            double* s4 = sum[j];
+            int k = 0;
             if (a < kPcaTri) {
-#pragma unroll 4
-                for (int k = 0; k < cnt; k++) sum[j][k & 3] += sm.sp[k][r[j]] * sm.sp[k][c[j]];
-            } else if (a < kPcaAcc) {
-#pragma unroll 4
-                for (int k = 0; k < cnt; k++) sum[j][k & 3] += sm.sp[k][r[j]];
+                for (; k + 4 <= cnt; k += 4) {
+#pragma unroll
+                    for (int q = 0; q < 4; q++) s4[q] = fma(sm.sp[k + q][rr], sm.sp[k + q][cc], s4[q]);
+                }
+#pragma unroll
+                for (int q = 0; q < 3; q++)
+                    if (k + q < cnt) s4[q] = fma(sm.sp[k + q][rr], sm.sp[k + q][cc], s4[q]);
+            } else {
+                for (; k + 4 <= cnt; k += 4) {
+#pragma unroll
+                    for (int q = 0; q < 4; q++) s4[q] += sm.sp[k + q][rr];
+                }
+#pragma unroll
+                for (int q = 0; q < 3; q++)
+                    if (k + q < cnt) s4[q] += sm.sp[k + q][rr];
             }
         }
         __syncthreads();

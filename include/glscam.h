@@ -242,8 +242,9 @@ typedef struct gls_frame_desc {
  * kernel runs every level of every frame (reconstruct, covariance,
  * eigen-solve and block matching, PyramidProcessor::denoise,
  * pyramid_processor.cpp:96-172) from a device work list whose tasks wait
- * on per-level counters, then the output transforms run; the results are
- * bit-identical to the stream-launched batch. The call returns after the
+ * on per-level counters, then the output transforms run; its block
+ * matching is the tensor-core matcher, so the results are bit-identical to
+ * the stream-launched batch with GLS_BM_TENSOR. The call returns after the
  * kernel, with GLS_ERR_TIMEOUT if a task's wait for its inputs ran past
  * its limit (2 s). Combined with GLS_GRAPH the whole sequence is recorded
  * and replayed. */
