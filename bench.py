@@ -844,6 +844,26 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def bm_dram_traffic(wl):
+    """DRAM bytes (read + write) of one frame's block-matching launches, from
+    the committed ncu capture of the default matcher on the 4032x3024
+    5-level workload (profiles/block_match_pair_dram_4032x3024.txt); None
+    for other workloads."""
+    f = Path(__file__).resolve().parent / "profiles" / "block_match_pair_dram_4032x3024.txt"
+    if (wl.width, wl.height, wl.levels) != (4032, 3024, 5) or not f.exists():
+        return None
+    vals = {}
+    for line in f.read_text().splitlines():
+        if "=" in line and line.split("=")[0].strip() in ("traffic_bytes_per_frame", "algorithmic_bytes_per_frame"):
+            vals[line.split("=")[0].strip()] = int(line.split("=")[1])
+    if "traffic_bytes_per_frame" not in vals:
+        return None
+    return {"bytes": vals["traffic_bytes_per_frame"],
+            "note": "dram__bytes_read.sum + dram__bytes_write.sum of one frame's 5 block-matching launches (one ncu "
+                    "capture, profiles/block_match_pair_dram_4032x3024.txt), per frame like achieved; algorithmic "
+                    f"bytes per frame {vals.get('algorithmic_bytes_per_frame')}"}
+
+
 def main_config(wl, world, frames=N_ROTATE):
     """The workload description shared by both arms' lines."""
     return {"workload": wl.name, "frame": f"{wl.width}x{wl.height} RGGB 12-bit", "levels": wl.levels,
@@ -1003,6 +1023,7 @@ def main():
 
     # roofline of the dominant kernel (block matching) from the live event times
     bm = per_kernel.get("block_match", {"launches": 1, "ms": float("nan")})
+    traffic = bm_dram_traffic(wl) if os.environ.get("GLS_BM_KERNEL", "") != "mma" else None
     px = sum((W >> i) * (H >> i) for i in range(wl.levels))
     taps = 21 * 21
     flop_per_tap = 50.0  # 8-D distance 24, chroma 6, two weights 8, accumulate 10 (FMA = 2)
@@ -1029,7 +1050,9 @@ def main():
         "speedup_vs_fp32_plain": ms32 / (ms_step / B),
         "roofline": {"bound": "fp32+mufu", "kernel": "block_match",
                      "achieved": bm_tflops, "peak": fp32_peak, "unit": "TFLOP/s", "frac": bm_tflops / fp32_peak,
-                     "mufu_frac": bm_mufu / mufu_rate, "traffic": None,
+                     "mufu_frac": bm_mufu / mufu_rate,
+                     "traffic": traffic["bytes"] if traffic else None,
+                     "traffic_note": traffic["note"] if traffic else "no DRAM capture for this matcher",
                      "share": bm["ms"] / total_prof_ms if total_prof_ms else None,
                      "ms_per_launch": bm["ms"] / max(1, bm["launches"]),
                      "peak_note": "nominal SIMT FP32 (148 SMs x 128 lanes x 2 x sampled SM clock); "

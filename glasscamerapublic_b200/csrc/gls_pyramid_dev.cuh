@@ -481,12 +481,36 @@ __device__ inline void pca_eigen_block(const double* __restrict__ part, int n_bl
             if (lane < EJ_N) sm.Z[lane][c] = z;
             __syncwarp();
         }
-        if (lane == 0) {
+        // select_pca_basis; when every eigenvalue is kept (the usual case) it
+        // reduces to signing each column by its largest-magnitude entry (first
+        // on ties), done here by the warp, lane = row, with the same result
+        const double lam0 = sm.lam[0] > 0.0 ? sm.lam[0] : 0.0;
+        bool all_kept = lam0 > 0.0;
+        for (int c = 0; c < EJ_TOP; c++) all_kept = all_kept && sm.lam[c] > 1e-9 * lam0;
+        if (all_kept) {
+            for (int c = 0; c < EJ_TOP; c++) {
+                const double v = lane < EJ_N ? sm.Z[lane][c] : 0.0;
+                double a = lane < EJ_N ? fabs(v) : -1.0;
+                int idx = lane;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double a2 = __shfl_xor_sync(0xffffffffu, a, o);
+                    const int i2 = __shfl_xor_sync(0xffffffffu, idx, o);
+                    if (a2 > a || (a2 == a && i2 < idx)) {
+                        a = a2;
+                        idx = i2;
+                    }
+                }
+                const double vmax = __shfl_sync(0xffffffffu, v, idx);
+                const double sgn = vmax < 0 ? -1.0 : 1.0;
+                if (lane < EJ_N) basis[lane * 8 + c] = float(v * sgn);
+            }
+        } else if (lane == 0) {
             double ev[EJ_TOP];
             for (int c = 0; c < EJ_TOP; c++) ev[c] = sm.lam[c];
             select_pca_basis(ev, &sm.Z[0][0], EJ_TOP + 1, sm.work, basis);
-            if (status) *status = sm.bad ? -1 : EJ_INV_ITERS;
         }
+        if (lane == 0 && status) *status = sm.bad ? -1 : EJ_INV_ITERS;
     }
 }
 
