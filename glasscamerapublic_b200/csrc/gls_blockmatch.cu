@@ -881,8 +881,8 @@ __global__ void __launch_bounds__(BM_THREADS, 2)
             }
             done = &cnt[tk.lev].sn;
         } else if (type == PT_COV) {
-            const int c0 = int(item) * kPcaCovGroup;
-            pca_cov_row<__half>(L.layer, L.part + size_t(item) * kPcaAcc, c0, min(c0 + kPcaCovGroup, L.chunks), sm.cov);
+            const int c0 = int(item) * L.cov_group;
+            pca_cov_row<__half>(L.layer, L.part + size_t(item) * kPcaAcc, c0, min(c0 + L.cov_group, L.chunks), sm.cov);
             done = &cnt[tk.lev].cov;
         } else if (type == PT_EIG) {
             persistent_eigen(L, sm.eig);

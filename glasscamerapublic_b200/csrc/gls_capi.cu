@@ -1078,6 +1078,7 @@ static gls_status persistent_plan(gls_converter* conv, const gls_frame_desc* fra
             d.n_sn = i < L - 1 ? tiles : 0;
             d.n_cov = pca_cov_rows(wi, hi);
             d.chunks = pca_cov_chunks(wi, hi);
+            d.cov_group = pca_cov_group(d.chunks);
             d.coarser = i < L - 1 ? first[f] + i + 1 : -1;
             lv.push_back(d);
         }

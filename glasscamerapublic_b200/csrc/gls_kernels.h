@@ -90,9 +90,15 @@ struct SubtractArgs {
 // patches (325, row-major) followed by sum p (25), FP64.
 constexpr int kPcaAcc = 25 + 325;
 constexpr int kPcaDim = 25, kPcaComp = 8;
-constexpr int kPcaCovGroup = 4;  // 64-patch chunks per covariance partial row
+// 64-patch chunks per covariance partial row of a level with `chunks`
+// chunks: about 372 rows per level (a few per SM) for the fine levels, one
+// chunk per row for the coarse ones (short per-block chains), at most 16
+__host__ __device__ inline int pca_cov_group(int chunks) {
+    const int g = chunks / 372;
+    return g < 1 ? 1 : (g > 16 ? 16 : g);
+}
 int pca_cov_chunks(int w, int h);  // 64-patch chunks of a level
-int pca_cov_rows(int w, int h);    // partial rows of a level: chunks / kPcaCovGroup, rounded up
+int pca_cov_rows(int w, int h);    // partial rows of a level: chunks / pca_cov_group(chunks), rounded up
 
 template <class S, int C>
 void launch_downsample(Plane<S, C> in, Plane<S, C> out, cudaStream_t s);
@@ -145,6 +151,7 @@ struct PLevel {
     int n_sn, n_cov, n_bm;                // task counts of the level
     int tiles_x;                          // 32-pixel tiles across the level
     int chunks;                           // 64-patch covariance chunks
+    int cov_group;                        // chunks per covariance row (pca_cov_group)
     int coarser;                          // descriptor of the next coarser level, -1 at the coarsest
 };
 struct PCounters {

@@ -1,7 +1,8 @@
 // gls_pyramid.cu — kernels of PyramidProcessor<levels>::denoise
 // (pyramid_processor.cpp:96-172): Gaussian-pyramid downsample, the
 // reconstruct (noise subtraction) step, the per-level PCA patch basis
-// (covariance + FP64 Jacobi eigen-solve on the device) and the 5x5-patch
+// (covariance + FP64 tridiagonal eigen-solve on the device; two-sided
+// Jacobi on the host for GLS_HOST_PCA) and the 5x5-patch
 // PCA projection. The block-matching denoise is in gls_blockmatch.cu.
 #include <cmath>
 #include <cstdio>
@@ -90,13 +91,13 @@ __global__ void __launch_bounds__(256) k_subtract_noise(Plane<S, 4> in, Plane<S,
 }
 
 template <class S>
-__global__ void __launch_bounds__(352) k_pca_cov(Plane<S, 4> img, double* __restrict__ part, int group, int n_chunks) {
+__global__ void __launch_bounds__(352, 3) k_pca_cov(Plane<S, 4> img, double* __restrict__ part, int group, int n_chunks) {
     __shared__ CovSmem sm;
     const int c0 = blockIdx.x * group;
     pca_cov_row<S>(img, part + size_t(blockIdx.x) * kPcaAcc, c0, min(c0 + group, n_chunks), sm);
 }
 
-constexpr int EJ_THREADS = 704;  // 22 warps: two partial sums per accumulator in the prologue
+constexpr int EJ_THREADS = 704;  // 22 warps: the prologue's 700 partial sums at once
 
 __global__ void __launch_bounds__(EJ_THREADS) k_pca_eigen(const double* __restrict__ part, int n_blocks,
                                                          int n_patches, float* __restrict__ basis, int* status) {
@@ -174,13 +175,17 @@ int pca_cov_chunks(int w, int h) {
     return n <= 0 ? 0 : (n + PC_CHUNK - 1) / PC_CHUNK;
 }
 
-int pca_cov_rows(int w, int h) { return (pca_cov_chunks(w, h) + kPcaCovGroup - 1) / kPcaCovGroup; }
+int pca_cov_rows(int w, int h) {
+    const int chunks = pca_cov_chunks(w, h), g = pca_cov_group(chunks);
+    return (chunks + g - 1) / g;
+}
 
 template <class S>
 void launch_pca_cov(Plane<S, 4> img, double* part, cudaStream_t s) {
     const int rows = pca_cov_rows(img.w, img.h);
     if (rows == 0) return;
-    k_pca_cov<S><<<rows, 352, 0, s>>>(img, part, kPcaCovGroup, pca_cov_chunks(img.w, img.h));
+    const int chunks = pca_cov_chunks(img.w, img.h);
+    k_pca_cov<S><<<rows, 352, 0, s>>>(img, part, pca_cov_group(chunks), chunks);
 }
 
 template <class S>

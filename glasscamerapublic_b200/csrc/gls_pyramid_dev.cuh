@@ -71,8 +71,8 @@ __device__ __forceinline__ void subtract_noise_px(const Plane<S, 4>& in, const P
 // the 5x5 luma neighbourhoods of (8x, 8y), x < W/8, y < H/8, taken in
 // chunks of 64. Partial row r holds the FP64 sums over chunks
 // [g r, g (r + 1)) (g chunks per row): the upper triangle of sum p p^T
-// (325, indexed by pca_tri_index) then sum p (25). A block stages two
-// chunks at a time in shared memory, converted to FP64 once per value; a
+// (325, indexed by pca_tri_index) then sum p (25). A block stages a
+// chunk at a time in shared memory, converted to FP64 once per value; a
 // thread issues all of its loads of a round before it stores any (the
 // rounds are latency-bound: a few loads per thread, from L2). Its threads
 // own the 350 accumulators (thread t the ones t, t + blockDim, ...), each
@@ -81,7 +81,7 @@ __device__ __forceinline__ void subtract_noise_px(const Plane<S, 4>& in, const P
 // staging. The rows are summed in order by the eigen-solve, so the result
 // does not depend on scheduling (no atomics).
 constexpr int PC_CHUNK = kPcaChunk;
-constexpr int PC_STAGE = 2 * PC_CHUNK;                       // patches staged per round
+constexpr int PC_STAGE = PC_CHUNK;                           // patches staged per round
 constexpr int PC_LOADS = (PC_STAGE * kPcaDim + 255) / 256;   // loads in flight per thread (256+ threads)
 
 struct CovSmem {
@@ -104,6 +104,11 @@ __device__ __forceinline__ void pca_cov_row(Plane<S, 4> img, double* __restrict_
         if (a < kPcaTri) pca_pair(a, r[j], c[j]);
         else if (a < kPcaAcc) r[j] = a - kPcaTri;
     }
+    // patch index -> (column, row) of the patch grid by a multiply-high:
+    // q = umulhi(p, floor((2^32 - 1) / gw) + 1) is p / gw exactly while
+    // p * gw < 2^32 (every frame up to ~100 MP); a division otherwise
+    const bool fast_div = gw > 1 && uint64_t(n) * uint64_t(gw) < (1ull << 32);
+    const uint32_t gmul = fast_div ? 0xffffffffu / uint32_t(gw) + 1u : 0u;
     const int p_end = min(chunk1 * PC_CHUNK, n);
     for (int base = chunk0 * PC_CHUNK; base < p_end; base += PC_STAGE) {
         const int cnt = min(PC_STAGE, p_end - base);
@@ -115,9 +120,11 @@ __device__ __forceinline__ void pca_cov_row(Plane<S, 4> img, double* __restrict_
                 const int i = i0 + t + u * nth;
                 v[u] = 0.f;
                 if (i < nv) {
-                    const int k = i / kPcaDim, e = i % kPcaDim;
+                    const int k = i / kPcaDim, e = i - k * kPcaDim;  // constant divisors
                     const int pidx = base + k;
-                    const int px = (pidx % gw) * 8 + (e % 5) - 2, py = (pidx / gw) * 8 + (e / 5) - 2;
+                    const int prow = fast_div ? int(__umulhi(uint32_t(pidx), gmul)) : pidx / gw;
+                    const int ey = e / 5;
+                    const int px = (pidx - prow * gw) * 8 + (e - ey * 5) - 2, py = prow * 8 + ey - 2;
                     v[u] = to_f(*img.pxc(px, py));
                 }
             }
@@ -173,9 +180,9 @@ __device__ __forceinline__ void pca_cov_row(Plane<S, 4> img, double* __restrict_
 // bisection / inverse-iteration methods of sections 8.4.1 and 8.2.2
 // (the tred2 / tridiagonal bisection / tinvit sequence of EISPACK):
 //   1. Householder tridiagonalisation, A = Q T Q^T, Q = H_0 ... H_22: 23
-//      reflector steps, each a warp-reduced column norm, the product
-//      p = beta A v (one warp per row), and the rank-2 update of the
-//      trailing block by all threads (matrix in shared memory);
+//      reflector steps, each a column norm, the product p = beta A v (a
+//      thread per row), and the rank-2 update of the trailing block by all
+//      threads (matrix in shared memory);
 //   2. the 8 largest eigenvalues of T by Sturm-sequence multisection:
 //      warp w brackets eigenvalue 24 - w (ascending order); its 32 lanes
 //      count the eigenvalues below 32 points of the bracket, which shrinks
@@ -184,10 +191,13 @@ __device__ __forceinline__ void pca_cov_row(Plane<S, 4> img, double* __restrict_
 //      T - lambda I is factored once with partial pivoting (lane 0 of the
 //      eigenvalue's warp) and solved three times from a start vector of its
 //      own; tiny pivots are raised to eps ||T|| so the solve stays finite;
-//   4. the back-transform z = H_0 (H_1 (... H_22 y)) by the warp, one
-//      reflector at a time, and modified Gram-Schmidt of the 8 vectors in
-//      eigenvalue order (exactly equal eigenvalues give an orthonormal basis
-//      of their eigenspace; distinct ones are already orthogonal).
+//   4. the back-transform z = H_0 (H_1 (... H_22 y)), one reflector at a
+//      time for all 8 vectors (a thread per dot product, then the block),
+//      and Gram-Schmidt of the 8 vectors in eigenvalue order, the classical
+//      form applied twice (exactly equal eigenvalues give an orthonormal
+//      basis of their eigenspace; distinct ones are already orthogonal).
+//      FP64 warp shuffles are slow on this part (about 15 lanes per SM per
+//      cycle), so no step reduces across a warp's lanes.
 // The top-8 eigenvectors (descending eigenvalue, each signed so its
 // largest-magnitude entry is positive; eigenvalues <= 1e-9 of the largest
 // completed as in select_pca_basis) are written as a row-major 25x8 FP32
@@ -209,6 +219,17 @@ __device__ __forceinline__ double rcp_nr(double x) {
     r = fma(r, e, r);
     e = fma(-x, r, 1.0);
     return fma(r, e, r);
+}
+
+// 1 / sqrt(x) to FP64 accuracy for normal x > 0: the hardware approximation
+// refined by two steps of Newton's method on f(r) = 1 / r^2 - x,
+// r <- r (3 - x r^2) / 2, each doubling the correct bits.
+__device__ __forceinline__ double rsqrt_nr(double x) {
+    double r;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    const double hx = 0.5 * x;
+    r = r * fma(-hx * r, r, 1.5);
+    return r * fma(-hx * r, r, 1.5);
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -233,11 +254,29 @@ __device__ __forceinline__ int sturm_count(const double* d, const double* ee, do
     return cnt;
 }
 
+// sum_{i in [i0, i1)} a[i * sa] * b[i * sb] in four interleaved partial
+// FP64 chains (i - i0 mod 4), added in a fixed order: a quarter of the
+// latency of one chain
+__device__ __forceinline__ double dot4(const double* a, int sa, const double* b, int sb, int i0, int i1) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    int i = i0;
+    for (; i + 4 <= i1; i += 4) {
+        s0 = fma(a[i * sa], b[i * sb], s0);
+        s1 = fma(a[(i + 1) * sa], b[(i + 1) * sb], s1);
+        s2 = fma(a[(i + 2) * sa], b[(i + 2) * sb], s2);
+        s3 = fma(a[(i + 3) * sa], b[(i + 3) * sb], s3);
+    }
+    if (i < i1) s0 = fma(a[i * sa], b[i * sb], s0);
+    if (i + 1 < i1) s1 = fma(a[(i + 1) * sa], b[(i + 1) * sb], s1);
+    if (i + 2 < i1) s2 = fma(a[(i + 2) * sa], b[(i + 2) * sb], s2);
+    return (s0 + s1) + (s2 + s3);
+}
+
 struct EigenSmem {
     double acc[kPcaAcc];
     double A[EJ_N][EJ_N + 1];       // covariance, reduced in place
     double V[EJ_N - 2][EJ_N];       // Householder vectors (zero above k + 1)
-    double beta[EJ_N - 2];
+    double beta[EJ_N - 2], vk1[EJ_N - 2];
     double d[EJ_N], e[EJ_N], ee[EJ_N];
     double p[EJ_N], w[EJ_N];
     double lam[EJ_TOP];
@@ -296,46 +335,44 @@ __device__ inline void pca_eigen_block(const double* __restrict__ part, int n_bl
     }
     __syncthreads();
 
-    // ---- 1. Householder tridiagonalisation
+    // ---- 1. Householder tridiagonalisation. Per step: thread 0 forms the
+    //         reflector from column k (a sequential FP64 norm); thread j > k
+    //         forms p_j = beta sum_i A[j][i] v_i; every thread forms
+    //         K = (beta / 2) p.v and updates its entries of the trailing
+    //         block, A' -= v w^T + w v^T with w = p - K v. v is column k below
+    //         the diagonal with its first entry replaced (vk1), read from A
+    //         itself; column k is outside every later trailing block.
     for (int k = 0; k < EJ_N - 2; k++) {
-        if (warp == 0) {
-            // v from column k below the diagonal: x = A[k+1..][k]
-            const double x = (lane > k && lane < EJ_N) ? sm.A[lane][k] : 0.0;
-            const double nrm2 = warp_sum(x * x);
-            const double x1 = __shfl_sync(0xffffffffu, x, k + 1);
-            const double nrm = sqrt(nrm2);
+        if (t == 0) {
+            // the norm and 1 / (v.v / 2) by refined hardware approximations:
+            // the IEEE square root and division are long serial sequences
+            // on this single thread's path
+            const double nrm2 = dot4(&sm.A[0][k], EJ_N + 1, &sm.A[0][k], EJ_N + 1, k + 1, EJ_N);
+            const double x1 = sm.A[k + 1][k];
+            const bool skip = !(nrm2 > 1e-280);
+            const double nrm = skip ? 0.0 : nrm2 * rsqrt_nr(nrm2);
             const double alpha = x1 >= 0.0 ? -nrm : nrm;
             const double den = nrm2 - alpha * x1;  // v.v / 2 > 0 unless the column is zero
-            const bool skip = !(nrm2 > 1e-280);
-            const double v = skip ? 0.0 : (lane == k + 1 ? x1 - alpha : x);
-            if (lane < EJ_N) sm.V[k][lane] = v;
-            if (lane == 0) {
-                sm.beta[k] = skip ? 0.0 : 1.0 / den;
-                sm.d[k] = sm.A[k][k];
-                sm.e[k] = skip ? x1 : alpha;
-            }
+            sm.beta[k] = skip ? 0.0 : rcp_nr(den);
+            sm.vk1[k] = skip ? 0.0 : x1 - alpha;
+            sm.d[k] = sm.A[k][k];
+            sm.e[k] = skip ? x1 : alpha;
         }
         __syncthreads();
         const double beta = sm.beta[k];
+        if (t < EJ_N) sm.V[k][t] = beta == 0.0 || t <= k ? 0.0 : (t == k + 1 ? sm.vk1[k] : sm.A[t][k]);
         if (beta == 0.0) continue;  // uniform: the column is already reduced
-        // p = beta A' v, one warp per row j > k
-        for (int j = k + 1 + warp; j < EJ_N; j += nth / 32) {
-            const double pr = warp_sum(lane < EJ_N ? sm.A[j][lane] * sm.V[k][lane] : 0.0);
-            if (lane == 0) sm.p[j] = beta * pr;
-        }
+        const double v1 = sm.vk1[k];
+        if (t > k && t < EJ_N)
+            sm.p[t] = beta * fma(sm.A[t][k + 1], v1, dot4(&sm.A[t][0], 1, &sm.A[0][k], EJ_N + 1, k + 2, EJ_N));
         __syncthreads();
-        if (warp == 0) {  // w = p - (beta/2)(p.v) v
-            const double vj = lane > k && lane < EJ_N ? sm.V[k][lane] : 0.0;
-            const double pj = lane > k && lane < EJ_N ? sm.p[lane] : 0.0;
-            const double pv = warp_sum(pj * vj);
-            if (lane > k && lane < EJ_N) sm.w[lane] = pj - 0.5 * beta * pv * vj;
-        }
-        __syncthreads();
-        // A' -= v w^T + w v^T on the trailing block
+        const double K = 0.5 * beta * fma(sm.p[k + 1], v1, dot4(sm.p, 1, &sm.A[0][k], EJ_N + 1, k + 2, EJ_N));
         const int m = EJ_N - k - 1;
         for (int q = t; q < m * m; q += nth) {
             const int i = k + 1 + q / m, j = k + 1 + q % m;
-            sm.A[i][j] -= sm.V[k][i] * sm.w[j] + sm.w[i] * sm.V[k][j];
+            const double vi = i == k + 1 ? v1 : sm.A[i][k], vj = j == k + 1 ? v1 : sm.A[j][k];
+            const double wi = sm.p[i] - K * vi, wj = sm.p[j] - K * vj;
+            sm.A[i][j] -= vi * wj + wi * vj;
         }
         __syncthreads();
     }
@@ -448,70 +485,79 @@ __device__ inline void pca_eigen_block(const double* __restrict__ part, int n_bl
             }
             double mx = 0.0;                            // rescale by the largest entry
             for (int i = 0; i < EJ_N; i++) mx = fmax(mx, fabs(y[i]));
-            const double inv = mx > 0.0 && mx < 1e300 ? 1.0 / mx : 0.0;
+            const double inv = mx > 1e-290 && mx < 1e300 ? rcp_nr(mx) : 0.0;
             for (int i = 0; i < EJ_N; i++) y[i] *= inv;
         }
     }
     __syncthreads();
-    // ---- 4. back-transform by the reflectors (warp c, lane = row), then
-    //         modified Gram-Schmidt in eigenvalue order (warp 0)
-    if (warp < EJ_TOP) {
-        const int c = warp;
-        double z = lane < EJ_N ? sm.y[c][lane] : 0.0;
-        for (int k = EJ_N - 3; k >= 0; k--) {
-            const double vk = lane < EJ_N ? sm.V[k][lane] : 0.0;
-            const double dot = warp_sum(vk * z);
-            z -= sm.beta[k] * dot * vk;
+    // ---- 4. back-transform z = H_0 (H_1 (... H_22 y)), one reflector at a
+    //         time for the 8 vectors: thread c forms the dot product of
+    //         reflector k with vector c (a sequential FP64 chain, no warp
+    //         reduction), then the block updates the vectors
+    for (int k = EJ_N - 3; k >= 0; k--) {
+        if (sm.beta[k] == 0.0) continue;  // uniform: the reflector is the identity
+        if (t < EJ_TOP) sm.p[t] = sm.beta[k] * dot4(sm.V[k], 1, sm.y[t], 1, k + 1, EJ_N);  // V[k][i] = 0 for i <= k
+        __syncthreads();
+        for (int q = t; q < EJ_TOP * EJ_N; q += nth) {
+            const int c = q / EJ_N, i = q % EJ_N;
+            if (i > k) sm.y[c][i] -= sm.p[c] * sm.V[k][i];
         }
-        if (lane < EJ_N) sm.Z[lane][c] = z;
+        __syncthreads();
     }
-    __syncthreads();
-    if (warp == 0) {
-        for (int c = 0; c < EJ_TOP; c++) {
-            double z = lane < EJ_N ? sm.Z[lane][c] : 0.0;
-            for (int pass = 0; pass < 2; pass++)
-                for (int k = 0; k < c; k++) {
-                    const double zk = lane < EJ_N ? sm.Z[lane][k] : 0.0;
-                    z -= warp_sum(zk * z) * zk;
-                }
-            const double nn = warp_sum(z * z);
-            const bool ok = nn > 0.0 && nn < 1e300;
-            z = ok ? z * (1.0 / sqrt(nn)) : 0.0;
-            if (!ok && lane == 0) sm.bad = 1;
-            if (lane < EJ_N) sm.Z[lane][c] = z;
-            __syncwarp();
-        }
-        // select_pca_basis; when every eigenvalue is kept (the usual case) it
-        // reduces to signing each column by its largest-magnitude entry (first
-        // on ties), done here by the warp, lane = row, with the same result
-        const double lam0 = sm.lam[0] > 0.0 ? sm.lam[0] : 0.0;
-        bool all_kept = lam0 > 0.0;
-        for (int c = 0; c < EJ_TOP; c++) all_kept = all_kept && sm.lam[c] > 1e-9 * lam0;
-        if (all_kept) {
-            for (int c = 0; c < EJ_TOP; c++) {
-                const double v = lane < EJ_N ? sm.Z[lane][c] : 0.0;
-                double a = lane < EJ_N ? fabs(v) : -1.0;
-                int idx = lane;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    const double a2 = __shfl_xor_sync(0xffffffffu, a, o);
-                    const int i2 = __shfl_xor_sync(0xffffffffu, idx, o);
-                    if (a2 > a || (a2 == a && i2 < idx)) {
-                        a = a2;
-                        idx = i2;
-                    }
-                }
-                const double vmax = __shfl_sync(0xffffffffu, v, idx);
-                const double sgn = vmax < 0 ? -1.0 : 1.0;
-                if (lane < EJ_N) basis[lane * 8 + c] = float(v * sgn);
+    // ---- 5. Gram-Schmidt in eigenvalue order, classical, twice per vector
+    //         (as stable as the modified form): the dot products of vector c
+    //         with the earlier ones by c threads at once, then the update by
+    //         row; exactly equal eigenvalues give an orthonormal basis of
+    //         their eigenspace, distinct ones are already orthogonal
+    for (int c = 0; c < EJ_TOP; c++) {
+        for (int pass = 0; pass < 2; pass++) {
+            if (c == 0) break;
+            if (t < c) sm.w[t] = dot4(sm.y[t], 1, sm.y[c], 1, 0, EJ_N);
+            __syncthreads();
+            if (t < EJ_N) {
+                double v = sm.y[c][t];
+                for (int k2 = 0; k2 < c; k2++) v -= sm.w[k2] * sm.y[k2][t];
+                sm.y[c][t] = v;
             }
-        } else if (lane == 0) {
-            double ev[EJ_TOP];
-            for (int c = 0; c < EJ_TOP; c++) ev[c] = sm.lam[c];
-            select_pca_basis(ev, &sm.Z[0][0], EJ_TOP + 1, sm.work, basis);
+            __syncthreads();
         }
-        if (lane == 0 && status) *status = sm.bad ? -1 : EJ_INV_ITERS;
+        if (t == 0) {
+            const double nn = dot4(sm.y[c], 1, sm.y[c], 1, 0, EJ_N);
+            const bool ok = nn > 1e-290 && nn < 1e300;
+            sm.w[EJ_TOP] = ok ? rsqrt_nr(nn) : 0.0;
+            if (!ok) sm.bad = 1;
+        }
+        __syncthreads();
+        if (t < EJ_N) sm.y[c][t] = sm.w[EJ_TOP] != 0.0 ? sm.y[c][t] * sm.w[EJ_TOP] : 0.0;  // a non-finite vector is zeroed
+        __syncthreads();
     }
+    for (int q = t; q < EJ_TOP * EJ_N; q += nth) sm.Z[q % EJ_N][q / EJ_N] = sm.y[q / EJ_N][q % EJ_N];
+    __syncthreads();
+    // ---- 6. select_pca_basis. When every eigenvalue is kept (the usual
+    //         case) it reduces to signing each column by its largest-magnitude
+    //         entry (first on ties): thread c scans column c, then the block
+    //         writes the basis, with the same result
+    const double lam0 = sm.lam[0] > 0.0 ? sm.lam[0] : 0.0;
+    bool all_kept = lam0 > 0.0;
+    for (int c = 0; c < EJ_TOP; c++) all_kept = all_kept && sm.lam[c] > 1e-9 * lam0;
+    if (all_kept) {
+        if (t < EJ_TOP) {
+            int amax = 0;
+            for (int r = 1; r < EJ_N; r++)
+                if (fabs(sm.y[t][r]) > fabs(sm.y[t][amax])) amax = r;
+            sm.w[t] = sm.y[t][amax] < 0 ? -1.0 : 1.0;
+        }
+        __syncthreads();
+        for (int q = t; q < EJ_N * EJ_TOP; q += nth) {
+            const int r = q / EJ_TOP, c = q % EJ_TOP;
+            basis[q] = float(sm.y[c][r] * sm.w[c]);
+        }
+    } else if (t == 0) {
+        double ev[EJ_TOP];
+        for (int c = 0; c < EJ_TOP; c++) ev[c] = sm.lam[c];
+        select_pca_basis(ev, &sm.Z[0][0], EJ_TOP + 1, sm.work, basis);
+    }
+    if (t == 0 && status) *status = sm.bad ? -1 : EJ_INV_ITERS;
 }
 
 
