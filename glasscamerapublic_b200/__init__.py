@@ -275,7 +275,9 @@ def device_memory(reset_peak: bool = False) -> tuple[int, int]:
 
 
 def block_match_tiles() -> list:
-    """The FP16 block matcher's autotuned tile heights: [(w, h, height)]."""
+    """The FP16 block matcher's autotuned tile variants: [(w, h, variant)],
+    variant = 10 x thread rows + pixels per thread (84, 162: 32x32-pixel
+    tiles; 44, 82: 32x16)."""
     buf = (C.c_int32 * 192)()
     n = C.c_int32(0)
     check(lib().gls_block_match_tiles(buf, 64, C.byref(n)))

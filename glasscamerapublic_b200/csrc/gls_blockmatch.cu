@@ -196,14 +196,19 @@ __global__ void __launch_bounds__(256) k_block_match_plain(Plane<S, 4> img, Plan
 //     is sw / sqrt(2 log2 e) times it;
 //   * both exponentials are ex2.approx (the reference uses half-precision
 //     exp under fast math here).
-constexpr int BX_NP = 4, BX_TX = 32, BX_W = BX_TX + 20;
-// tile height variants (TY threads down, 4 pixels each): 32 x 32 or 32 x 16
-// pixels; the autotuner picks one per level size (launch_block_match)
-template <int TY>
+constexpr int BX_TX = 32, BX_W = BX_TX + 20;
+// tile variants: TY thread rows of NP vertically adjacent pixels (NP = 4:
+// two pixel pairs per thread, NP = 2: one), tiles of 32 x (NP TY) = 32 x 32
+// or 32 x 16 pixels; the autotuner picks one per level size
+// (launch_block_match). Variant code 10 TY + NP: 84, 44, 82, 162.
+template <int TY, int NP>
 struct BxTile {
-    static constexpr int H = BX_NP * TY + 20;  // window rows staged
-    static constexpr int LH = H + 4;           // luma rows staged
+    static constexpr int H = NP * TY + 20;  // window rows staged
+    static constexpr int LH = H + 4;        // luma rows staged
     static constexpr int THREADS = BX_TX * TY;
+    static constexpr int MIN_BLOCKS = THREADS >= 512 ? 1 : (NP == 4 && TY == 8 ? 2 : 3);
+    static_assert(NP == 2 || NP == 4, "one or two pixel pairs per thread");
+    static_assert(NP * TY == 16 || NP * TY == 32, "tile heights divide the 32-row centring tiles");
 };
 
 // ---------------------------------------------------------------- FFMA2 form
@@ -237,10 +242,10 @@ __device__ __forceinline__ u64 add2(u64 a, u64 b) {
     return d;
 }
 
-template <int TY>
+template <int H>
 struct BmPairSmem {
-    uint4 pca[BxTile<TY>::H * BX_W];   // q - c, 8 halves
-    float4 ycc[BxTile<TY>::H * BX_W];  // Y, Cb, Cr, |q - c|^2
+    uint4 pca[H * BX_W];   // q - c, 8 halves
+    float4 ycc[H * BX_W];  // Y, Cb, Cr, |q - c|^2
     float4 sp[22 * 21];       // (sw(j)/sqrt(lk), sw(j-1)/sqrt(lk), -log2 sw(j), -log2 sw(j-1)), j = table row
 };
 
@@ -303,15 +308,15 @@ constexpr int BX_LW = BX_W + 4;  // luma tile width, origin (x0 - 12, y0 - 12)
 
 __device__ __forceinline__ uint32_t h2u(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
 
-template <int TY>
-__global__ void __launch_bounds__(BxTile<TY>::THREADS, TY == 8 ? 2 : 3)
+template <int TY, int NP>
+__global__ void __launch_bounds__(BxTile<TY, NP>::THREADS, BxTile<TY, NP>::MIN_BLOCKS)
     k_block_match_pair(Plane<__half, 4> img, Plane<__half, 2> grad, const float* __restrict__ basis,
                        Plane<__half, 4> out, BlockMatchArgs a) {
-    using T = BxTile<TY>;
-    constexpr int BX_H = T::H, BX_LH = T::LH, NT = T::THREADS;
+    using T = BxTile<TY, NP>;
+    constexpr int BX_H = T::H, BX_LH = T::LH, NT = T::THREADS, BX_NP = NP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    BmPairSmem<TY>& sm = *reinterpret_cast<BmPairSmem<TY>*>(smem_raw);
-    __half* luma = reinterpret_cast<__half*>(smem_raw + sizeof(BmPairSmem<TY>));  // BX_LH x BX_LW
+    BmPairSmem<BX_H>& sm = *reinterpret_cast<BmPairSmem<BX_H>*>(smem_raw);
+    __half* luma = reinterpret_cast<__half*>(smem_raw + sizeof(BmPairSmem<BX_H>));  // BX_LH x BX_LW
     __shared__ float cen[8];
     __shared__ float bsm[25][8];
     const int x0 = blockIdx.x * BX_TX, y0 = blockIdx.y * (BX_NP * TY);
@@ -419,32 +424,32 @@ __global__ void __launch_bounds__(BxTile<TY>::THREADS, TY == 8 ? 2 : 3)
         o1[p] = c1[p] * in.y;
         o2[p] = c2[p] * in.z;
     }
-    BmPair PA, PB;
-    for (int c = 0; c < 8; c++) {
-        PA.p[c] = pk2(-2.f * kl[0] * pc[0][c], -2.f * kl[1] * pc[1][c]);
-        PB.p[c] = pk2(-2.f * kl[2] * pc[2][c], -2.f * kl[3] * pc[3][c]);
+    BmPair PP[NP / 2];
+#pragma unroll
+    for (int q = 0; q < NP / 2; q++) {
+        for (int c = 0; c < 8; c++) PP[q].p[c] = pk2(-2.f * kl[2 * q] * pc[2 * q][c], -2.f * kl[2 * q + 1] * pc[2 * q + 1][c]);
+        PP[q].kl = pk2(kl[2 * q], kl[2 * q + 1]);
+        PP[q].base = pk2(base[2 * q], base[2 * q + 1]);
+        PP[q].c1 = pk2(c1[2 * q], c1[2 * q + 1]);
+        PP[q].c2 = pk2(c2[2 * q], c2[2 * q + 1]);
+        PP[q].no1 = pk2(-o1[2 * q], -o1[2 * q + 1]);
+        PP[q].no2 = pk2(-o2[2 * q], -o2[2 * q + 1]);
     }
-    PA.kl = pk2(kl[0], kl[1]);
-    PB.kl = pk2(kl[2], kl[3]);
-    PA.base = pk2(base[0], base[1]);
-    PB.base = pk2(base[2], base[3]);
-    PA.c1 = pk2(c1[0], c1[1]);
-    PB.c1 = pk2(c1[2], c1[3]);
-    PA.c2 = pk2(c2[0], c2[1]);
-    PB.c2 = pk2(c2[2], c2[3]);
-    PA.no1 = pk2(-o1[0], -o1[1]);
-    PB.no1 = pk2(-o1[2], -o1[3]);
-    PA.no2 = pk2(-o2[0], -o2[1]);
-    PB.no2 = pk2(-o2[2], -o2[3]);
     u64 acc[2][5];
     for (int k = 0; k < 5; k++) acc[0][k] = acc[1][k] = pk2(0.f, 0.f);
     const int col = threadIdx.x, row0 = BX_NP * threadIdx.y;
     auto rb = [&](int r) { return (row0 + r) * BX_W + col; };
-    bmp2_row<true, false>(sm, rb(0), 0, PA, PB, acc);
-    bmp2_row<true, false>(sm, rb(1), 1, PA, PB, acc);
-    for (int r = 2; r <= 21; r++) bmp2_row<true, true>(sm, rb(r), r, PA, PB, acc);
-    bmp2_row<false, true>(sm, rb(22), 22, PA, PB, acc);
-    bmp2_row<false, true>(sm, rb(23), 23, PA, PB, acc);
+    const BmPair& PA = PP[0];
+    const BmPair& PB = PP[NP / 2 - 1];  // the second pair (unused when NP = 2)
+    if constexpr (NP == 4) {
+        bmp2_row<true, false>(sm, rb(0), 0, PA, PB, acc);
+        bmp2_row<true, false>(sm, rb(1), 1, PA, PB, acc);
+        for (int r = 2; r <= 21; r++) bmp2_row<true, true>(sm, rb(r), r, PA, PB, acc);
+        bmp2_row<false, true>(sm, rb(22), 22, PA, PB, acc);
+        bmp2_row<false, true>(sm, rb(23), 23, PA, PB, acc);
+    } else {
+        for (int r = 0; r <= 21; r++) bmp2_row<true, false>(sm, rb(r), r, PA, PB, acc);
+    }
     float v[2][5][2];
     for (int q = 0; q < 2; q++)
         for (int k = 0; k < 5; k++) upk2(acc[q][k], v[q][k][0], v[q][k][1]);
@@ -460,14 +465,28 @@ __global__ void __launch_bounds__(BxTile<TY>::THREADS, TY == 8 ? 2 : 3)
 }
 
 
-template <int TY>
+template <int TY, int NP>
 static void launch_pair(Plane<__half, 4> img, Plane<__half, 2> grad, const float* basis, Plane<__half, 4> out,
                         const BlockMatchArgs& a, cudaStream_t s) {
-    const size_t smem = sizeof(BmPairSmem<TY>) + sizeof(__half) * BX_LW * BxTile<TY>::LH;
-    ensure_dynamic_smem(reinterpret_cast<const void*>(k_block_match_pair<TY>), int(smem));
+    using T = BxTile<TY, NP>;
+    const size_t smem = sizeof(BmPairSmem<T::H>) + sizeof(__half) * BX_LW * T::LH;
+    ensure_dynamic_smem(reinterpret_cast<const void*>(k_block_match_pair<TY, NP>), int(smem));
     dim3 b(BX_TX, TY);
-    dim3 g((img.w + BX_TX - 1) / BX_TX, (img.h + BX_NP * TY - 1) / (BX_NP * TY));
-    k_block_match_pair<TY><<<g, b, smem, s>>>(img, grad, basis, out, a);
+    dim3 g((img.w + BX_TX - 1) / BX_TX, (img.h + NP * TY - 1) / (NP * TY));
+    k_block_match_pair<TY, NP><<<g, b, smem, s>>>(img, grad, basis, out, a);
+}
+
+// the pair kernel's variants by code (10 TY + NP)
+static constexpr int kBmVariants[4] = {84, 44, 82, 162};
+
+static void launch_pair_variant(int code, Plane<__half, 4> img, Plane<__half, 2> grad, const float* basis,
+                                Plane<__half, 4> out, const BlockMatchArgs& a, cudaStream_t s) {
+    switch (code) {
+        case 44: launch_pair<4, 4>(img, grad, basis, out, a, s); break;
+        case 82: launch_pair<8, 2>(img, grad, basis, out, a, s); break;
+        case 162: launch_pair<16, 2>(img, grad, basis, out, a, s); break;
+        default: launch_pair<8, 4>(img, grad, basis, out, a, s); break;
+    }
 }
 
 // ============================================================ FP16-storage path, tensor-core form
@@ -916,15 +935,18 @@ void launch_pyramid_persistent(const PTask* tasks, int n, const PLevel* lv, PCou
     k_pyramid_persistent<<<grid, BM_THREADS, sizeof(PSmem), s>>>(tasks, n, lv, cnt, next, err, limit_ns);
 }
 
-// Tile-height autotuner of the FP16 block matcher. Both heights compute
-// identical results (the same per-pixel arithmetic and the same centring),
-// so the choice only changes speed: 32 x 32 tiles amortise the staged halo
-// better, 32 x 16 tiles fill the GPU on small pyramid levels. The first call
-// for a level size times both on the caller's stream (leaving the result in
-// `out`) and keeps the faster; later calls reuse the choice, and so do calls
-// made while the stream is being captured into a graph (default 32 x 32 for
-// a size not timed yet). GLS_BM_TILE=8 or 4 in the environment fixes the
-// height.
+// Tile autotuner of the FP16 block matcher. Its variants (thread rows x
+// pixels per thread: 8 x 4 and 16 x 2 for 32 x 32 tiles, 4 x 4 and 8 x 2
+// for 32 x 16) compute identical results (the same per-pixel arithmetic,
+// pairs of pixels in packed FP32, and the same centring), so the choice only
+// changes speed: 32 x 32 tiles amortise the staged halo better, 32 x 16
+// tiles fill the GPU on small pyramid levels, and one pair per thread
+// trades the reuse of a staged neighbour for occupancy. The first call for
+// a level size times every variant on the caller's stream (leaving the
+// result in `out`) and keeps the fastest; later calls reuse the choice, and
+// so do calls made while the stream is being captured into a graph
+// (default 8 x 4 for a size not timed yet). GLS_BM_TILE=84, 44, 82 or 162 in
+// the environment (or 8 / 4 for 84 / 44) fixes the variant.
 static std::mutex g_tile_mu;
 static std::map<std::pair<int, int>, int> g_tile_choice;
 
@@ -943,31 +965,44 @@ int bm_tile_list(int* whty, int max) {
 }
 
 template <class Run>
-static int bm_tile_height(int w, int h, Run&& run_variant, cudaStream_t s) {
+static int bm_tile_variant(int w, int h, Run&& run_variant, cudaStream_t s) {
     static const int forced = [] {
         const char* e = std::getenv("GLS_BM_TILE");
-        return e ? std::atoi(e) : 0;
+        const int v = e ? std::atoi(e) : 0;
+        if (v == 8) return 84;  // the thread-row counts of the two NP = 4 variants
+        if (v == 4) return 44;
+        for (int c : kBmVariants)
+            if (v == c) return v;
+        return 0;
     }();
-    if (forced == 4 || forced == 8) return forced;
+    if (forced) return forced;
     {
         std::lock_guard<std::mutex> lk(g_tile_mu);
         auto it = g_tile_choice.find({w, h});
         if (it != g_tile_choice.end()) return it->second;
     }
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return 8;
-    cudaEvent_t e[3];
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return 84;
+    constexpr int NV = sizeof(kBmVariants) / sizeof(kBmVariants[0]);
+    cudaEvent_t e[NV + 1];
     for (auto& ev : e) cudaEventCreate(&ev);
     cudaEventRecord(e[0], s);
-    run_variant(8);
-    cudaEventRecord(e[1], s);
-    run_variant(4);
-    cudaEventRecord(e[2], s);
-    float t8 = 0.f, t4 = 0.f;
-    int choice = 8;
-    if (cudaEventSynchronize(e[2]) == cudaSuccess && cudaEventElapsedTime(&t8, e[0], e[1]) == cudaSuccess &&
-        cudaEventElapsedTime(&t4, e[1], e[2]) == cudaSuccess)
-        choice = t4 < t8 ? 4 : 8;
+    for (int v = 0; v < NV; v++) {
+        run_variant(kBmVariants[v]);
+        cudaEventRecord(e[v + 1], s);
+    }
+    int choice = 84;
+    if (cudaEventSynchronize(e[NV]) == cudaSuccess) {
+        float best = 0.f;
+        for (int v = 0; v < NV; v++) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, e[v], e[v + 1]) != cudaSuccess) continue;
+            if (v == 0 || t < best) {
+                best = t;
+                choice = kBmVariants[v];
+            }
+        }
+    }
     for (auto& ev : e) cudaEventDestroy(ev);
     std::lock_guard<std::mutex> lk(g_tile_mu);
     g_tile_choice[{w, h}] = choice;
@@ -988,12 +1023,10 @@ void launch_block_match(Plane<S, 4> img, Plane<S, 2> grad, Plane<S, 8> pca, cons
             launch_mma(img, grad, basis, out, a, s);
             return;
         }
-        const int ty = bm_tile_height(img.w, img.h, [&](int t) {
-            if (t == 8) launch_pair<8>(img, grad, basis, out, a, s);
-            else launch_pair<4>(img, grad, basis, out, a, s);
+        const int code = bm_tile_variant(img.w, img.h, [&](int c) {
+            launch_pair_variant(c, img, grad, basis, out, a, s);
         }, s);
-        if (ty == 8) launch_pair<8>(img, grad, basis, out, a, s);
-        else if (ty == 4) launch_pair<4>(img, grad, basis, out, a, s);
+        if (code) launch_pair_variant(code, img, grad, basis, out, a, s);
     } else {
         ensure_dynamic_smem(reinterpret_cast<const void*>(k_block_match_plain<S>), int(sizeof(BmPlainSmem)));
         dim3 b(BP_TX, BP_TY);

@@ -392,8 +392,8 @@ __global__ void __launch_bounds__(256) k_raw_cross_denoise(Plane<S, 4> quad, Pla
 // Fused demosaic: interpolateGreen (demosaic.metal:215-316) ->
 // interpolateRedBlue (:318-416) -> interpolateRedBlueAtGreen (:418-521) ->
 // blendHighlightsImage (:523-564) -> optional transformImage (:649-662).
-// Output tile 32 x 16; halos: red/blue temporary +-3, green +-5, raw +-7.
-constexpr int DM_TW = 32, DM_TH = 16;
+// Output tile 32 x 32; halos: red/blue temporary +-3, green +-5, raw +-7.
+constexpr int DM_TW = 32, DM_TH = 32;
 constexpr int DM_RW = DM_TW + 14, DM_RH = DM_TH + 14;  // raw, origin -7
 constexpr int DM_GW = DM_TW + 10, DM_GH = DM_TH + 10;  // green + gradient, origin -5
 constexpr int DM_CW = DM_TW + 6, DM_CH = DM_TH + 6;    // red/blue temporary, origin -3

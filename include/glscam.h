@@ -341,11 +341,12 @@ gls_status gls_grain_tables(uint32_t seed, int32_t* perm, float* grad);
 
 /* Decisions of the FP16 block matcher's tile autotuner (no reference
  * counterpart): for each pyramid level size met so far in this process,
- * (width, height, tile height in threads: 8 = 32x32-pixel tiles, 4 = 32x16).
- * The first frame of a size times both heights and keeps the faster; both
- * compute identical results. Writes at most max_entries triples to
- * entries; *n receives the count. GLS_BM_TILE=8 or 4 in the environment
- * fixes the height. */
+ * (width, height, variant), variant = 10 x thread rows + pixels per thread:
+ * 84 and 162 for 32x32-pixel tiles, 44 and 82 for 32x16. The first frame of
+ * a size times every variant and keeps the fastest; all compute identical
+ * results. Writes at most max_entries triples to entries; *n receives the
+ * count. GLS_BM_TILE=84, 44, 82 or 162 in the environment (8 or 4 for 84 or
+ * 44) fixes the variant. */
 gls_status gls_block_match_tiles(int32_t* entries, int32_t max_entries, int32_t* n);
 
 /* ---- CameraCalibration<levels> (CameraCalibration.hpp:24-39) ----

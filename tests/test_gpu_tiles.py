@@ -1,9 +1,10 @@
 """The FFMA2 pair form of the FP16 block matcher (the default one) and
-its tile-height autotuner: 32 x 32 and 32 x 16 pixel tiles compute the same
-bits (same per-pixel arithmetic, same centring vector), so forcing either
-height through GLS_BM_TILE, or letting the autotuner choose, gives
+its tile autotuner: the variants (thread rows x pixels per thread 8x4,
+16x2 for 32 x 32 pixel tiles, 4x4, 8x2 for 32 x 16) compute the same bits
+(same per-pixel arithmetic, same pairing, same centring vector), so forcing
+any of them through GLS_BM_TILE, or letting the autotuner choose, gives
 identical frames. Each setting runs in its own process because the kernel
-choice and the height are read once per process."""
+choice and the variant are read once per process."""
 import json
 import os
 import subprocess
@@ -57,15 +58,18 @@ def _run(tmp_path, tag, tile):
     return frames, json.load(open(base + ".json"))
 
 
-def test_tile_heights_are_bit_identical(tmp_path):
-    f8, _ = _run(tmp_path, "h8", 8)
-    f4, _ = _run(tmp_path, "h4", 4)
+def test_tile_variants_are_bit_identical(tmp_path):
+    ref, _ = _run(tmp_path, "v84", 84)
+    for code in (44, 82, 162):
+        got, _ = _run(tmp_path, f"v{code}", code)
+        for rep in range(2):
+            for a, b in zip(ref[rep], got[rep]):
+                assert np.array_equal(a, b), code
     fa, tiles = _run(tmp_path, "auto", None)
     for rep in range(2):
-        for a, b, c in zip(f8[rep], f4[rep], fa[rep]):
-            assert np.array_equal(a, b)
+        for a, c in zip(ref[rep], fa[rep]):
             assert np.array_equal(a, c)
     # the autotuner timed every FP16 pyramid level size it met
-    assert tiles and all(t[2] in (4, 8) for t in tiles)
+    assert tiles and all(t[2] in (84, 44, 82, 162) for t in tiles)
     sizes = {(t[0], t[1]) for t in tiles}
     assert (640, 480) in sizes and (320, 240) in sizes
