@@ -232,12 +232,6 @@ __device__ __forceinline__ double rsqrt_nr(double x) {
     return r * fma(-hx * r, r, 1.5);
 }
 
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
 // Number of eigenvalues of the symmetric tridiagonal (d, e) below x: the
 // signs of the pivots of T - x I (Sturm sequence); a pivot smaller than
 // pivmin in magnitude is replaced by -pivmin.
