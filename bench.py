@@ -566,7 +566,7 @@ def mixed_leg(args, rank, local, conv, stream):
                    "note": "the one batch split over the ranks by pixel count (longest-processing-time); "
                            "value = batch MP / the slowest rank's share time"},
         "block_match_tile_heights": [list(t) for t in block_match_tiles()],
-        "note": "one CUDA graph replay per batch; frames spread largest-first over 3 slot streams; "
+        "note": "one CUDA graph replay per batch; frames spread largest-first over 6 slot streams; "
                 "block_match_tile_heights: autotuned (width, height, variant = 10 x thread rows + pixels per thread: 84 and 162 are 32x32-pixel tiles, 44 and 82 are 32x16)",
     }
 

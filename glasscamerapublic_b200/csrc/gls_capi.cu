@@ -205,8 +205,11 @@ struct KScope {
 }  // namespace gls
 
 // Frames of a batch run concurrently on kSlots streams, each slot with its
-// own planes; slot 0 also serves the single-frame calls.
-constexpr int kSlots = 3;
+// own planes (about 0.7 GB per slot at 12 MP in FP16); slot 0 also serves
+// the single-frame calls. Six slots: a 6-frame 12 MP batch runs 1% faster
+// than with three (more single-block kernels of one frame overlap other
+// frames' work), 2.5% faster than with two.
+constexpr int kSlots = 6;
 
 struct gls_converter {
     int device = 0;

@@ -665,36 +665,70 @@ __global__ void __launch_bounds__(256) k_demosaic(Plane<S, 1> raw, Plane<S, 2> g
 
 // --------------------------------------------------------------------------
 // despeckleLumaMedianChromaImage, demosaic.metal:1161-1283.
-__device__ __forceinline__ void sort2(float& a, float& b) {
-    const float t = fminf(a, b);
-    b = fmaxf(a, b);
-    a = t;
+// The chroma pair (Cb, Cr) of a pixel as one value for the median
+// network: a half2 on the FP16 path (the planes hold halves, so packing is
+// exact and one min/max instruction serves both channels), two floats on the
+// FP32 path.
+template <class S>
+struct ChromaPair {
+    float2 v;
+    __device__ __forceinline__ static ChromaPair of(const f4& p) { return {make_float2(p.y, p.z)}; }
+    __device__ __forceinline__ static ChromaPair mn(ChromaPair a, ChromaPair b) {
+        return {make_float2(fminf(a.v.x, b.v.x), fminf(a.v.y, b.v.y))};
+    }
+    __device__ __forceinline__ static ChromaPair mx(ChromaPair a, ChromaPair b) {
+        return {make_float2(fmaxf(a.v.x, b.v.x), fmaxf(a.v.y, b.v.y))};
+    }
+    __device__ __forceinline__ float2 get() const { return v; }
+};
+template <>
+struct ChromaPair<__half> {
+    __half2 v;
+    __device__ __forceinline__ static ChromaPair of(const f4& p) { return {__floats2half2_rn(p.y, p.z)}; }
+    __device__ __forceinline__ static ChromaPair mn(ChromaPair a, ChromaPair b) { return {__hmin2(a.v, b.v)}; }
+    __device__ __forceinline__ static ChromaPair mx(ChromaPair a, ChromaPair b) { return {__hmax2(a.v, b.v)}; }
+    __device__ __forceinline__ float2 get() const { return __half22float2(v); }
+};
+
+// a row of three sorted: (lo, mid, hi)
+template <class C>
+struct Sorted3 {
+    C lo, mid, hi;
+};
+template <class C>
+__device__ __forceinline__ Sorted3<C> sort3(C a, C b, C c) {
+    const C l1 = C::mn(a, b), h1 = C::mx(a, b);   // a, b ordered
+    const C m2 = C::mn(h1, c), hi = C::mx(h1, c);  // the largest
+    return {C::mn(l1, m2), C::mx(l1, m2), hi};
 }
-// exact median of 9 (a min/max selection network)
-__device__ __forceinline__ float median9(float v[9]) {
-    sort2(v[1], v[2]); sort2(v[4], v[5]); sort2(v[7], v[8]);
-    sort2(v[0], v[1]); sort2(v[3], v[4]); sort2(v[6], v[7]);
-    sort2(v[1], v[2]); sort2(v[4], v[5]); sort2(v[7], v[8]);
-    sort2(v[0], v[3]); sort2(v[5], v[8]); sort2(v[4], v[7]);
-    sort2(v[3], v[6]); sort2(v[1], v[4]); sort2(v[2], v[5]);
-    sort2(v[4], v[7]); sort2(v[4], v[2]); sort2(v[6], v[4]);
-    sort2(v[4], v[2]);
-    return v[4];
+template <class C>
+__device__ __forceinline__ C med3(C a, C b, C c) {
+    return C::mx(C::mn(a, b), C::mn(C::mx(a, b), c));
+}
+// The median of a 3 x 3 neighbourhood from its three sorted rows: the median
+// of (the largest row minimum, the median of the row medians, the smallest
+// row maximum). Exact (the median is one of the nine values), as the
+// reference's min/max elimination network (demosaic.metal:1161-1196) is;
+// the adjoint's selection network (gls_front_jvp.cu) picks the same value.
+template <class C>
+__device__ __forceinline__ C median9_rows(const Sorted3<C>& r0, const Sorted3<C>& r1, const Sorted3<C>& r2) {
+    const C lo = C::mx(C::mx(r0.lo, r1.lo), r2.lo);
+    const C hi = C::mn(C::mn(r0.hi, r1.hi), r2.hi);
+    return med3(lo, med3(r0.mid, r1.mid, r2.mid), hi);
 }
 
-// One output pixel from its 3 x 3 neighbourhood, rows r0..r2 of 3 loaded
-// pixels each, taken in the reference's order (j = -1..1, i = -1..1).
-__device__ __forceinline__ f4 despeckle_px(const f4 (&r0)[3], const f4 (&r1)[3], const f4 (&r2)[3], float va,
-                                           float vb) {
-    float cb[9], cr[9];
+// The luma part of one output pixel from its 3 x 3 neighbourhood, rows
+// r0..r2 of 3 loaded pixels each, taken in the reference's order
+// (j = -1..1, i = -1..1).
+__device__ __forceinline__ float despeckle_luma(const f4 (&r0)[3], const f4 (&r1)[3], const f4 (&r2)[3], float va,
+                                                float vb) {
     float fmx = 0.f, smx = 0.f, fmn = INFINITY, smn = INFINITY, sample = 0.f;
     const f4* rows[3] = {r0, r1, r2};
 #pragma unroll
     for (int j = 0; j < 3; j++)
 #pragma unroll
         for (int i = 0; i < 3; i++) {
-            const f4 p = rows[j][i];
-            const float v = p.x;
+            const float v = rows[j][i].x;
             smx = (v <= fmx && v > smx) ? v : smx;
             smx = v > fmx ? fmx : smx;
             fmx = v > fmx ? v : fmx;
@@ -702,19 +736,19 @@ __device__ __forceinline__ f4 despeckle_px(const f4 (&r0)[3], const f4 (&r1)[3],
             smn = v < fmn ? fmn : smn;
             fmn = v < fmn ? v : fmn;
             if (i == 1 && j == 1) sample = v;
-            cb[3 * j + i] = p.y;
-            cr[3 * j + i] = p.z;
         }
     const float sigma = sqrtf(va + vb * sample);
     const float mn = mixf(smn, fmn, smoothstepf(sigma, 4.f * sigma, smn - fmn));
     const float mx = mixf(smx, fmx, smoothstepf(sigma, 4.f * sigma, fmx - smx));
-    return f4{clampf(sample, mn, mx), median9(cb), median9(cr), 0.f};
+    return clampf(sample, mn, mx);
 }
 
 // Two vertically adjacent pixels per thread: they share two of their three
-// neighbourhood rows (12 loads instead of 18).
+// neighbourhood rows (12 loads instead of 18), and the chroma medians share
+// the sorting of those rows (four row sorts for two medians).
 template <class S>
 __global__ void __launch_bounds__(256) k_despeckle(Plane<S, 4> in, Plane<S, 4> out, float va, float vb) {
+    using C = ChromaPair<S>;
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = 2 * (blockIdx.y * blockDim.y + threadIdx.y);
     if (x >= in.w || y >= in.h) return;
     f4 r[4][3];
@@ -722,8 +756,15 @@ __global__ void __launch_bounds__(256) k_despeckle(Plane<S, 4> in, Plane<S, 4> o
     for (int j = 0; j < 4; j++)
 #pragma unroll
         for (int i = 0; i < 3; i++) r[j][i] = ld4<S>(in.pxc(x + i - 1, y + j - 1));
-    st4<S>(out.px(x, y), despeckle_px(r[0], r[1], r[2], va, vb));
-    if (y + 1 < in.h) st4<S>(out.px(x, y + 1), despeckle_px(r[1], r[2], r[3], va, vb));
+    Sorted3<C> rs[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) rs[j] = sort3(C::of(r[j][0]), C::of(r[j][1]), C::of(r[j][2]));
+    const float2 m0 = median9_rows(rs[0], rs[1], rs[2]).get();
+    st4<S>(out.px(x, y), f4{despeckle_luma(r[0], r[1], r[2], va, vb), m0.x, m0.y, 0.f});
+    if (y + 1 < in.h) {
+        const float2 m1 = median9_rows(rs[1], rs[2], rs[3]).get();
+        st4<S>(out.px(x, y + 1), f4{despeckle_luma(r[1], r[2], r[3], va, vb), m1.x, m1.y, 0.f});
+    }
 }
 
 // transformImage, demosaic.metal:649-662, from plane S4 to an output of
