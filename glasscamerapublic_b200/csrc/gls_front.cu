@@ -96,11 +96,11 @@ __global__ void __launch_bounds__(256) k_scale_raw8(const uint16_t* __restrict__
 
 // --------------------------------------------------------------------------
 // rawImageSobel + sampledConvolutionSobel fused, demosaic.metal:120-213.
-// Output tile 32 x 16 per 256-thread block. Shared memory: the scaled raw
+// Output tile 32 x 32 per 256-thread block. Shared memory: the scaled raw
 // tile with a 5-pixel halo (+1 right/bottom for the bilinear pair) and the
 // Sobel (gx, gy) tile with a 4/5-pixel halo. The blur taps are bilinear
 // samples at integer + fractional offsets (host-computed Gaussian folding).
-constexpr int SB_TW = 32, SB_TH = 16;
+constexpr int SB_TW = 32, SB_TH = 32;
 constexpr int SB_RW = SB_TW + 11, SB_RH = SB_TH + 11;  // raw tile, origin -5
 constexpr int SB_SW = SB_TW + 9, SB_SH = SB_TH + 9;    // sobel tile, origin -4
 
