@@ -366,21 +366,51 @@ __global__ void __launch_bounds__(256) k_raw_cross_denoise(Plane<S, 4> quad, Pla
 #pragma unroll
     for (int c = 0; c < 4; c++) inv[c] = 1.f / (a.strength * sqrtf(a.var[c] * (pc[c] + 0.0001f)));
     float sum[4] = {0, 0, 0, 0}, sw = 0;
-    for (int j = -2; j <= 2; j++)
-        for (int i = -2; i <= 2; i++) {
-            const f4 s = ld4<S>(quad.pxc(qx + i, qy + j));
-            const float sc[4] = {s.x, s.y, s.z, s.w};
-            float d2 = 0;
+    if (is_half<S>::value && a.fast) {
+        // FP16 storage: the weight exp(-2 d^2) as exp2(-|(p - s) k|^2) with
+        // k = inv sqrt(2 log2 e) folded into the inverse, and (p - s) k as
+        // one FMA per channel with p k precomputed
+        float ki[4], pk[4];
 #pragma unroll
-            for (int c = 0; c < 4; c++) {
-                const float d = (pc[c] - sc[c]) * inv[c];
-                d2 += d * d;
-            }
-            const float w = a.fast ? __expf(-2.f * d2) : expf(-2.f * d2);
-#pragma unroll
-            for (int c = 0; c < 4; c++) sum[c] += w * sc[c];
-            sw += w;
+        for (int c = 0; c < 4; c++) {
+            ki[c] = inv[c] * 1.6986436f;  // sqrt(2 log2 e)
+            pk[c] = pc[c] * ki[c];
         }
+#pragma unroll
+        for (int j = -2; j <= 2; j++)
+#pragma unroll
+            for (int i = -2; i <= 2; i++) {
+                const f4 s = ld4<S>(quad.pxc(qx + i, qy + j));
+                const float sc[4] = {s.x, s.y, s.z, s.w};
+                float d2 = 0.f;
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    const float d = fmaf(-sc[c], ki[c], pk[c]);
+                    d2 = fmaf(d, d, d2);
+                }
+                float w;
+                asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(w) : "f"(-d2));
+#pragma unroll
+                for (int c = 0; c < 4; c++) sum[c] = fmaf(w, sc[c], sum[c]);
+                sw += w;
+            }
+    } else {
+        for (int j = -2; j <= 2; j++)
+            for (int i = -2; i <= 2; i++) {
+                const f4 s = ld4<S>(quad.pxc(qx + i, qy + j));
+                const float sc[4] = {s.x, s.y, s.z, s.w};
+                float d2 = 0;
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    const float d = (pc[c] - sc[c]) * inv[c];
+                    d2 += d * d;
+                }
+                const float w = a.fast ? __expf(-2.f * d2) : expf(-2.f * d2);
+#pragma unroll
+                for (int c = 0; c < 4; c++) sum[c] += w * sc[c];
+                sw += w;
+            }
+    }
 #pragma unroll
     for (int c = 0; c < 4; c++) {
         const int ox = kBayer[a.pattern][c][0], oy = kBayer[a.pattern][c][1];
