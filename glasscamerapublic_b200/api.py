@@ -140,8 +140,8 @@ class RawConverter:
 
         ``raws``/``outs``: torch CUDA tensors (device I/O), or host buffers
         (numpy arrays or pinned torch CPU tensors; copied inside the call).
-        ``tensor_bm``: the tensor-core block matcher (GLS_BM_TENSOR), the one
-        the persistent batch runs.
+        ``tensor_bm``: the tensor-core block matcher (GLS_BM_TENSOR; stream-
+        launched batches, the persistent batch runs the default matcher).
         """
         n = len(raws)
         frames = (FrameDesc * n)()

@@ -308,19 +308,35 @@ constexpr int BX_LW = BX_W + 4;  // luma tile width, origin (x0 - 12, y0 - 12)
 
 __device__ __forceinline__ uint32_t h2u(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
 
+// shared memory of one pair-form tile: the staged window region, the
+// centring vector and basis, then the luma tile (BX_LH x BX_LW halves)
 template <int TY, int NP>
-__global__ void __launch_bounds__(BxTile<TY, NP>::THREADS, BxTile<TY, NP>::MIN_BLOCKS)
-    k_block_match_pair(Plane<__half, 4> img, Plane<__half, 2> grad, const float* __restrict__ basis,
-                       Plane<__half, 4> out, BlockMatchArgs a) {
+struct BmPairTileSmem {
+    BmPairSmem<BxTile<TY, NP>::H> w;
+    float cen[8];
+    float bsm[25][8];
+};
+template <int TY, int NP>
+constexpr size_t bm_pair_smem_bytes() {
+    return sizeof(BmPairTileSmem<TY, NP>) + sizeof(__half) * BX_LW * BxTile<TY, NP>::LH;
+}
+
+// One tile (origin x0, y0) of the pair form by TY x 32 threads; the thread
+// is (tcol, trow) of the tile. Shared by the stream kernel and the
+// persistent kernel's block-matching tasks.
+template <int TY, int NP>
+__device__ __forceinline__ void bm_pair_tile(int x0, int y0, int tcol, int trow, const Plane<__half, 4>& img,
+                                             const Plane<__half, 2>& grad, const float* __restrict__ basis,
+                                             const Plane<__half, 4>& out, const BlockMatchArgs& a,
+                                             unsigned char* smem_raw) {
     using T = BxTile<TY, NP>;
     constexpr int BX_H = T::H, BX_LH = T::LH, NT = T::THREADS, BX_NP = NP;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    BmPairSmem<BX_H>& sm = *reinterpret_cast<BmPairSmem<BX_H>*>(smem_raw);
-    __half* luma = reinterpret_cast<__half*>(smem_raw + sizeof(BmPairSmem<BX_H>));  // BX_LH x BX_LW
-    __shared__ float cen[8];
-    __shared__ float bsm[25][8];
-    const int x0 = blockIdx.x * BX_TX, y0 = blockIdx.y * (BX_NP * TY);
-    const int tid = threadIdx.y * BX_TX + threadIdx.x;
+    BmPairTileSmem<TY, NP>& st = *reinterpret_cast<BmPairTileSmem<TY, NP>*>(smem_raw);
+    BmPairSmem<BX_H>& sm = st.w;
+    __half* luma = reinterpret_cast<__half*>(smem_raw + sizeof(BmPairTileSmem<TY, NP>));  // BX_LH x BX_LW
+    float* cen = st.cen;
+    float (*bsm)[8] = st.bsm;
+    const int tid = trow * BX_TX + tcol;
     const float kLog2e = 1.4426950408889634f, lk = 2.f * kLog2e, isq = rsqrtf(lk);
     for (int k = tid; k < 22 * 21; k += NT) {
         const int j = k / 21, i = k % 21 - 10;
@@ -403,11 +419,11 @@ __global__ void __launch_bounds__(BxTile<TY, NP>::THREADS, BxTile<TY, NP>::MIN_B
         }
     }
     __syncthreads();
-    const int x = x0 + threadIdx.x, y = y0 + BX_NP * threadIdx.y;
+    const int x = x0 + tcol, y = y0 + BX_NP * trow;
     float pc[BX_NP][8], kl[BX_NP], base[BX_NP], c1[BX_NP], c2[BX_NP], o1[BX_NP], o2[BX_NP];
 #pragma unroll
     for (int p = 0; p < BX_NP; p++) {
-        const int c = (BX_NP * threadIdx.y + p + 10) * BX_W + threadIdx.x + 10;
+        const int c = (BX_NP * trow + p + 10) * BX_W + tcol + 10;
         const float4 in = sm.ycc[c];
         const uint4 u = sm.pca[c];
         const float2 a0 = __half22float2(u2h_(u.x)), a1 = __half22float2(u2h_(u.y));
@@ -437,7 +453,7 @@ __global__ void __launch_bounds__(BxTile<TY, NP>::THREADS, BxTile<TY, NP>::MIN_B
     }
     u64 acc[2][5];
     for (int k = 0; k < 5; k++) acc[0][k] = acc[1][k] = pk2(0.f, 0.f);
-    const int col = threadIdx.x, row0 = BX_NP * threadIdx.y;
+    const int col = tcol, row0 = BX_NP * trow;
     auto rb = [&](int r) { return (row0 + r) * BX_W + col; };
     const BmPair& PA = PP[0];
     const BmPair& PB = PP[NP / 2 - 1];  // the second pair (unused when NP = 2)
@@ -466,10 +482,18 @@ __global__ void __launch_bounds__(BxTile<TY, NP>::THREADS, BxTile<TY, NP>::MIN_B
 
 
 template <int TY, int NP>
+__global__ void __launch_bounds__(BxTile<TY, NP>::THREADS, BxTile<TY, NP>::MIN_BLOCKS)
+    k_block_match_pair(Plane<__half, 4> img, Plane<__half, 2> grad, const float* __restrict__ basis,
+                       Plane<__half, 4> out, BlockMatchArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    bm_pair_tile<TY, NP>(blockIdx.x * BX_TX, blockIdx.y * (NP * TY), threadIdx.x, threadIdx.y, img, grad, basis, out,
+                         a, smem_raw);
+}
+
+template <int TY, int NP>
 static void launch_pair(Plane<__half, 4> img, Plane<__half, 2> grad, const float* basis, Plane<__half, 4> out,
                         const BlockMatchArgs& a, cudaStream_t s) {
-    using T = BxTile<TY, NP>;
-    const size_t smem = sizeof(BmPairSmem<T::H>) + sizeof(__half) * BX_LW * T::LH;
+    const size_t smem = bm_pair_smem_bytes<TY, NP>();
     ensure_dynamic_smem(reinterpret_cast<const void*>(k_block_match_pair<TY, NP>), int(smem));
     dim3 b(BX_TX, TY);
     dim3 g((img.w + BX_TX - 1) / BX_TX, (img.h + NP * TY - 1) / (NP * TY));
@@ -814,7 +838,7 @@ static void launch_mma(Plane<__half, 4> img, Plane<__half, 2> grad, const float*
 // returns GLS_ERR_TIMEOUT.
 struct PSmem {
     union {
-        BmMmaSmem bm;
+        alignas(16) unsigned char bm[bm_pair_smem_bytes<8, 4>()];  // a 32 x 32 tile of the pair form
         EigenSmem eig;
         CovSmem cov;
     };
@@ -836,6 +860,14 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
 // do not weigh on the block-matching path
 __device__ __noinline__ void persistent_eigen(const PLevel& L, EigenSmem& sm) {
     pca_eigen_block(L.part, L.n_cov, (L.layer.w / 8) * (L.layer.h / 8), L.basis, L.status, sm);
+}
+
+// a block-matching task: one 32 x 32 tile of the default (pair-form)
+// matcher in its 8 x 4 variant, the same bits as every stream variant
+__device__ __noinline__ void persistent_bm(const PLevel& L, uint32_t item, unsigned char* smem) {
+    const int tx = int(item) % L.tiles_x, ty = int(item) / L.tiles_x;
+    bm_pair_tile<8, 4>(tx * BM_T, ty * BM_T, threadIdx.x & 31, threadIdx.x >> 5, L.layer, L.grad, L.basis, L.den,
+                       L.ba, smem);
 }
 
 __global__ void __launch_bounds__(BM_THREADS, 2)
@@ -907,8 +939,7 @@ __global__ void __launch_bounds__(BM_THREADS, 2)
             persistent_eigen(L, sm.eig);
             done = &cnt[tk.lev].eig;
         } else {
-            const int tx = item % L.tiles_x, ty = item / L.tiles_x;
-            bm_mma_tile(tx * BM_T, ty * BM_T, L.layer, L.grad, L.basis, L.den, L.ba, sm.bm);
+            persistent_bm(L, item, sm.bm);
             done = &cnt[tk.lev].bm;
         }
         __syncthreads();  // the task's writes, and its shared memory, are finished

@@ -142,10 +142,10 @@ enum {
     GLS_SURF_CORRECTED = 1u << 7, /* gls_surf_detect_and_compute: the corrected detector (see there) */
     GLS_PERSISTENT = 1u << 8,    /* gls_demosaic_batch: every pyramid level of every frame in one persistent
                                     launch (see there) */
-    GLS_BM_TENSOR = 1u << 9      /* FP16 storage: block matching with the patch distances and the weighted
-                                    sums on the tensor cores and the weights in half precision (the matcher
-                                    the persistent batch runs); without it the FP16 matcher computes every
-                                    weight in packed FP32 */
+    GLS_BM_TENSOR = 1u << 9      /* FP16 storage, stream-launched: block matching with the patch distances
+                                    and the weighted sums on the tensor cores and the weights in half
+                                    precision; without it the FP16 matcher computes every weight in packed
+                                    FP32 (the persistent batch always does) */
 };
 
 /* Planes a converter exposes after gls_demosaic, for stage checks. */
@@ -242,9 +242,10 @@ typedef struct gls_frame_desc {
  * kernel runs every level of every frame (reconstruct, covariance,
  * eigen-solve and block matching, PyramidProcessor::denoise,
  * pyramid_processor.cpp:96-172) from a device work list whose tasks wait
- * on per-level counters, then the output transforms run; its block
- * matching is the tensor-core matcher, so the results are bit-identical to
- * the stream-launched batch with GLS_BM_TENSOR. The call returns after the
+ * on per-level counters, then the output transforms run; it runs the
+ * stream kernels' device code (the default packed-FP32 block matcher), so
+ * the results are bit-identical to the stream-launched batch. The call
+ * returns after the
  * kernel, with GLS_ERR_TIMEOUT if a task's wait for its inputs ran past
  * its limit (2 s). Combined with GLS_GRAPH the whole sequence is recorded
  * and replayed. */

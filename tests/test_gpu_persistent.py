@@ -1,9 +1,9 @@
 """The persistent batch kernel (GLS_PERSISTENT): every pyramid level of
 every frame of a batch in one launch, from a device work list whose tasks
 wait on per-level counters. It runs the stream kernels' device code (the
-tensor-core block matcher, GLS_BM_TENSOR), so a batch of uneven frames
-gives the same bits as the stream-launched batch with that matcher, also
-when recorded and replayed as a graph. Failure detection: a task
+default block matcher's tile), so a batch of uneven frames gives the same
+bits as the stream-launched batch, also when recorded and replayed as a
+graph. Failure detection: a task
 whose input never arrives ends its bounded wait with GLS_ERR_TIMEOUT and
 leaves the device usable (no fault, no hang)."""
 import ctypes as C
@@ -40,7 +40,7 @@ def test_persistent_batch_bit_identical_to_stream_batch(converter):
     st = torch.cuda.Stream()
     raws, params = _batch(500)
     ref, got = _outs(), _outs()
-    converter.demosaic_batch(raws, params, ref, stream=st, tensor_bm=True)
+    converter.demosaic_batch(raws, params, ref, stream=st)
     converter.demosaic_batch(raws, params, got, stream=st, persistent=True)
     st.synchronize()
     for a, b in zip(ref, got):
@@ -57,14 +57,14 @@ def test_persistent_batch_recorded_as_graph(converter):
     st = torch.cuda.Stream()
     raws, params = _batch(600)
     ref, got = _outs(), _outs()
-    converter.demosaic_batch(raws, params, ref, stream=st, tensor_bm=True)
+    converter.demosaic_batch(raws, params, ref, stream=st)
     converter.demosaic_batch(raws, params, got, stream=st, persistent=True, graph=True)  # runs and records
     st.synchronize()
     assert all(torch.equal(a, b) for a, b in zip(ref, got))
     new_raws, _ = _batch(700)
     for r, n in zip(raws, new_raws):
         r.copy_(n)
-    converter.demosaic_batch(raws, params, ref, stream=st, tensor_bm=True)
+    converter.demosaic_batch(raws, params, ref, stream=st)
     for o in got:
         o.zero_()
     converter.demosaic_batch(raws, params, got, stream=st, persistent=True, graph=True)  # replays
@@ -94,7 +94,7 @@ def test_persistent_wait_times_out_and_device_stays_usable(converter):
     st = torch.cuda.Stream()
     raws, params = _batch(900)
     ref, got = _outs(), _outs()
-    converter.demosaic_batch(raws, params, ref, stream=st, tensor_bm=True)
+    converter.demosaic_batch(raws, params, ref, stream=st)
     converter.demosaic_batch(raws, params, got, stream=st, persistent=True)
     st.synchronize()
     assert all(torch.equal(a, b) for a, b in zip(ref, got))
