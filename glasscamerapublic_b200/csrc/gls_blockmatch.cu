@@ -819,7 +819,7 @@ static void launch_mma(Plane<__half, 4> img, Plane<__half, 2> grad, const float*
 // ============================================================ persistent batch kernel
 // PyramidProcessor::denoise (pyramid_processor.cpp:96-172) for every frame
 // of a batch in one launch. The host lists the work of every (frame,
-// level) as tasks: reconstruct tiles (SN, 32 x 32 pixels), covariance
+// level) as tasks: reconstruct tiles (SN, 64 x 64 pixels), covariance
 // partial rows (COV), the eigen-solve (EIG) and block-matching tiles (BM,
 // 32 x 32), level by level from the coarsest, all frames' SN / COV / EIG of
 // a level before their BM tiles. A block takes the next task from a
@@ -856,18 +856,31 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
     return v;
 }
 
+// The two calls below take the block's shared memory from the extern
+// array itself, not as a pointer argument: across a call boundary a pointer
+// is generic, and the tile's staged reads would compile to generic loads
+// instead of shared-memory loads. Their level arguments are copied out of
+// the descriptor once, as a kernel's parameters would be.
+
 // the rarely taken eigen-solve as a call of its own, so that its registers
 // do not weigh on the block-matching path
-__device__ __noinline__ void persistent_eigen(const PLevel& L, EigenSmem& sm) {
-    pca_eigen_block(L.part, L.n_cov, (L.layer.w / 8) * (L.layer.h / 8), L.basis, L.status, sm);
+__device__ __noinline__ void persistent_eigen(const PLevel& L) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    pca_eigen_block(L.part, L.n_cov, (L.layer.w / 8) * (L.layer.h / 8), L.basis, L.status,
+                    reinterpret_cast<PSmem*>(smem_raw)->eig);
 }
 
 // a block-matching task: one 32 x 32 tile of the default (pair-form)
 // matcher in its 8 x 4 variant, the same bits as every stream variant
-__device__ __noinline__ void persistent_bm(const PLevel& L, uint32_t item, unsigned char* smem) {
+__device__ __noinline__ void persistent_bm(const PLevel& L, uint32_t item) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Plane<__half, 4> layer = L.layer, den = L.den;
+    const Plane<__half, 2> grad = L.grad;
+    const float* basis = L.basis;
+    const BlockMatchArgs ba = L.ba;
     const int tx = int(item) % L.tiles_x, ty = int(item) / L.tiles_x;
-    bm_pair_tile<8, 4>(tx * BM_T, ty * BM_T, threadIdx.x & 31, threadIdx.x >> 5, L.layer, L.grad, L.basis, L.den,
-                       L.ba, smem);
+    bm_pair_tile<8, 4>(tx * BM_T, ty * BM_T, threadIdx.x & 31, threadIdx.x >> 5, layer, grad, basis, den, ba,
+                       reinterpret_cast<PSmem*>(smem_raw)->bm);
 }
 
 __global__ void __launch_bounds__(BM_THREADS, 2)
@@ -924,9 +937,9 @@ __global__ void __launch_bounds__(BM_THREADS, 2)
         if (!s_ok) break;
         int* done;
         if (type == PT_SN) {
-            const int tx = item % L.tiles_x, ty = item / L.tiles_x;
-            for (int k = threadIdx.x; k < BM_T * BM_T; k += BM_THREADS) {
-                const int x = tx * BM_T + k % BM_T, y = ty * BM_T + k / BM_T;
+            const int tx = item % L.sn_tiles_x, ty = item / L.sn_tiles_x;
+            for (int k = threadIdx.x; k < kPSnTile * kPSnTile; k += BM_THREADS) {
+                const int x = tx * kPSnTile + k % kPSnTile, y = ty * kPSnTile + k / kPSnTile;
                 if (x < L.img.w && y < L.img.h)
                     subtract_noise_px<__half>(L.img, L.coarse, L.coarse_den, L.grad, L.layer, L.sa, L.rx, L.ry, x, y);
             }
@@ -936,10 +949,10 @@ __global__ void __launch_bounds__(BM_THREADS, 2)
             pca_cov_row<__half>(L.layer, L.part + size_t(item) * kPcaAcc, c0, min(c0 + L.cov_group, L.chunks), sm.cov);
             done = &cnt[tk.lev].cov;
         } else if (type == PT_EIG) {
-            persistent_eigen(L, sm.eig);
+            persistent_eigen(L);
             done = &cnt[tk.lev].eig;
         } else {
-            persistent_bm(L, item, sm.bm);
+            persistent_bm(L, item);
             done = &cnt[tk.lev].bm;
         }
         __syncthreads();  // the task's writes, and its shared memory, are finished

@@ -1076,13 +1076,19 @@ static gls_status persistent_plan(gls_converter* conv, const gls_frame_desc* fra
             d.basis = static_cast<float*>(P.basis.p) + i * 200;
             d.status = static_cast<int*>(P.status.p) + i;
             d.tiles_x = (wi + 31) / 32;
-            const int tiles = d.tiles_x * ((hi + 31) / 32);
-            d.n_bm = tiles;
-            d.n_sn = i < L - 1 ? tiles : 0;
+            d.n_bm = d.tiles_x * ((hi + 31) / 32);
+            d.sn_tiles_x = (wi + kPSnTile - 1) / kPSnTile;
+            d.n_sn = i < L - 1 ? d.sn_tiles_x * ((hi + kPSnTile - 1) / kPSnTile) : 0;
             d.n_cov = pca_cov_rows(wi, hi);
             d.chunks = pca_cov_chunks(wi, hi);
             d.cov_group = pca_cov_group(d.chunks);
             d.coarser = i < L - 1 ? first[f] + i + 1 : -1;
+            // every plane the kernel reads or writes must exist (the front
+            // ends, which run before the plan is built, size them)
+            if (!d.img.p || !d.grad.p || !d.layer.p || !d.den.p || !P.acc.p || !P.basis.p || !P.status.p ||
+                (i < L - 1 && (!d.coarse.p || !d.coarse_den.p)))
+                return set_error(GLS_ERR_INVALID_ARG, "persistent plan: frame %d level %d has unallocated planes", f,
+                                 i);
             lv.push_back(d);
         }
     }

@@ -138,6 +138,9 @@ struct PTask {
     uint32_t item;  // type in the top 2 bits; tile / row index below
 };
 constexpr uint32_t kPTaskItemMask = 0x3fffffffu;
+// side of a persistent reconstruct task's tile: 64 x 64 pixels (16 per
+// thread), so the per-task fetch and bookkeeping stay small beside the work
+constexpr int kPSnTile = 64;
 struct PLevel {
     Plane<__half, 4> img, layer, den;  // the level's image, reconstructed layer, denoised output
     Plane<__half, 2> grad;
@@ -149,7 +152,8 @@ struct PLevel {
     float rx, ry;                         // coarse / fine size ratios
     BlockMatchArgs ba;
     int n_sn, n_cov, n_bm;                // task counts of the level
-    int tiles_x;                          // 32-pixel tiles across the level
+    int tiles_x;                          // 32-pixel block-matching tiles across the level
+    int sn_tiles_x;                       // reconstruct tiles (kPSnTile pixels square) across the level
     int chunks;                           // 64-patch covariance chunks
     int cov_group;                        // chunks per covariance row (pca_cov_group)
     int coarser;                          // descriptor of the next coarser level, -1 at the coarsest
