@@ -195,6 +195,28 @@ class CalibrationTuner:
         t.base_params = base_params
         return t
 
+    @staticmethod
+    def job_share(sizes, dist=None) -> list[int]:
+        """This rank's frames of a job of frames with the given (width,
+        height): the pixel-count split of shard.assign_frames, all frames
+        without a process group."""
+        from .shard import assign_frames
+        active = dist is not None and dist.is_available() and dist.is_initialized()
+        world, rank = (dist.get_world_size(), dist.get_rank()) if active else (1, 0)
+        return assign_frames([(int(w), int(h)) for w, h in sizes], world)[rank]
+
+    @classmethod
+    def for_job(cls, converter, frames: Sequence, targets: Sequence, base_params, lr: float = 0.05,
+                dist=None, stream=None) -> "CalibrationTuner":
+        """for_frames over this rank's share of the whole job's frames
+        (job_share of their sizes). Every rank passes the same lists; each
+        steps on the mean over all of them."""
+        if len(frames) != len(targets):
+            raise ValueError("frames and targets differ in length")
+        mine = cls.job_share([(f.shape[1], f.shape[0]) for f in frames], dist)
+        return cls.for_frames(converter, [frames[i] for i in mine], [targets[i] for i in mine], base_params, lr,
+                              dist, stream)
+
     def params(self):
         """The current parameters as DemosaicParams (tuners from for_frames)."""
         from .adjoint import theta_to_params

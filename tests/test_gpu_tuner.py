@@ -31,6 +31,9 @@ def test_tuner_mean_matches_per_frame_adjoint(converter):
     per = [A.loss_and_grad(converter, r, p, t) for r, t in zip(raws, targets)]
     assert loss == pytest.approx(np.mean([l for l, _ in per]), rel=1e-12)
     assert np.allclose(grad, np.mean([g.astype(np.float64) for _, g in per], axis=0), rtol=1e-12, atol=0)
+    # one process holds the whole job: for_job takes every frame
+    lj, gj = CalibrationTuner.for_job(converter, raws, targets, p).evaluate()
+    assert lj == loss and np.array_equal(gj, grad)
 
 
 def test_tuner_lowers_the_loss_from_a_miscalibrated_start(converter, tmp_path):

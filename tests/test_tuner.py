@@ -154,3 +154,47 @@ def test_two_gloo_ranks_step_together(tmp_path):
     back = CalibrationTuner(np.ones(ADJ_NPARAMS), None, 0)
     back.load(ck)
     assert back.theta.tolist() == th0
+
+
+def test_job_share_without_a_process_group_is_every_frame():
+    assert CalibrationTuner.job_share([(64, 48), (32, 24), (128, 96)]) == [0, 1, 2]
+
+
+_JOB_SIZES = [(640, 480), (320, 240), (800, 600), (160, 120)]
+
+
+def _share_worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        mine = CalibrationTuner.job_share(_JOB_SIZES, dist)
+        t0 = _theta0()
+        fn = _quadratic(t0 * 0.8, np.ones(ADJ_NPARAMS))
+        tun = CalibrationTuner(t0, lambda th, i: fn(th, mine[i]), len(mine), lr=0.05, dist=dist)
+        tun.run(4)
+        q.put((rank, mine, tun.theta.tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [3, 5])
+def test_gloo_ranks_share_a_job(world):
+    # five ranks over four frames: one rank holds none and still takes part
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_share_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert sorted(i for _, mine, _ in res for i in mine) == list(range(len(_JOB_SIZES)))
+    assert all(th == res[0][2] for _, _, th in res)
+    t0 = _theta0()
+    single = CalibrationTuner(t0, _quadratic(t0 * 0.8, np.ones(ADJ_NPARAMS)), len(_JOB_SIZES), lr=0.05)
+    single.run(4)
+    assert np.allclose(res[0][2], single.theta, rtol=1e-12, atol=0)
