@@ -258,7 +258,9 @@ struct BmPair {  // two pixels, each member of a pair register = one pixel
 template <bool A, bool B, class Sm>
 __device__ __forceinline__ void bmp2_row(const Sm& sm, int base, int r, const BmPair& pa, const BmPair& pb,
                                          u64 (&acc)[2][5]) {
-#pragma unroll 7
+    // unrolled 3 of the row's 21 taps: 0.9% faster per 12 MP frame than 7,
+    // 1.2% than 1, 1.6% than all 21 (which spills)
+#pragma unroll 3
     for (int i = 0; i < 21; i++) {
         const uint4 u = sm.pca[base + i];
         const float2 a0 = __half22float2(u2h_(u.x)), a1 = __half22float2(u2h_(u.y));
